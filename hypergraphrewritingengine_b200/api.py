@@ -1,0 +1,493 @@
+"""ctypes binding of ``libhgx.so`` (include/hgx.h) and the reference-shaped Python API.
+
+Two layers:
+
+* ``Engine`` -- thin wrapper of the C-ABI: ``evolve``, ``evolve_batch`` and the serving calls,
+  returning results as numpy arrays (``EvolveResult``).
+* ``make_rule`` / ``RuleBuilder`` / ``Hypergraph`` / ``ParallelEvolutionEngine`` -- the same
+  surface as the reference C++ engine API (hypergraph/include/hypergraph/pattern.hpp:142-213,
+  parallel_evolution.hpp:743-1041, hypergraph.hpp:567-811), so a caller of the reference can
+  switch with the same call sequence:
+
+      hg = Hypergraph()
+      engine = ParallelEvolutionEngine(hg)
+      engine.add_rule(make_rule(0).lhs([0, 1]).lhs([1, 2]).rhs([0, 1]).rhs([1, 2]).rhs([2, 0]).build())
+      engine.set_transitive_reduction(False)
+      engine.evolve([[1, 2], [2, 3], [3, 1]], 5)
+      hg.num_states(), hg.num_events(), hg.num_canonical_states()
+
+The CUDA library is required: there is no CPU fallback, and every call fails loudly (OSError
+or HgxError) when the library or a device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhgx.so")
+
+HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_ERR_INTERNAL = range(6)
+(OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
+ OPT_KEEP_STATE_EDGES, OPT_TIMING) = range(7)
+(COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
+ COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES) = range(10)
+(ARR_STATE_HASH, ARR_STATE_DEPTH, ARR_EVENTS, ARR_CAUSAL, ARR_BRANCHIAL, ARR_EVENT_CONS_OFF,
+ ARR_EVENT_CONS, ARR_EVENT_PROD, ARR_STATE_EDGE_OFF, ARR_STATE_EDGE_IDS, ARR_STATE_ARITY,
+ ARR_STATE_VERT_OFF, ARR_STATE_VERTS) = range(13)
+
+# Every symbol include/hgx.h declares (the library must export all of them).
+EXPORTS = (
+    "hgx_last_error", "hgx_version", "hgx_engine_create", "hgx_engine_destroy",
+    "hgx_engine_add_rule", "hgx_engine_clear_rules", "hgx_engine_set_option", "hgx_evolve",
+    "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_step",
+    "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_device_bytes", "hgx_result_count",
+    "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times",
+)
+
+
+class HgxError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"hgx status {status}: {message}")
+        self.status = status
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("rules", ctypes.POINTER(ctypes.c_uint32)), ("rules_len", ctypes.c_size_t),
+                ("roots", ctypes.POINTER(ctypes.c_uint32)), ("roots_len", ctypes.c_size_t),
+                ("steps", ctypes.c_uint32), ("quotient", ctypes.c_uint32),
+                ("max_states", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libhgx.so (raises OSError if it is missing -- build it with build.build())."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: build the CUDA library first "
+                      "(python -m hypergraphrewritingengine_b200.build)")
+    L = ctypes.CDLL(path)
+    vp, u32p, u64p = ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)
+    sig = {
+        "hgx_last_error": ([], ctypes.c_char_p),
+        "hgx_version": ([], ctypes.c_char_p),
+        "hgx_engine_create": ([ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
+        "hgx_engine_destroy": ([vp], None),
+        "hgx_engine_add_rule": ([vp, u32p, ctypes.c_size_t], ctypes.c_int),
+        "hgx_engine_clear_rules": ([vp], ctypes.c_int),
+        "hgx_engine_set_option": ([vp, ctypes.c_int, ctypes.c_uint64], ctypes.c_int),
+        "hgx_evolve": ([vp, u32p, ctypes.c_size_t, ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
+        "hgx_evolve_batch": ([vp, ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
+        "hgx_serve_reset": ([vp], ctypes.c_int),
+        "hgx_serve_admit": ([vp, ctypes.POINTER(Job), u32p], ctypes.c_int),
+        "hgx_serve_step": ([vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "hgx_serve_take_finished": ([vp, u32p, ctypes.c_uint32, u32p], ctypes.c_int),
+        "hgx_serve_collect": ([vp, ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
+        "hgx_serve_device_bytes": ([vp, u64p], ctypes.c_int),
+        "hgx_result_count": ([vp, ctypes.c_int], ctypes.c_uint64),
+        "hgx_result_copy": ([vp, ctypes.c_int, vp, ctypes.c_size_t], ctypes.c_int),
+        "hgx_result_free": ([vp], None),
+        "hgx_engine_stage_times": ([vp, ctypes.POINTER(ctypes.c_double), u64p], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(status: int):
+    if status != HGX_OK:
+        raise HgxError(status, load_library().hgx_last_error().decode())
+
+
+def _u32p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+
+
+# ---------------------------------------------------------------------------------------------
+# Blob encodings (include/hgx.h)
+# ---------------------------------------------------------------------------------------------
+
+def encode_rule(lhs, rhs) -> np.ndarray:
+    out = []
+    for side in (lhs, rhs):
+        out.append(len(side))
+        for e in side:
+            out.append(len(e))
+            out.extend(int(v) for v in e)
+    return np.asarray(out, dtype=np.uint32)
+
+
+def encode_rules(rules) -> np.ndarray:
+    parts = [np.asarray([len(rules)], dtype=np.uint32)]
+    parts += [encode_rule(lhs, rhs) for lhs, rhs in rules]
+    return np.concatenate(parts)
+
+
+def encode_roots(roots) -> np.ndarray:
+    out = [len(roots)]
+    for st in roots:
+        out.append(len(st))
+        for e in st:
+            out.append(len(e))
+            out.extend(int(v) for v in e)
+    return np.asarray(out, dtype=np.uint32)
+
+
+# ---------------------------------------------------------------------------------------------
+# Results
+# ---------------------------------------------------------------------------------------------
+
+@dataclass
+class EvolveResult:
+    """One evolution's result (ids local to the evolution).
+
+    state_hash[s]  WL canonical hash;  state_depth[s];  events[e] = (in, out, rule, step);
+    causal[k] = (producer, consumer, edge);  branchial[k] = (a, b);  plus the consumed /
+    produced edges per event and (optionally) every state's edge record.
+    """
+
+    state_hash: np.ndarray
+    state_depth: np.ndarray
+    events: np.ndarray
+    causal: np.ndarray
+    branchial: np.ndarray
+    event_cons_off: np.ndarray
+    event_cons: np.ndarray
+    event_prod: np.ndarray
+    state_edge_off: np.ndarray
+    state_edge_ids: np.ndarray
+    state_arity: np.ndarray
+    state_vert_off: np.ndarray
+    state_verts: np.ndarray
+    num_classes: int
+    truncated: bool
+
+    @property
+    def num_states(self) -> int:
+        return len(self.state_hash)
+
+    @property
+    def num_events(self) -> int:
+        return len(self.events)
+
+    def state_edges(self, s: int):
+        """Edges (lists of vertex ids) of state s (needs keep_state_edges)."""
+        e0, e1 = self.state_edge_off[s], self.state_edge_off[s + 1]
+        v = self.state_vert_off[s]
+        out = []
+        for a in self.state_arity[e0:e1]:
+            out.append(self.state_verts[v:v + a].tolist())
+            v += a
+        return out
+
+    def bytes(self) -> int:
+        return sum(getattr(self, f).nbytes for f in (
+            "state_hash", "state_depth", "events", "causal", "branchial", "event_cons_off",
+            "event_cons", "event_prod", "state_edge_off", "state_edge_ids", "state_arity",
+            "state_vert_off", "state_verts"))
+
+
+def _read_result(handle) -> EvolveResult:
+    L = load_library()
+    cnt = lambda w: int(L.hgx_result_count(handle, w))  # noqa: E731
+    ns, ne, nc, nb = cnt(COUNT_STATES), cnt(COUNT_EVENTS), cnt(COUNT_CAUSAL), cnt(COUNT_BRANCHIAL)
+    ncons, nse, nsv = cnt(COUNT_CONSUMED), cnt(COUNT_STATE_EDGES), cnt(COUNT_STATE_VERTS)
+    has_edges = nse > 0
+    arrays = {
+        ARR_STATE_HASH: np.empty(ns, np.uint64), ARR_STATE_DEPTH: np.empty(ns, np.uint32),
+        ARR_EVENTS: np.empty((ne, 4), np.uint32), ARR_CAUSAL: np.empty((nc, 3), np.uint32),
+        ARR_BRANCHIAL: np.empty((nb, 2), np.uint32), ARR_EVENT_CONS_OFF: np.empty(ne + 1, np.uint32),
+        ARR_EVENT_CONS: np.empty(ncons, np.uint32), ARR_EVENT_PROD: np.empty((ne, 2), np.uint32),
+        ARR_STATE_EDGE_OFF: np.empty(ns + 1 if has_edges else 1, np.uint32),
+        ARR_STATE_EDGE_IDS: np.empty(nse, np.uint32), ARR_STATE_ARITY: np.empty(nse, np.uint32),
+        ARR_STATE_VERT_OFF: np.empty(ns + 1 if has_edges else 1, np.uint32),
+        ARR_STATE_VERTS: np.empty(nsv, np.uint32),
+    }
+    for what, a in arrays.items():
+        _check(L.hgx_result_copy(handle, what, a.ctypes.data_as(ctypes.c_void_p), a.nbytes))
+    return EvolveResult(
+        state_hash=arrays[ARR_STATE_HASH], state_depth=arrays[ARR_STATE_DEPTH],
+        events=arrays[ARR_EVENTS], causal=arrays[ARR_CAUSAL], branchial=arrays[ARR_BRANCHIAL],
+        event_cons_off=arrays[ARR_EVENT_CONS_OFF], event_cons=arrays[ARR_EVENT_CONS],
+        event_prod=arrays[ARR_EVENT_PROD], state_edge_off=arrays[ARR_STATE_EDGE_OFF],
+        state_edge_ids=arrays[ARR_STATE_EDGE_IDS], state_arity=arrays[ARR_STATE_ARITY],
+        state_vert_off=arrays[ARR_STATE_VERT_OFF], state_verts=arrays[ARR_STATE_VERTS],
+        num_classes=cnt(COUNT_CLASSES), truncated=bool(cnt(COUNT_TRUNCATED)))
+
+
+class Engine:
+    """A device engine (one CUDA stream and its device arrays). Reusable across calls."""
+
+    def __init__(self, device: int = 0, keep_state_edges: bool = True, causal: bool = True,
+                 branchial: bool = True, timing: bool = False):
+        L = load_library()
+        h = ctypes.c_void_p()
+        _check(L.hgx_engine_create(int(device), ctypes.byref(h)))
+        self._h = h
+        self._L = L
+        self.set_option(OPT_KEEP_STATE_EDGES, keep_state_edges)
+        self.set_option(OPT_RECORD_CAUSAL, causal)
+        self.set_option(OPT_RECORD_BRANCHIAL, branchial)
+        self.set_option(OPT_TIMING, timing)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hgx_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_option(self, opt: int, value) -> None:
+        _check(self._L.hgx_engine_set_option(self._h, int(opt), int(value)))
+
+    def evolve(self, rules, roots, steps, quotient=True, max_states=0) -> EvolveResult:
+        L = self._L
+        _check(L.hgx_engine_clear_rules(self._h))
+        for lhs, rhs in rules:
+            b = encode_rule(lhs, rhs)
+            _check(L.hgx_engine_add_rule(self._h, _u32p(b), len(b)))
+        self.set_option(OPT_QUOTIENT, quotient)
+        self.set_option(OPT_MAX_STATES, max_states)
+        rb = encode_roots(roots)
+        out = ctypes.c_void_p()
+        _check(L.hgx_evolve(self._h, _u32p(rb), len(rb), int(steps), ctypes.byref(out)))
+        try:
+            return _read_result(out)
+        finally:
+            L.hgx_result_free(out)
+
+    @staticmethod
+    def make_jobs(evolutions):
+        """ctypes job array for a list of workloads.Evolution (keeps the blobs alive)."""
+        blobs = []
+        jobs = (Job * len(evolutions))()
+        for i, ev in enumerate(evolutions):
+            rb, sb = encode_rules(ev.rules), encode_roots(ev.roots)
+            blobs += [rb, sb]
+            jobs[i] = Job(_u32p(rb), len(rb), _u32p(sb), len(sb), int(ev.steps), int(bool(ev.quotient)),
+                          int(ev.max_states))
+        return jobs, blobs
+
+    def evolve_batch(self, evolutions, jobs=None):
+        if jobs is None:
+            jobs, _keep = self.make_jobs(evolutions)
+        n = len(jobs)
+        outs = (ctypes.c_void_p * n)()
+        _check(self._L.hgx_evolve_batch(self._h, jobs, n, outs))
+        res = []
+        for i in range(n):
+            try:
+                res.append(_read_result(outs[i]))
+            finally:
+                self._L.hgx_result_free(outs[i])
+        return res
+
+    # --- serving ---
+    def serve_reset(self):
+        _check(self._L.hgx_serve_reset(self._h))
+
+    def serve_admit(self, job: Job) -> int:
+        i = ctypes.c_uint32()
+        _check(self._L.hgx_serve_admit(self._h, ctypes.byref(job), ctypes.byref(i)))
+        return int(i.value)
+
+    def serve_step(self) -> bool:
+        a = ctypes.c_int()
+        _check(self._L.hgx_serve_step(self._h, ctypes.byref(a)))
+        return bool(a.value)
+
+    def serve_take_finished(self, cap: int = 1 << 16):
+        ids = (ctypes.c_uint32 * cap)()
+        n = ctypes.c_uint32()
+        _check(self._L.hgx_serve_take_finished(self._h, ids, cap, ctypes.byref(n)))
+        return list(ids[: n.value])
+
+    def serve_collect(self, evo: int) -> EvolveResult:
+        out = ctypes.c_void_p()
+        _check(self._L.hgx_serve_collect(self._h, int(evo), ctypes.byref(out)))
+        try:
+            return _read_result(out)
+        finally:
+            self._L.hgx_result_free(out)
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_uint64()
+        _check(self._L.hgx_serve_device_bytes(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+    def stage_times(self):
+        out = (ctypes.c_double * 8)()
+        launches = ctypes.c_uint64()
+        _check(self._L.hgx_engine_stage_times(self._h, out, ctypes.byref(launches)))
+        names = ("count", "scan", "expand", "select", "materialize", "branchial", "roots", "total")
+        return dict(zip(names, list(out))), int(launches.value)
+
+
+# ---------------------------------------------------------------------------------------------
+# Reference-shaped API
+# ---------------------------------------------------------------------------------------------
+
+MAX_PATTERN_EDGES, MAX_ARITY, MAX_VARS = 16, 16, 32
+
+
+@dataclass
+class RewriteRule:
+    """A rule: LHS / RHS pattern edges over variables (pattern.hpp:71-140)."""
+
+    index: int
+    lhs: list
+    rhs: list
+
+    @property
+    def num_lhs_edges(self):
+        return len(self.lhs)
+
+    @property
+    def num_rhs_edges(self):
+        return len(self.rhs)
+
+    def new_var_mask(self) -> int:
+        lm = 0
+        rm = 0
+        for e in self.lhs:
+            for v in e:
+                lm |= 1 << v
+        for e in self.rhs:
+            for v in e:
+                rm |= 1 << v
+        return rm & ~lm
+
+
+class RuleBuilder:
+    """Fluent builder (pattern.hpp:142-206); raises ValueError where the reference throws
+    std::length_error (more than 16 edges, arity above 16, variable index >= 32)."""
+
+    def __init__(self, index: int = 0):
+        self._rule = RewriteRule(index, [], [])
+
+    def _edge(self, side, vars_):
+        vars_ = [int(v) for v in vars_]
+        if len(side) >= MAX_PATTERN_EDGES:
+            raise ValueError("RuleBuilder: exceeds MAX_PATTERN_EDGES")
+        if len(vars_) > MAX_ARITY:
+            raise ValueError("RuleBuilder: edge arity exceeds MAX_ARITY")
+        if any(v < 0 or v >= MAX_VARS for v in vars_):
+            raise ValueError("RuleBuilder: pattern variable index exceeds MAX_VARS")
+        side.append(vars_)
+        return self
+
+    def lhs(self, vars_):
+        return self._edge(self._rule.lhs, vars_)
+
+    def rhs(self, vars_):
+        return self._edge(self._rule.rhs, vars_)
+
+    def build(self) -> RewriteRule:
+        return RewriteRule(self._rule.index, [list(e) for e in self._rule.lhs],
+                           [list(e) for e in self._rule.rhs])
+
+
+def make_rule(index: int = 0) -> RuleBuilder:
+    return RuleBuilder(index)
+
+
+class CausalGraph:
+    def __init__(self, res: EvolveResult | None):
+        self._r = res
+
+    def get_causal_edges(self):
+        """(producer, consumer, edge) triples."""
+        return [] if self._r is None else [tuple(map(int, t)) for t in self._r.causal]
+
+    def get_branchial_edges(self):
+        """(event1, event2) pairs with event1 < event2."""
+        return [] if self._r is None else [tuple(map(int, t)) for t in self._r.branchial]
+
+    def num_causal_edges(self):
+        return 0 if self._r is None else len(self._r.causal)
+
+    def num_branchial_edges(self):
+        return 0 if self._r is None else len(self._r.branchial)
+
+
+class Hypergraph:
+    """Holds the evolution a ParallelEvolutionEngine produced (hypergraph.hpp:567-811)."""
+
+    def __init__(self):
+        self.result: EvolveResult | None = None
+
+    def num_states(self) -> int:
+        """Raw states: every root plus one per event (hypergraph.hpp:567)."""
+        if self.result is None:
+            return 0
+        roots = int(np.sum(self.result.state_depth == 0))
+        return roots + self.result.num_events
+
+    def num_canonical_states(self) -> int:
+        """Distinct WL canonical hashes."""
+        return 0 if self.result is None else int(self.result.num_classes)
+
+    def num_events(self) -> int:
+        return 0 if self.result is None else self.result.num_events
+
+    def get_or_compute_canonical_hash(self, sid: int) -> int:
+        return int(self.result.state_hash[sid])
+
+    def causal_graph(self) -> CausalGraph:
+        return CausalGraph(self.result)
+
+
+class ParallelEvolutionEngine:
+    """Same call sequence as the reference engine (parallel_evolution.hpp:743-1041); the
+    evolution runs on the GPU. num_threads is accepted for signature compatibility."""
+
+    def __init__(self, hg: Hypergraph, num_threads: int = 0, device: int = 0):
+        self._hg = hg
+        self._rules: list[RewriteRule] = []
+        self._quotient = False
+        self._max_states = 0
+        self._engine = Engine(device)
+
+    def add_rule(self, rule: RewriteRule):
+        self._rules.append(rule)
+
+    def set_explore_from_canonical_states_only(self, enable: bool):
+        self._quotient = bool(enable)
+
+    def set_transitive_reduction(self, enable: bool):
+        if enable:
+            raise NotImplementedError("transitive reduction is not implemented on this path")
+
+    def set_max_states(self, n: int):
+        self._max_states = int(n)
+
+    def num_states(self):
+        return self._hg.num_states()
+
+    def num_events(self):
+        return self._hg.num_events()
+
+    def num_canonical_states(self):
+        return self._hg.num_canonical_states()
+
+    def evolve(self, initial, steps: int):
+        """initial: a list of edges (one root) or a list of states (several roots)."""
+        if not self._rules:
+            return
+        roots = initial if initial and isinstance(initial[0][0], (list, tuple)) else [initial]
+        rules = [(r.lhs, r.rhs) for r in sorted(self._rules, key=lambda r: r.index)]
+        self._hg.result = self._engine.evolve(rules, roots, steps, self._quotient, self._max_states)

@@ -1,0 +1,348 @@
+// extern "C" boundary of the multiway step (declared in include/hgx.h).
+#include "../../include/hgx.h"
+
+#include <chrono>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+struct hgx_engine {
+    hgx::Engine engine;
+    std::vector<hgx::RuleSpec> rules;
+    bool quotient = false;
+    uint64_t max_states = 0;
+    hgx::RunOptions opt;
+    explicit hgx_engine(int dev) : engine(dev) {}
+};
+
+struct hgx_result {
+    hgx::EvolutionResult r;
+    std::vector<uint32_t> events_flat;   // (in, out, rule, step)
+    std::vector<uint32_t> prod_flat;     // (first, count)
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+hgx_status fail(hgx_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+template <class F>
+hgx_status guarded(F&& f) {
+    try {
+        g_err.clear();
+        return f();
+    } catch (const hgx::CudaError& e) {
+        return fail(HGX_ERR_CUDA, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(HGX_ERR_INVALID, e.what());
+    } catch (const std::length_error& e) {
+        return fail(HGX_ERR_INVALID, e.what());
+    } catch (const std::exception& e) {
+        const std::string m = e.what();
+        if (m.find("no CUDA device") != std::string::npos) return fail(HGX_ERR_NO_DEVICE, m);
+        if (m.find("capacity") != std::string::npos || m.find("exhausted") != std::string::npos)
+            return fail(HGX_ERR_CAPACITY, m);
+        return fail(HGX_ERR_INTERNAL, m);
+    } catch (...) {
+        return fail(HGX_ERR_INTERNAL, "unknown error");
+    }
+}
+
+struct Reader {
+    const uint32_t* p;
+    size_t n, i = 0;
+    uint32_t get() {
+        if (i >= n) throw std::invalid_argument("blob: truncated");
+        return p[i++];
+    }
+};
+
+std::vector<std::vector<uint8_t>> read_pattern_edges(Reader& r) {
+    const uint32_t ne = r.get();
+    if (ne > 16) throw std::length_error("rule: more than 16 pattern edges (MAX_PATTERN_EDGES)");
+    std::vector<std::vector<uint8_t>> out(ne);
+    for (auto& e : out) {
+        const uint32_t a = r.get();
+        if (a == 0 || a > 16) throw std::length_error("rule: edge arity must be 1..16 (MAX_ARITY)");
+        e.resize(a);
+        for (auto& v : e) {
+            const uint32_t x = r.get();
+            if (x >= 32) throw std::length_error("rule: pattern variable index exceeds MAX_VARS");
+            v = static_cast<uint8_t>(x);
+        }
+    }
+    return out;
+}
+
+hgx::RuleSpec read_rule(Reader& r) {
+    hgx::RuleSpec s;
+    s.lhs = read_pattern_edges(r);
+    s.rhs = read_pattern_edges(r);
+    if (s.lhs.empty()) throw std::invalid_argument("rule: empty left-hand side");
+    return s;
+}
+
+std::vector<hgx::RuleSpec> read_rules(const uint32_t* p, size_t n) {
+    Reader r{p, n};
+    const uint32_t nr = r.get();
+    std::vector<hgx::RuleSpec> out;
+    for (uint32_t i = 0; i < nr; ++i) out.push_back(read_rule(r));
+    return out;
+}
+
+std::vector<std::vector<std::vector<uint32_t>>> read_roots(const uint32_t* p, size_t n) {
+    Reader r{p, n};
+    const uint32_t nr = r.get();
+    std::vector<std::vector<std::vector<uint32_t>>> out(nr);
+    for (auto& st : out) {
+        const uint32_t ne = r.get();
+        st.resize(ne);
+        for (auto& e : st) {
+            const uint32_t a = r.get();
+            if (a == 0 || a > 16) throw std::invalid_argument("state: edge arity must be 1..16");
+            e.resize(a);
+            for (auto& v : e) v = r.get();
+        }
+    }
+    return out;
+}
+
+hgx::EvolutionSpec spec_of(const hgx_job& j) {
+    if (!j.rules || !j.roots) throw std::invalid_argument("job: null rules or roots");
+    hgx::EvolutionSpec s;
+    s.rules = read_rules(j.rules, j.rules_len);
+    s.roots = read_roots(j.roots, j.roots_len);
+    s.steps = j.steps;
+    s.quotient = j.quotient != 0;
+    s.max_states = j.max_states;
+    return s;
+}
+
+hgx_result* wrap(hgx::EvolutionResult&& r) {
+    auto* out = new hgx_result;
+    out->r = std::move(r);
+    const auto& x = out->r;
+    out->events_flat.resize(4 * x.ev_in.size());
+    out->prod_flat.resize(2 * x.ev_in.size());
+    for (size_t i = 0; i < x.ev_in.size(); ++i) {
+        out->events_flat[4 * i] = x.ev_in[i];
+        out->events_flat[4 * i + 1] = x.ev_out[i];
+        out->events_flat[4 * i + 2] = x.ev_rule[i];
+        out->events_flat[4 * i + 3] = x.ev_step[i];
+        out->prod_flat[2 * i] = x.ev_prod_first[i];
+        out->prod_flat[2 * i + 1] = x.ev_prod_count[i];
+    }
+    if (out->r.ev_cons_off.empty()) out->r.ev_cons_off.push_back(0);
+    if (out->r.state_edge_off.empty()) out->r.state_edge_off.push_back(0);
+    if (out->r.state_vert_off.empty()) out->r.state_vert_off.push_back(0);
+    return out;
+}
+
+template <class T>
+hgx_status copy_out(const std::vector<T>& v, void* dst, size_t bytes) {
+    const size_t need = v.size() * sizeof(T);
+    if (bytes < need) return fail(HGX_ERR_INVALID, "hgx_result_copy: destination too small");
+    if (need) std::memcpy(dst, v.data(), need);
+    return HGX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hgx_last_error(void) { return g_err.c_str(); }
+
+const char* hgx_version(void) { return "hgx 0.1 (sm_100a)"; }
+
+hgx_status hgx_engine_create(int device, hgx_engine** out) {
+    if (!out) return fail(HGX_ERR_INVALID, "null output pointer");
+    return guarded([&] {
+        *out = new hgx_engine(device);
+        return HGX_OK;
+    });
+}
+
+void hgx_engine_destroy(hgx_engine* e) {
+    try {
+        delete e;
+    } catch (...) {
+    }
+}
+
+hgx_status hgx_engine_add_rule(hgx_engine* e, const uint32_t* rule, size_t len) {
+    if (!e || !rule) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        Reader r{rule, len};
+        e->rules.push_back(read_rule(r));
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_engine_clear_rules(hgx_engine* e) {
+    if (!e) return fail(HGX_ERR_INVALID, "null engine");
+    e->rules.clear();
+    return HGX_OK;
+}
+
+hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) {
+    if (!e) return fail(HGX_ERR_INVALID, "null engine");
+    switch (opt) {
+        case HGX_OPT_QUOTIENT: e->quotient = value != 0; return HGX_OK;
+        case HGX_OPT_MAX_STATES: e->max_states = value; return HGX_OK;
+        case HGX_OPT_TRANSITIVE_REDUCTION:
+            if (value) return fail(HGX_ERR_INVALID, "transitive reduction is not implemented on this path");
+            return HGX_OK;
+        case HGX_OPT_RECORD_CAUSAL: e->opt.causal = value != 0; return HGX_OK;
+        case HGX_OPT_RECORD_BRANCHIAL: e->opt.branchial = value != 0; return HGX_OK;
+        case HGX_OPT_KEEP_STATE_EDGES: e->opt.keep_state_edges = value != 0; return HGX_OK;
+        case HGX_OPT_TIMING: e->engine.set_timing(value != 0); return HGX_OK;
+    }
+    return fail(HGX_ERR_INVALID, "unknown option");
+}
+
+hgx_status hgx_evolve(hgx_engine* e, const uint32_t* roots, size_t roots_len, uint32_t steps,
+                      hgx_result** out) {
+    if (!e || !roots || !out) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        if (e->rules.empty()) throw std::invalid_argument("evolve: no rules added");
+        hgx::EvolutionSpec s;
+        s.rules = e->rules;
+        s.roots = read_roots(roots, roots_len);
+        s.steps = steps;
+        s.quotient = e->quotient;
+        s.max_states = e->max_states;
+        auto res = e->engine.run({s}, e->opt);
+        *out = wrap(std::move(res[0]));
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_evolve_batch(hgx_engine* e, const hgx_job* jobs, uint32_t n, hgx_result** out) {
+    if (!e || (!jobs && n) || (!out && n)) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        std::vector<hgx::EvolutionSpec> specs;
+        specs.reserve(n);
+        for (uint32_t i = 0; i < n; ++i) specs.push_back(spec_of(jobs[i]));
+        auto res = e->engine.run(specs, e->opt);
+        for (uint32_t i = 0; i < n; ++i) out[i] = wrap(std::move(res[i]));
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_serve_reset(hgx_engine* e) {
+    if (!e) return fail(HGX_ERR_INVALID, "null engine");
+    return guarded([&] {
+        e->engine.reset();
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_serve_admit(hgx_engine* e, const hgx_job* job, uint32_t* id) {
+    if (!e || !job || !id) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        *id = e->engine.admit(spec_of(*job));
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_serve_step(hgx_engine* e, int* still_active) {
+    if (!e) return fail(HGX_ERR_INVALID, "null engine");
+    return guarded([&] {
+        const bool more = e->engine.step(e->opt);
+        if (still_active) *still_active = more ? 1 : 0;
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_serve_take_finished(hgx_engine* e, uint32_t* ids, uint32_t cap, uint32_t* n) {
+    if (!e || !n || (!ids && cap)) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        auto f = e->engine.take_finished();
+        if (f.size() > cap) throw std::invalid_argument("take_finished: id buffer too small");
+        std::memcpy(ids, f.data(), f.size() * sizeof(uint32_t));
+        *n = static_cast<uint32_t>(f.size());
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_serve_collect(hgx_engine* e, uint32_t evo, hgx_result** out) {
+    if (!e || !out) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        *out = wrap(e->engine.collect(evo, e->opt));
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_serve_device_bytes(hgx_engine* e, uint64_t* bytes) {
+    if (!e || !bytes) return fail(HGX_ERR_INVALID, "null argument");
+    *bytes = e->engine.device_bytes_in_use();
+    return HGX_OK;
+}
+
+uint64_t hgx_result_count(const hgx_result* res, hgx_count what) {
+    if (!res) return 0;
+    const auto& r = res->r;
+    switch (what) {
+        case HGX_COUNT_STATES: return r.state_hash.size();
+        case HGX_COUNT_EVENTS: return r.ev_in.size();
+        case HGX_COUNT_CLASSES: return r.num_classes;
+        case HGX_COUNT_CAUSAL: return r.causal.size() / 3;
+        case HGX_COUNT_BRANCHIAL: return r.branchial.size() / 2;
+        case HGX_COUNT_TRUNCATED: return r.truncated ? 1 : 0;
+        case HGX_COUNT_CONSUMED: return r.ev_cons.size();
+        case HGX_COUNT_STATE_EDGES: return r.state_edge_ids.size();
+        case HGX_COUNT_STATE_VERTS: return r.state_verts.size();
+        case HGX_COUNT_RAW_STATES: {
+            uint64_t roots = 0;
+            for (uint32_t ev : r.state_event) roots += (ev == 0xFFFFFFFFu) ? 1 : 0;
+            return roots + r.ev_in.size();
+        }
+    }
+    return 0;
+}
+
+hgx_status hgx_result_copy(const hgx_result* res, hgx_array what, void* dst, size_t bytes) {
+    if (!res || (!dst && bytes)) return fail(HGX_ERR_INVALID, "null argument");
+    const auto& r = res->r;
+    switch (what) {
+        case HGX_ARR_STATE_HASH: return copy_out(r.state_hash, dst, bytes);
+        case HGX_ARR_STATE_DEPTH: return copy_out(r.state_depth, dst, bytes);
+        case HGX_ARR_EVENTS: return copy_out(res->events_flat, dst, bytes);
+        case HGX_ARR_CAUSAL: return copy_out(r.causal, dst, bytes);
+        case HGX_ARR_BRANCHIAL: return copy_out(r.branchial, dst, bytes);
+        case HGX_ARR_EVENT_CONS_OFF: return copy_out(r.ev_cons_off, dst, bytes);
+        case HGX_ARR_EVENT_CONS: return copy_out(r.ev_cons, dst, bytes);
+        case HGX_ARR_EVENT_PROD: return copy_out(res->prod_flat, dst, bytes);
+        case HGX_ARR_STATE_EDGE_OFF: return copy_out(r.state_edge_off, dst, bytes);
+        case HGX_ARR_STATE_EDGE_IDS: return copy_out(r.state_edge_ids, dst, bytes);
+        case HGX_ARR_STATE_ARITY: return copy_out(r.state_arity, dst, bytes);
+        case HGX_ARR_STATE_VERT_OFF: return copy_out(r.state_vert_off, dst, bytes);
+        case HGX_ARR_STATE_VERTS: return copy_out(r.state_verts, dst, bytes);
+    }
+    return fail(HGX_ERR_INVALID, "unknown array");
+}
+
+void hgx_result_free(hgx_result* r) { delete r; }
+
+hgx_status hgx_engine_stage_times(hgx_engine* e, double* out, uint64_t* launches) {
+    if (!e || !out) return fail(HGX_ERR_INVALID, "null argument");
+    const auto& t = e->engine.times();
+    out[0] = t.count;
+    out[1] = t.scan;
+    out[2] = t.expand;
+    out[3] = t.select;
+    out[4] = t.materialize;
+    out[5] = t.branchial;
+    out[6] = t.roots;
+    out[7] = t.count + t.scan + t.expand + t.select + t.materialize + t.branchial + t.roots;
+    if (launches) *launches = t.launches;
+    return HGX_OK;
+}
+
+}  // extern "C"

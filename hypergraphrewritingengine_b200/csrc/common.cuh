@@ -1,0 +1,83 @@
+// Shared device/host definitions for the B200 multiway evolution step.
+//
+// Integer hash primitives restate common/include/hgcommon/core.hpp:47-87 of the reference
+// (FNV-1a step, splitmix64 finaliser) and the reserved empty-state hash (core.hpp:169). They
+// must agree bit for bit with the reference because every state identity is built from them.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+
+#ifdef __CUDACC__
+#define HGX_HD __host__ __device__ __forceinline__
+#else
+#define HGX_HD inline
+#endif
+
+namespace hgx {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint64_t kFnvOffset = 0xcbf29ce484222325ULL;
+constexpr uint64_t kFnvPrime = 0x100000001b3ULL;
+constexpr uint64_t kEmptyStateHash = 0x9E3779B97F4A7C15ULL;
+constexpr uint32_t kWlMaxRounds = 100;
+
+// Limits of the rule representation (the reference's MAX_PATTERN_EDGES / MAX_ARITY /
+// MAX_VARS, common/include/hgcommon/core.hpp:42-44).
+constexpr int kMaxPatternEdges = 16;
+constexpr int kMaxArity = 16;
+constexpr int kMaxVars = 32;
+constexpr int kMaxSideVars = 64;   // total positions over one rule side (16 edges x 4 avg)
+
+HGX_HD uint64_t fnv(uint64_t h, uint64_t x) { return (h ^ x) * kFnvPrime; }
+
+HGX_HD uint64_t smix(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+// A rewrite rule as the kernels read it: one fixed-size record, copied to shared memory by
+// the warp that applies it. `sched` is the binding order of the LHS positions; matches are
+// enumerated in lexicographic order of their edges' state positions taken in that order.
+struct DevRule {
+    uint8_t n_lhs, n_rhs, n_fresh, lhs_total, rhs_total;
+    uint8_t pad[3];
+    uint32_t new_mask;       // variables that occur only on the RHS
+    uint8_t lhs_ar[kMaxPatternEdges], lhs_off[kMaxPatternEdges];
+    uint8_t rhs_ar[kMaxPatternEdges], rhs_off[kMaxPatternEdges];
+    uint8_t sched[kMaxPatternEdges];
+    uint8_t fresh_rank[kMaxVars];   // n-th fresh variable -> n (ascending variable order)
+    uint8_t lhs_vars[kMaxSideVars];
+    uint8_t rhs_vars[kMaxSideVars];
+};
+static_assert(sizeof(DevRule) % 4 == 0, "rule record must be word aligned");
+
+// Per-evolution bookkeeping the kernels read.
+struct DevEvo {
+    uint32_t rule_begin;     // first rule of this evolution in the rule table
+    uint32_t rule_count;
+    uint32_t steps;          // expansion budget: states at depth < steps are expanded
+    uint32_t quotient;       // 1 = expand each WL class once (at its shortest depth)
+    uint64_t table_off;      // slot offset of this evolution's dedup table
+    uint64_t table_mask;     // capacity - 1 (power of two); slot mask+1 holds key 0
+    uint64_t max_states;     // 0 = unlimited
+};
+
+// Device-side error channel (typed, host-visible; never a trap).
+enum ErrorBits : uint32_t {
+    kErrTableFull = 1u << 0,
+    kErrStateTooLarge = 1u << 1,
+    kErrArenaFull = 1u << 2,
+    kErrBadRule = 1u << 3,
+};
+
+}  // namespace hgx
+
+#define HGX_CUDA_CHECK(expr)                                                                 \
+    do {                                                                                     \
+        cudaError_t _e = (expr);                                                             \
+        if (_e != cudaSuccess) {                                                             \
+            throw ::hgx::CudaError(_e, #expr, __FILE__, __LINE__);                           \
+        }                                                                                    \
+    } while (0)

@@ -1,0 +1,987 @@
+// Host side of the B200 multiway evolution step: device memory, the per-level launch sequence,
+// admission of evolutions and result readback. Kernels live in step_kernels.cu (same
+// translation unit, so launches need no separate device linking).
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "step_kernels.cu"
+
+namespace hgx {
+
+namespace {
+
+constexpr int kNumSMs = 148;
+constexpr size_t kMaxDynSmem = 227 * 1024;
+
+uint64_t next_pow2(uint64_t x) {
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+template <class T>
+struct DVec {
+    T* p = nullptr;
+    size_t cap = 0;
+    // Grow to hold n elements, preserving the first `keep`.
+    void ensure(size_t n, size_t keep, cudaStream_t s) {
+        if (n <= cap) return;
+        size_t nc = std::max<size_t>(n, cap + cap / 2 + 1024);
+        T* np = nullptr;
+        HGX_CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&np), nc * sizeof(T), s));
+        if (p && keep)
+            HGX_CUDA_CHECK(cudaMemcpyAsync(np, p, std::min(keep, cap) * sizeof(T),
+                                           cudaMemcpyDeviceToDevice, s));
+        if (p) HGX_CUDA_CHECK(cudaFreeAsync(p, s));
+        p = np;
+        cap = nc;
+    }
+    void release(cudaStream_t s) {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        cap = 0;
+    }
+    size_t bytes() const { return cap * sizeof(T); }
+};
+
+struct RuleMax {
+    uint32_t rhs = 0, rhs_total = 0, fresh = 0, arity = 1, grow_e = 0, grow_o = 0, stride = 1;
+};
+
+DevRule pack_rule(const RuleSpec& r) {
+    DevRule d;
+    std::memset(&d, 0, sizeof(d));
+    if (r.lhs.empty() || r.lhs.size() > kMaxPatternEdges || r.rhs.size() > kMaxPatternEdges)
+        throw std::invalid_argument("rule: LHS must have 1..16 edges and RHS at most 16");
+    uint32_t lhs_mask = 0, rhs_mask = 0, off = 0;
+    d.n_lhs = static_cast<uint8_t>(r.lhs.size());
+    d.n_rhs = static_cast<uint8_t>(r.rhs.size());
+    for (size_t i = 0; i < r.lhs.size(); ++i) {
+        const auto& e = r.lhs[i];
+        if (e.empty() || e.size() > kMaxArity) throw std::invalid_argument("rule: LHS edge arity must be 1..16");
+        d.lhs_ar[i] = static_cast<uint8_t>(e.size());
+        d.lhs_off[i] = static_cast<uint8_t>(off);
+        for (uint8_t v : e) {
+            if (v >= kMaxVars) throw std::invalid_argument("rule: pattern variable must be < 32");
+            if (off >= kMaxSideVars) throw std::invalid_argument("rule: LHS has more than 64 positions");
+            d.lhs_vars[off++] = v;
+            lhs_mask |= 1u << v;
+        }
+    }
+    d.lhs_total = static_cast<uint8_t>(off);
+    off = 0;
+    for (size_t i = 0; i < r.rhs.size(); ++i) {
+        const auto& e = r.rhs[i];
+        if (e.empty() || e.size() > kMaxArity) throw std::invalid_argument("rule: RHS edge arity must be 1..16");
+        d.rhs_ar[i] = static_cast<uint8_t>(e.size());
+        d.rhs_off[i] = static_cast<uint8_t>(off);
+        for (uint8_t v : e) {
+            if (v >= kMaxVars) throw std::invalid_argument("rule: pattern variable must be < 32");
+            if (off >= kMaxSideVars) throw std::invalid_argument("rule: RHS has more than 64 positions");
+            d.rhs_vars[off++] = v;
+            rhs_mask |= 1u << v;
+        }
+    }
+    d.rhs_total = static_cast<uint8_t>(off);
+    d.new_mask = rhs_mask & ~lhs_mask;
+    uint32_t rank = 0;
+    for (uint32_t v = 0; v < kMaxVars; ++v)
+        if ((d.new_mask >> v) & 1u) d.fresh_rank[v] = static_cast<uint8_t>(rank++);
+    d.n_fresh = static_cast<uint8_t>(rank);
+    // Binding schedule: position 0, then the lowest-index position sharing a variable with
+    // those already scheduled (else the lowest unscheduled). Fixes the canonical event order.
+    std::vector<bool> used(d.n_lhs, false);
+    uint32_t bound = 0;
+    for (uint32_t s = 0; s < d.n_lhs; ++s) {
+        int pick = -1;
+        for (uint32_t i = 0; i < d.n_lhs && pick < 0; ++i) {
+            if (used[i]) continue;
+            uint32_t m = 0;
+            for (uint32_t q = 0; q < d.lhs_ar[i]; ++q) m |= 1u << d.lhs_vars[d.lhs_off[i] + q];
+            if (s == 0 || (m & bound)) pick = static_cast<int>(i);
+        }
+        if (pick < 0)
+            for (uint32_t i = 0; i < d.n_lhs; ++i)
+                if (!used[i]) { pick = static_cast<int>(i); break; }
+        used[pick] = true;
+        for (uint32_t q = 0; q < d.lhs_ar[pick]; ++q) bound |= 1u << d.lhs_vars[d.lhs_off[pick] + q];
+        d.sched[s] = static_cast<uint8_t>(pick);
+    }
+    return d;
+}
+
+uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, bool wl) {
+    Layout L;
+    std::memset(&L, 0, sizeof(L));
+    NE = std::max<uint32_t>(NE, 1);
+    NOCC = std::max<uint32_t>(NOCC, 1);
+    L.NE = NE;
+    L.NOCC = NOCC;
+    L.CNE = NE + rm.rhs;
+    L.CNOCC = NOCC + rm.rhs_total;
+    L.V = NOCC + rm.fresh;
+    L.W = (NE + 31) / 32;
+    L.NBR = wl ? L.CNOCC * rm.arity : 0;
+    uint32_t off = 0;
+    auto take = [&](uint32_t bytes, uint32_t align) {
+        off = align_up(off, align);
+        const uint32_t o = off;
+        off += bytes;
+        return o;
+    };
+    if (wl) {
+        L.o_cur = take(8 * L.V, 8);
+        L.o_nxt = take(8 * L.V, 8);
+        L.o_csum = take(8 * L.V, 8);
+        L.o_ccnt = take(8 * L.V, 8);
+        L.o_nbr = take(8 * L.NBR, 8);
+    }
+    L.o_peid = take(4 * NE, 4);
+    L.o_occ = take(4 * (wl ? L.CNOCC : NOCC), 4);
+    L.o_deg = take(4 * (wl ? L.V : NOCC), 4);
+    if (wl) {
+        L.o_ooff = take(4 * (L.V + 1), 4);
+        L.o_nbo = take(4 * (L.V + 1), 4);
+        L.o_nn = take(4 * L.V, 4);
+        L.o_comp = take(4 * L.V, 4);
+    }
+    L.o_cand = take(4 * kMaxPatternEdges * L.W, 4);
+    L.o_taken = take(4 * L.W, 4);
+    L.o_misc = take(4 * kMaxPatternEdges, 4);
+    L.o_pevo = take(2 * NE, 2);
+    L.o_vloc = take(2 * (NOCC + rm.rhs_total), 2);
+    if (wl) L.o_cvo = take(2 * L.CNE, 2);
+    L.o_bind = take(2 * kMaxVars, 2);
+    L.o_match = take(2 * kMaxPatternEdges, 2);
+    L.o_mdepth = take(2 * kMaxPatternEdges, 2);
+    L.o_pear = take(NE, 1);
+    if (wl) L.o_car = take(L.CNE, 1);
+    L.o_rule = take(sizeof(DevRule), 4);
+    L.bytes = align_up(off, 16);
+    return L;
+}
+
+struct LaunchShape {
+    uint32_t grid, block, smem;
+};
+
+}  // namespace
+
+// ==========================================================================================
+
+struct Engine::Impl {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    bool timing = false;
+    StageTimes times;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+
+    // device arrays
+    DVec<DevRule> rules;
+    DVec<DevEvo> evos;
+    DVec<uint64_t> st_off, st_hash;
+    DVec<uint32_t> st_ne, st_nocc, st_evo, st_depth, st_event;
+    DVec<uint32_t> arena;
+    DVec<unsigned long long> arena_top;
+    DVec<uint32_t> edge_creator;
+    DVec<uint32_t> ev_in, ev_rule, ev_coff, ev_prod, ev_fresh, ev_out, ev_cons, ev_cprod;
+    DVec<uint8_t> ev_kept;
+    DVec<uint64_t> ev_hash;
+    DVec<uint32_t> state_of_arrival;
+    DVec<unsigned long long> tab_keys;
+    DVec<uint32_t> tab_vals;
+    DVec<unsigned long long> evo_classes, evo_states;
+    DVec<uint32_t> evo_cut, evo_first_ev, evo_last_ev, evo_stopped, evo_front;
+    DVec<uint32_t> err;
+    // level temporaries
+    DVec<uint32_t> frontier, next_frontier, counts, item_ev, item_cons, item_prod, item_fresh;
+    DVec<uint32_t> work, flag_new, scan_new, flag_rep, flag_front, new_state_event, level_max;
+    DVec<uint32_t> bcount, boff, bpairs, scan_sums, sync_buf, root_ids;
+
+    // host mirrors
+    std::vector<DevRule> h_rules;
+    std::vector<DevEvo> h_evos;
+    std::vector<uint8_t> evo_done, evo_reported;
+    std::vector<uint32_t> finished;
+    RuleMax rm;
+    uint64_t n_states = 0, n_edges = 0, n_events = 0, n_cons = 0, n_bpairs = 0;
+    uint64_t next_vertex = 0, arena_words = 0, tab_slots = 0;
+    uint32_t frontier_size = 0;
+    uint32_t ne_bound = 1, nocc_bound = 1;
+    uint64_t launches = 0;
+
+    explicit Impl(int dev) : device(dev) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n <= dev)
+            throw std::runtime_error("hgx: no CUDA device available (the step has no CPU fallback)");
+        HGX_CUDA_CHECK(cudaSetDevice(device));
+        HGX_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        HGX_CUDA_CHECK(cudaEventCreate(&ev_a));
+        HGX_CUDA_CHECK(cudaEventCreate(&ev_b));
+        cudaMemPool_t pool;
+        HGX_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        for (const void* k : {(const void*)k_count, (const void*)k_expand, (const void*)k_roots})
+            HGX_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                static_cast<int>(kMaxDynSmem)));
+        arena_top.ensure(1, 0, st);
+        err.ensure(1, 0, st);
+        work.ensure(8, 0, st);
+        level_max.ensure(4, 0, st);
+        sync_buf.ensure(16, 0, st);
+        reset();
+    }
+
+    ~Impl() {
+        cudaSetDevice(device);
+        cudaStreamSynchronize(st);
+        for (auto* v : std::initializer_list<DVec<uint32_t>*>{
+                 &st_ne, &st_nocc, &st_evo, &st_depth, &st_event, &arena, &edge_creator, &ev_in,
+                 &ev_rule, &ev_coff, &ev_prod, &ev_fresh, &ev_out, &ev_cons, &ev_cprod,
+                 &state_of_arrival, &tab_vals, &evo_cut, &evo_first_ev, &evo_last_ev,
+                 &evo_stopped, &evo_front, &err, &frontier, &next_frontier, &counts, &item_ev,
+                 &item_cons, &item_prod, &item_fresh, &work, &flag_new, &scan_new, &flag_rep,
+                 &flag_front, &new_state_event, &level_max, &bcount, &boff, &bpairs, &scan_sums,
+                 &sync_buf, &root_ids})
+            v->release(st);
+        st_off.release(st);
+        st_hash.release(st);
+        ev_hash.release(st);
+        ev_kept.release(st);
+        arena_top.release(st);
+        tab_keys.release(st);
+        evo_classes.release(st);
+        evo_states.release(st);
+        rules.release(st);
+        evos.release(st);
+        cudaStreamSynchronize(st);
+        cudaEventDestroy(ev_a);
+        cudaEventDestroy(ev_b);
+        cudaStreamDestroy(st);
+    }
+
+    void reset() {
+        h_rules.clear();
+        h_evos.clear();
+        evo_done.clear();
+        evo_reported.clear();
+        finished.clear();
+        rm = RuleMax{};
+        n_states = n_edges = n_events = n_cons = n_bpairs = 0;
+        next_vertex = arena_words = tab_slots = 0;
+        frontier_size = 0;
+        ne_bound = nocc_bound = 1;
+        HGX_CUDA_CHECK(cudaMemsetAsync(arena_top.p, 0, sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
+        times = StageTimes{};
+        launches = 0;
+    }
+
+    DevPtrs ptrs() const {
+        DevPtrs P;
+        P.rules = rules.p;
+        P.evos = evos.p;
+        P.st_off = st_off.p;
+        P.st_ne = st_ne.p;
+        P.st_nocc = st_nocc.p;
+        P.st_evo = st_evo.p;
+        P.st_depth = st_depth.p;
+        P.st_event = st_event.p;
+        P.st_hash = st_hash.p;
+        P.arena = arena.p;
+        P.arena_top = arena_top.p;
+        P.arena_cap = arena.cap;
+        P.edge_creator = edge_creator.p;
+        P.ev_in = ev_in.p;
+        P.ev_rule = ev_rule.p;
+        P.ev_coff = ev_coff.p;
+        P.ev_prod = ev_prod.p;
+        P.ev_fresh = ev_fresh.p;
+        P.ev_out = ev_out.p;
+        P.ev_kept = ev_kept.p;
+        P.ev_hash = ev_hash.p;
+        P.ev_cons = ev_cons.p;
+        P.ev_cprod = ev_cprod.p;
+        P.state_of_arrival = state_of_arrival.p;
+        P.tab_keys = tab_keys.p;
+        P.tab_vals = tab_vals.p;
+        P.evo_classes = evo_classes.p;
+        P.evo_states = evo_states.p;
+        P.evo_cut = evo_cut.p;
+        P.evo_first_ev = evo_first_ev.p;
+        P.evo_stopped = evo_stopped.p;
+        P.err = err.p;
+        return P;
+    }
+
+    // ---- small helpers ------------------------------------------------------------------
+    void tic() {
+        if (timing) HGX_CUDA_CHECK(cudaEventRecord(ev_a, st));
+    }
+    void toc(double& acc) {
+        if (!timing) return;
+        HGX_CUDA_CHECK(cudaEventRecord(ev_b, st));
+        HGX_CUDA_CHECK(cudaEventSynchronize(ev_b));
+        float ms = 0;
+        HGX_CUDA_CHECK(cudaEventElapsedTime(&ms, ev_a, ev_b));
+        acc += ms;
+    }
+    void check_launch() {
+        ++launches;
+        HGX_CUDA_CHECK(cudaGetLastError());
+    }
+
+    static uint32_t grid_for(uint64_t n, uint32_t block) {
+        const uint64_t g = (n + block - 1) / block;
+        return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(g, kNumSMs * 16)));
+    }
+
+    template <class K>
+    LaunchShape warp_shape(K kernel, const Layout& L, uint64_t items) {
+        if (L.bytes > kMaxDynSmem)
+            throw std::runtime_error("hgx: a state exceeds the per-warp shared-memory capacity (" +
+                                     std::to_string(L.bytes) + " bytes needed)");
+        uint32_t wpb = static_cast<uint32_t>(std::min<size_t>(8, std::max<size_t>(1, (96 * 1024) / L.bytes)));
+        LaunchShape s;
+        s.block = 32 * wpb;
+        s.smem = L.bytes * wpb;
+        int bps = 0;
+        HGX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, s.block, s.smem));
+        bps = std::max(bps, 1);
+        const uint64_t want = (items + wpb - 1) / wpb;
+        s.grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(want, uint64_t(kNumSMs) * bps)));
+        return s;
+    }
+
+    void scan(const uint32_t* in, uint32_t* out, uint32_t n) {
+        if (n == 0) {
+            HGX_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(uint32_t), st));
+            return;
+        }
+        const uint32_t nb = (n + kScanTile - 1) / kScanTile;
+        scan_sums.ensure(nb + 1, 0, st);
+        k_scan_reduce<<<nb, kScanThreads, 0, st>>>(in, n, scan_sums.p);
+        check_launch();
+        k_scan_sums<<<1, kScanThreads, 0, st>>>(scan_sums.p, nb);
+        check_launch();
+        k_scan_down<<<nb, kScanThreads, 0, st>>>(in, out, n, scan_sums.p, nb);
+        check_launch();
+    }
+
+    // ---- admission ------------------------------------------------------------------------
+    uint32_t admit(const EvolutionSpec& spec) {
+        if (spec.rules.empty()) throw std::invalid_argument("evolve: no rules");
+        if (spec.roots.empty()) throw std::invalid_argument("evolve: no initial state");
+        const uint32_t evo = static_cast<uint32_t>(h_evos.size());
+        DevEvo d;
+        std::memset(&d, 0, sizeof(d));
+        d.rule_begin = static_cast<uint32_t>(h_rules.size());
+        d.rule_count = static_cast<uint32_t>(spec.rules.size());
+        d.steps = spec.steps;
+        d.quotient = spec.quotient ? 1u : 0u;
+        d.max_states = spec.max_states;
+        for (const auto& r : spec.rules) {
+            DevRule pr = pack_rule(r);
+            h_rules.push_back(pr);
+            rm.rhs = std::max<uint32_t>(rm.rhs, pr.n_rhs);
+            rm.rhs_total = std::max<uint32_t>(rm.rhs_total, pr.rhs_total);
+            rm.fresh = std::max<uint32_t>(rm.fresh, pr.n_fresh);
+            for (uint32_t i = 0; i < pr.n_rhs; ++i) rm.arity = std::max<uint32_t>(rm.arity, pr.rhs_ar[i]);
+            rm.grow_e = std::max<int>(rm.grow_e, int(pr.n_rhs) - int(pr.n_lhs));
+            rm.grow_o = std::max<int>(rm.grow_o, int(pr.rhs_total) - int(pr.lhs_total));
+        }
+        rm.stride = std::max<uint32_t>(rm.stride, d.rule_count);
+
+        // roots: edge records, uploaded to the arena
+        std::vector<uint32_t> words;
+        std::vector<uint64_t> offs;
+        std::vector<uint32_t> nes, noccs;
+        uint64_t max_label = 0;
+        for (const auto& root : spec.roots) {
+            const uint32_t ne = static_cast<uint32_t>(root.size());
+            uint32_t nocc = 0;
+            for (const auto& e : root) {
+                if (e.empty() || e.size() > kMaxArity)
+                    throw std::invalid_argument("evolve: initial edge arity must be 1..16");
+                nocc += static_cast<uint32_t>(e.size());
+                rm.arity = std::max<uint32_t>(rm.arity, static_cast<uint32_t>(e.size()));
+                for (uint32_t v : e) max_label = std::max<uint64_t>(max_label, v);
+            }
+            if (ne == 0) throw std::invalid_argument("evolve: an initial state has no edges");
+            offs.push_back(arena_words + words.size());
+            nes.push_back(ne);
+            noccs.push_back(nocc);
+            const uint32_t aw = (ne + 3) / 4;
+            const size_t base = words.size();
+            words.resize(base + ne + aw + nocc, 0);
+            uint32_t vo = 0;
+            for (uint32_t i = 0; i < ne; ++i) {
+                words[base + i] = static_cast<uint32_t>(n_edges + i);
+                words[base + ne + i / 4] |= static_cast<uint32_t>(root[i].size()) << ((i % 4) * 8);
+                for (uint32_t v : root[i]) words[base + ne + aw + vo++] = v;
+            }
+            n_edges += ne;
+            ne_bound = std::max(ne_bound, ne);
+            nocc_bound = std::max(nocc_bound, nocc);
+        }
+        next_vertex = std::max<uint64_t>(next_vertex, max_label + 1);
+        const uint32_t nr = static_cast<uint32_t>(spec.roots.size());
+
+        // dedup table region
+        const uint64_t cap = next_pow2(std::max<uint64_t>(256, 4ull * nr));
+        d.table_off = tab_slots;
+        d.table_mask = cap - 1;
+        const uint64_t new_slots = tab_slots + cap + 1;
+        tab_keys.ensure(new_slots, tab_slots, st);
+        tab_vals.ensure(new_slots, tab_slots, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_keys.p + tab_slots, 0, (cap + 1) * sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_vals.p + tab_slots, 0xFF, (cap + 1) * sizeof(uint32_t), st));
+        tab_slots = new_slots;
+
+        h_evos.push_back(d);
+        evo_done.push_back(0);
+        evo_reported.push_back(0);
+        const size_t nevo = h_evos.size();
+        // per-evolution device arrays
+        rules.ensure(h_rules.size(), h_rules.size() - spec.rules.size(), st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(rules.p + d.rule_begin, h_rules.data() + d.rule_begin,
+                                       spec.rules.size() * sizeof(DevRule), cudaMemcpyHostToDevice, st));
+        evos.ensure(nevo, nevo - 1, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + evo, &h_evos[evo], sizeof(DevEvo), cudaMemcpyHostToDevice, st));
+        evo_classes.ensure(nevo, nevo - 1, st);
+        evo_states.ensure(nevo, nevo - 1, st);
+        evo_cut.ensure(nevo, nevo - 1, st);
+        evo_first_ev.ensure(nevo, nevo - 1, st);
+        evo_last_ev.ensure(nevo, nevo - 1, st);
+        evo_stopped.ensure(nevo, nevo - 1, st);
+        evo_front.ensure(nevo, nevo - 1, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_classes.p + evo, 0, sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_states.p + evo, 0, sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_cut.p + evo, 0xFF, sizeof(uint32_t), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_stopped.p + evo, 0, sizeof(uint32_t), st));
+
+        // arena
+        arena.ensure(arena_words + words.size(), arena_words, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(arena.p + arena_words, words.data(), words.size() * 4,
+                                       cudaMemcpyHostToDevice, st));
+        arena_words += words.size();
+        const unsigned long long top = arena_words;
+        HGX_CUDA_CHECK(cudaMemcpyAsync(arena_top.p, &top, sizeof(top), cudaMemcpyHostToDevice, st));
+        // initial edges have no producer
+        uint64_t total_root_edges = 0;
+        for (uint32_t ne : nes) total_root_edges += ne;
+        const uint64_t e0 = n_edges - total_root_edges;
+        edge_creator.ensure(n_edges, e0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(edge_creator.p + e0, 0xFF, total_root_edges * sizeof(uint32_t), st));
+
+        // states and root pseudo-events
+        const uint64_t s0 = n_states, a0 = n_events;
+        grow_states(n_states + nr);
+        grow_events(n_events + nr);
+        std::vector<uint32_t> h_evo(nr, evo), h_zero(nr, 0), h_ev(nr), h_sid(nr), h_none(nr, kNone);
+        std::vector<uint8_t> h_kept(nr, 0);
+        for (uint32_t i = 0; i < nr; ++i) { h_ev[i] = static_cast<uint32_t>(a0 + i); h_sid[i] = static_cast<uint32_t>(s0 + i); }
+        auto up = [&](auto* dst, const auto& src) {
+            HGX_CUDA_CHECK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(src[0]), cudaMemcpyHostToDevice, st));
+        };
+        up(st_off.p + s0, offs);
+        up(st_ne.p + s0, nes);
+        up(st_nocc.p + s0, noccs);
+        up(st_evo.p + s0, h_evo);
+        up(st_depth.p + s0, h_zero);
+        up(st_event.p + s0, h_ev);
+        up(ev_in.p + a0, h_none);
+        up(ev_out.p + a0, h_sid);
+        up(ev_kept.p + a0, h_kept);
+        up(state_of_arrival.p + a0, h_sid);
+        n_states += nr;
+        n_events += nr;
+
+        // hash the roots on the device and seed the table
+        root_ids.ensure(nr, 0, st);
+        up(root_ids.p, h_sid);
+        RuleMax none;
+        none.arity = rm.arity;
+        uint32_t mne = *std::max_element(nes.begin(), nes.end());
+        uint32_t mno = *std::max_element(noccs.begin(), noccs.end());
+        Layout L = make_layout(mne, mno, none, true);
+        HGX_CUDA_CHECK(cudaMemsetAsync(work.p, 0, 8 * sizeof(uint32_t), st));
+        LaunchShape s = warp_shape(k_roots, L, nr);
+        tic();
+        k_roots<<<s.grid, s.block, s.smem, st>>>(ptrs(), root_ids.p, nr, work.p, L);
+        check_launch();
+        k_root_counts<<<grid_for(nr, 256), 256, 0, st>>>(ptrs(), root_ids.p, nr);
+        check_launch();
+        toc(times.roots);
+
+        if (spec.steps > 0) {
+            frontier.ensure(frontier_size + nr, frontier_size, st);
+            up(frontier.p + frontier_size, h_sid);
+            frontier_size += nr;
+        } else {
+            evo_done[evo] = 1;
+            finished.push_back(evo);
+        }
+        return evo;
+    }
+
+    void grow_states(uint64_t n) {
+        const uint64_t k = n_states;
+        st_off.ensure(n, k, st);
+        st_hash.ensure(n, k, st);
+        st_ne.ensure(n, k, st);
+        st_nocc.ensure(n, k, st);
+        st_evo.ensure(n, k, st);
+        st_depth.ensure(n, k, st);
+        st_event.ensure(n, k, st);
+    }
+
+    void grow_events(uint64_t n) {
+        const uint64_t k = n_events;
+        ev_in.ensure(n, k, st);
+        ev_rule.ensure(n, k, st);
+        ev_coff.ensure(n, k, st);
+        ev_prod.ensure(n, k, st);
+        ev_fresh.ensure(n, k, st);
+        ev_out.ensure(n, k, st);
+        ev_kept.ensure(n, k, st);
+        ev_hash.ensure(n, k, st);
+        state_of_arrival.ensure(n, k, st);
+    }
+
+    // Rebuild an evolution's dedup table at a larger capacity.
+    void regrow_table(uint32_t evo, uint64_t need) {
+        DevEvo& d = h_evos[evo];
+        const uint64_t cap = next_pow2(std::max<uint64_t>(need * 2, (d.table_mask + 1) * 2));
+        const uint64_t off = tab_slots;
+        const uint64_t new_slots = tab_slots + cap + 1;
+        tab_keys.ensure(new_slots, tab_slots, st);
+        tab_vals.ensure(new_slots, tab_slots, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_keys.p + off, 0, (cap + 1) * sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_vals.p + off, 0xFF, (cap + 1) * sizeof(uint32_t), st));
+        tab_slots = new_slots;
+        DevEvo nd = d;
+        nd.table_off = off;
+        nd.table_mask = cap - 1;
+        const uint64_t old_n = d.table_mask + 2;
+        k_rehash<<<grid_for(old_n, 256), 256, 0, st>>>(tab_keys.p, tab_vals.p, d.table_off, d.table_mask, nd.table_off, nd.table_mask, err.p);
+        check_launch();
+        d = nd;
+        HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + evo, &d, sizeof(DevEvo), cudaMemcpyHostToDevice, st));
+    }
+
+    void read_results(const std::vector<uint32_t>& which, const RunOptions& opt,
+                      std::vector<EvolutionResult>& out);
+
+    // ---- one level for every evolution in the frontier ---------------------------------------
+    bool level(const RunOptions& opt) {
+        const uint32_t F = frontier_size;
+        if (F == 0) return false;
+        const uint32_t R = rm.stride;
+        const uint64_t items = uint64_t(F) * R;
+        if (items + 1 > 0xFFFFFFFFull) throw std::runtime_error("hgx: frontier too large for one level");
+        const uint32_t NI = static_cast<uint32_t>(items);
+        counts.ensure(NI, 0, st);
+        item_ev.ensure(NI + 1, 0, st);
+        item_cons.ensure(NI + 1, 0, st);
+        item_prod.ensure(NI + 1, 0, st);
+        item_fresh.ensure(NI + 1, 0, st);
+        bcount.ensure(F, 0, st);
+        boff.ensure(F + 1, 0, st);
+
+        LevelArgs A;
+        std::memset(&A, 0, sizeof(A));
+        A.frontier = frontier.p;
+        A.n_frontier = F;
+        A.rules_stride = R;
+        A.counts = counts.p;
+        A.item_ev = item_ev.p;
+        A.item_cons = item_cons.p;
+        A.item_prod = item_prod.p;
+        A.item_fresh = item_fresh.p;
+        A.work = work.p;
+        A.level_max = level_max.p;
+        A.bcount = bcount.p;
+        A.boff = boff.p;
+        A.ev_base = static_cast<uint32_t>(n_events);
+        A.cons_base = static_cast<uint32_t>(n_cons);
+        A.prod_base = static_cast<uint32_t>(n_edges);
+        A.fresh_base = static_cast<uint32_t>(next_vertex);
+
+        HGX_CUDA_CHECK(cudaMemsetAsync(work.p, 0, 8 * sizeof(uint32_t), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(level_max.p, 0, 4 * sizeof(uint32_t), st));
+
+        // ---- count
+        const Layout Lc = make_layout(ne_bound, nocc_bound, rm, false);
+        LaunchShape sc = warp_shape(k_count, Lc, F);
+        tic();
+        k_count<<<sc.grid, sc.block, sc.smem, st>>>(ptrs(), A, Lc);
+        check_launch();
+        k_frontier_max<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A);
+        check_launch();
+        toc(times.count);
+
+        // ---- scans of the per-item sizes
+        tic();
+        k_item_sizes<<<grid_for(NI, 256), 256, 0, st>>>(ptrs(), A);
+        check_launch();
+        scan(item_ev.p, item_ev.p, NI);
+        scan(item_cons.p, item_cons.p, NI);
+        scan(item_prod.p, item_prod.p, NI);
+        scan(item_fresh.p, item_fresh.p, NI);
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_first_ev.p, 0xFF, h_evos.size() * 4, st));
+        k_evo_first<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p);
+        check_launch();
+        toc(times.scan);
+
+        // ---- sync 1: level totals, per-evolution event ranges, exact frontier maxima
+        uint32_t tot[6];
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[0], item_ev.p + NI, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[1], item_cons.p + NI, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[2], item_prod.p + NI, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[3], item_fresh.p + NI, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[4], level_max.p + 2, 8, cudaMemcpyDeviceToHost, st));
+        const size_t nevo = h_evos.size();
+        std::vector<uint32_t> h_first(nevo), h_last(nevo);
+        std::vector<unsigned long long> h_classes(nevo);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(h_first.data(), evo_first_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(h_last.data(), evo_last_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(h_classes.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        const uint32_t n_ev = tot[0], n_cons_lv = tot[1], n_prod = tot[2], n_fresh = tot[3];
+        const uint32_t fmax_ne = tot[4], fmax_nocc = tot[5];
+        if (uint64_t(n_events) + n_ev >= 0xFFFFFFF0ull || uint64_t(n_edges) + n_prod >= 0xFFFFFFF0ull ||
+            uint64_t(next_vertex) + n_fresh >= 0xFFFFFFF0ull || uint64_t(n_cons) + n_cons_lv >= 0xFFFFFFF0ull)
+            throw std::runtime_error("hgx: 32-bit id space exhausted (events, edges or vertices)");
+        A.n_events = n_ev;
+
+        // capacity
+        grow_events(n_events + n_ev);
+        ev_cons.ensure(n_cons + n_cons_lv, n_cons, st);
+        ev_cprod.ensure(n_cons + n_cons_lv, n_cons, st);
+        edge_creator.ensure(n_edges + n_prod, n_edges, st);
+        flag_new.ensure(n_ev + 1, 0, st);
+        scan_new.ensure(n_ev + 1, 0, st);
+        flag_rep.ensure(n_ev + 1, 0, st);
+        flag_front.ensure(n_ev + 1, 0, st);
+        A.flag_new = flag_new.p;
+        A.scan_new = scan_new.p;
+        A.flag_rep = flag_rep.p;
+        A.flag_front = flag_front.p;
+        // tables: room for every event of the level plus every class seen
+        bool any_cap = false;
+        for (size_t e = 0; e < nevo; ++e) {
+            if (evo_done[e] || h_first[e] == kNone) continue;
+            if (h_evos[e].max_states) any_cap = true;
+            const uint64_t lv = (h_last[e] >= h_first[e]) ? h_last[e] - h_first[e] : 0;
+            const uint64_t need = h_classes[e] + lv + 1;
+            if (2 * need > h_evos[e].table_mask + 1) regrow_table(static_cast<uint32_t>(e), need);
+        }
+
+        // ---- expand: events, produced edges, children's WL hashes, table inserts
+        if (n_ev) {
+            const Layout Le = make_layout(std::max<uint32_t>(fmax_ne, 1), std::max<uint32_t>(fmax_nocc, 1), rm, true);
+            LaunchShape se = warp_shape(k_expand, Le, F);
+            tic();
+            k_expand<<<se.grid, se.block, se.smem, st>>>(ptrs(), A, Le);
+            check_launch();
+            toc(times.expand);
+            ++times.expand_launches;
+
+            // ---- select / cap / representatives
+            tic();
+            k_select<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+            check_launch();
+            if (any_cap) {
+                scan(flag_new.p, scan_new.p, n_ev);
+                k_cut<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+                check_launch();
+            }
+            k_rep<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+            check_launch();
+            scan(flag_rep.p, flag_rep.p, n_ev);
+            scan(flag_front.p, flag_front.p, n_ev);
+            toc(times.select);
+        } else {
+            HGX_CUDA_CHECK(cudaMemsetAsync(flag_rep.p, 0, 4, st));
+            HGX_CUDA_CHECK(cudaMemsetAsync(flag_front.p, 0, 4, st));
+        }
+        if (opt.branchial && n_ev) {
+            tic();
+            k_bcount<<<grid_for(uint64_t(F) * 32, 256), 256, 0, st>>>(ptrs(), A);
+            check_launch();
+            scan(bcount.p, boff.p, F);
+            toc(times.branchial);
+        } else {
+            HGX_CUDA_CHECK(cudaMemsetAsync(boff.p + F, 0, 4, st));
+        }
+
+        // ---- sync 2: new states, next frontier, branchial pairs, errors
+        uint32_t s2[4];
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[0], flag_rep.p + n_ev, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[1], flag_front.p + n_ev, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + F, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[3], err.p, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (s2[3]) throw std::runtime_error("hgx: device error flags 0x" + std::to_string(s2[3]));
+        const uint32_t n_new = s2[0], n_front = s2[1], n_b = s2[2];
+
+        grow_states(n_states + n_new);
+        new_state_event.ensure(n_new, 0, st);
+        next_frontier.ensure(n_front, 0, st);
+        const uint64_t max_ne = uint64_t(fmax_ne) + rm.grow_e, max_no = uint64_t(fmax_nocc) + rm.grow_o;
+        const uint64_t rec_words = max_ne + (max_ne + 3) / 4 + max_no;
+        arena.ensure(arena_words + uint64_t(n_new) * rec_words, arena_words, st);
+        bpairs.ensure(2ull * (n_bpairs + n_b), 2ull * n_bpairs, st);
+        A.state_base = static_cast<uint32_t>(n_states);
+        A.new_state_event = new_state_event.p;
+        A.next_frontier = next_frontier.p;
+        A.bpairs = bpairs.p;
+        A.bbase = static_cast<uint32_t>(n_bpairs);
+        if (n_ev) {
+            tic();
+            k_assign<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+            check_launch();
+            k_outstate<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+            check_launch();
+            if (n_new) {
+                k_materialize<<<grid_for(uint64_t(n_new) * 32, 256), 256, 0, st>>>(ptrs(), A, n_new);
+                check_launch();
+            }
+            toc(times.materialize);
+        }
+        if (opt.branchial && n_b) {
+            tic();
+            // pair offsets are absolute: shift by the running total
+            A.boff = boff.p;
+            A.bpairs = bpairs.p + 2ull * n_bpairs;
+            k_bemit<<<grid_for(uint64_t(F) * 32, 256), 256, 0, st>>>(ptrs(), A);
+            check_launch();
+            toc(times.branchial);
+        }
+
+        // which evolutions still have a frontier
+        std::vector<uint8_t> present(nevo, 0);
+        if (n_front) {
+            evo_front.ensure(nevo, 0, st);
+            HGX_CUDA_CHECK(cudaMemsetAsync(evo_front.p, 0, nevo * 4, st));
+            k_mark_front<<<grid_for(n_front, 256), 256, 0, st>>>(ptrs(), next_frontier.p, n_front, evo_front.p);
+            check_launch();
+            std::vector<uint32_t> hf(nevo);
+            HGX_CUDA_CHECK(cudaMemcpyAsync(hf.data(), evo_front.p, nevo * 4, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            for (size_t e = 0; e < nevo; ++e) present[e] = hf[e] ? 1 : 0;
+        }
+        for (size_t e = 0; e < nevo; ++e)
+            if (!evo_done[e] && h_first[e] != kNone && !present[e]) {
+                evo_done[e] = 1;
+                finished.push_back(static_cast<uint32_t>(e));
+            }
+
+        // advance
+        n_events += n_ev;
+        n_cons += n_cons_lv;
+        n_edges += n_prod;
+        next_vertex += n_fresh;
+        n_states += n_new;
+        n_bpairs += n_b;
+        arena_words += uint64_t(n_new) * rec_words;   // host bound >= the device bump pointer
+        std::swap(frontier, next_frontier);
+        frontier_size = n_front;
+        ne_bound = static_cast<uint32_t>(max_ne);
+        nocc_bound = static_cast<uint32_t>(max_no);
+        return frontier_size > 0;
+    }
+};
+
+// ==========================================================================================
+// Result readback (bulk copy, then split by evolution on the host).
+// ==========================================================================================
+
+namespace {
+
+template <class T>
+std::vector<T> d2h(const T* p, size_t n, cudaStream_t st) {
+    std::vector<T> v(n);
+    if (n) HGX_CUDA_CHECK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+    return v;
+}
+
+}  // namespace
+
+void Engine::Impl::read_results(const std::vector<uint32_t>& which, const RunOptions& opt,
+                                std::vector<EvolutionResult>& out) {
+    Impl& I = *this;
+    cudaStream_t st = I.st;
+    const size_t nevo = I.h_evos.size();
+    auto s_evo = d2h(I.st_evo.p, I.n_states, st);
+    auto s_depth = d2h(I.st_depth.p, I.n_states, st);
+    auto s_hash = d2h(I.st_hash.p, I.n_states, st);
+    auto s_event = d2h(I.st_event.p, I.n_states, st);
+    auto e_in = d2h(I.ev_in.p, I.n_events, st);
+    auto e_out = d2h(I.ev_out.p, I.n_events, st);
+    auto e_rule = d2h(I.ev_rule.p, I.n_events, st);
+    auto e_kept = d2h(I.ev_kept.p, I.n_events, st);
+    auto e_coff = d2h(I.ev_coff.p, I.n_events, st);
+    auto e_prod = d2h(I.ev_prod.p, I.n_events, st);
+    auto e_cons = d2h(I.ev_cons.p, I.n_cons, st);
+    auto e_cprod = d2h(I.ev_cprod.p, I.n_cons, st);
+    auto bp = d2h(I.bpairs.p, 2 * I.n_bpairs, st);
+    auto evc = d2h(I.evo_classes.p, nevo, st);
+    auto evs = d2h(I.evo_stopped.p, nevo, st);
+    std::vector<uint64_t> s_off;
+    std::vector<uint32_t> s_ne, s_nocc, arena;
+    if (opt.keep_state_edges) {
+        s_off = d2h(I.st_off.p, I.n_states, st);
+        s_ne = d2h(I.st_ne.p, I.n_states, st);
+        s_nocc = d2h(I.st_nocc.p, I.n_states, st);
+        unsigned long long top = 0;
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&top, I.arena_top.p, sizeof(top), cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        arena = d2h(I.arena.p, top, st);
+    }
+    HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+
+    std::vector<int32_t> slot(nevo, -1);
+    out.assign(which.size(), EvolutionResult{});
+    for (size_t i = 0; i < which.size(); ++i) slot[which[i]] = static_cast<int32_t>(i);
+
+    // local state ids
+    std::vector<uint32_t> local_state(I.n_states, kNone);
+    for (uint64_t s = 0; s < I.n_states; ++s) {
+        const int32_t k = slot[s_evo[s]];
+        if (k < 0) continue;
+        EvolutionResult& r = out[k];
+        local_state[s] = static_cast<uint32_t>(r.state_hash.size());
+        r.state_hash.push_back(s_hash[s]);
+        r.state_depth.push_back(s_depth[s]);
+        r.state_event.push_back(s_event[s]);   // global arrival, remapped below
+        if (opt.keep_state_edges) {
+            if (r.state_edge_off.empty()) { r.state_edge_off.push_back(0); r.state_vert_off.push_back(0); }
+            const uint32_t* rec = arena.data() + s_off[s];
+            const uint32_t ne = s_ne[s], aw = (ne + 3) / 4;
+            for (uint32_t i = 0; i < ne; ++i) {
+                r.state_edge_ids.push_back(rec[i]);
+                r.state_arity.push_back((rec[ne + i / 4] >> ((i % 4) * 8)) & 0xFFu);
+            }
+            r.state_verts.insert(r.state_verts.end(), rec + ne + aw, rec + ne + aw + s_nocc[s]);
+            r.state_edge_off.push_back(static_cast<uint32_t>(r.state_edge_ids.size()));
+            r.state_vert_off.push_back(static_cast<uint32_t>(r.state_verts.size()));
+        }
+    }
+    // local event ids
+    std::vector<uint32_t> local_event(I.n_events, kNone);
+    for (uint64_t e = 0; e < I.n_events; ++e) {
+        if (e_in[e] == kNone || !e_kept[e]) continue;
+        const uint32_t in = e_in[e];
+        const int32_t k = slot[s_evo[in]];
+        if (k < 0) continue;
+        EvolutionResult& r = out[k];
+        local_event[e] = static_cast<uint32_t>(r.ev_in.size());
+        r.ev_in.push_back(local_state[in]);
+        r.ev_out.push_back(e_out[e] < I.n_states ? local_state[e_out[e]] : kNone);
+        r.ev_rule.push_back(e_rule[e] - I.h_evos[s_evo[in]].rule_begin);
+        r.ev_step.push_back(s_depth[in] + 1);
+        const DevRule& R = I.h_rules[e_rule[e]];
+        if (r.ev_cons_off.empty()) r.ev_cons_off.push_back(0);
+        for (uint32_t k2 = 0; k2 < R.n_lhs; ++k2) r.ev_cons.push_back(e_cons[e_coff[e] + k2]);
+        r.ev_cons_off.push_back(static_cast<uint32_t>(r.ev_cons.size()));
+        r.ev_prod_first.push_back(e_prod[e]);
+        r.ev_prod_count.push_back(R.n_rhs);
+    }
+    for (auto& r : out)
+        for (auto& se : r.state_event) se = (se < local_event.size() && local_event[se] != kNone) ? local_event[se] : kNone;
+    // causal triples
+    if (opt.causal) {
+        for (uint64_t e = 0; e < I.n_events; ++e) {
+            if (local_event[e] == kNone) continue;
+            EvolutionResult& r = out[slot[s_evo[e_in[e]]]];
+            const DevRule& R = I.h_rules[e_rule[e]];
+            for (uint32_t k2 = 0; k2 < R.n_lhs; ++k2) {
+                const uint32_t p = e_cprod[e_coff[e] + k2];
+                if (p == kNone || local_event[p] == kNone) continue;
+                r.causal.push_back(local_event[p]);
+                r.causal.push_back(local_event[e]);
+                r.causal.push_back(e_cons[e_coff[e] + k2]);
+            }
+        }
+    }
+    for (uint64_t i = 0; i < I.n_bpairs; ++i) {
+        const uint32_t a = bp[2 * i], b = bp[2 * i + 1];
+        const int32_t k = slot[s_evo[e_in[a]]];
+        if (k < 0) continue;
+        out[k].branchial.push_back(local_event[a]);
+        out[k].branchial.push_back(local_event[b]);
+    }
+    for (size_t i = 0; i < which.size(); ++i) {
+        out[i].num_classes = evc[which[i]];
+        out[i].truncated = evs[which[i]] != 0;
+        if (out[i].truncated)
+            out[i].warnings.push_back(
+                "capacity limit reached: the state cap stopped the evolution; the states, events "
+                "and relations returned are valid and incomplete");
+    }
+}
+
+// ==========================================================================================
+
+Engine::Engine(int device) : impl_(new Impl(device)) {}
+Engine::~Engine() = default;
+
+std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs, const RunOptions& opt) {
+    Impl& I = *impl_;
+    HGX_CUDA_CHECK(cudaSetDevice(I.device));
+    I.reset();
+    std::vector<uint32_t> ids;
+    for (const auto& s : specs) ids.push_back(I.admit(s));
+    while (I.level(opt)) {}
+    std::vector<EvolutionResult> out;
+    I.read_results(ids, opt, out);
+    I.times.launches = I.launches;
+    return out;
+}
+
+void Engine::reset() { impl_->reset(); }
+uint32_t Engine::admit(const EvolutionSpec& spec) { return impl_->admit(spec); }
+bool Engine::step(const RunOptions& opt) { return impl_->level(opt); }
+std::vector<uint32_t> Engine::take_finished() {
+    std::vector<uint32_t> f;
+    f.swap(impl_->finished);
+    return f;
+}
+EvolutionResult Engine::collect(uint32_t evo, const RunOptions& opt) {
+    std::vector<EvolutionResult> out;
+    impl_->read_results({evo}, opt, out);
+    return std::move(out[0]);
+}
+uint32_t Engine::active() const {
+    uint32_t n = 0;
+    for (uint8_t d : impl_->evo_done) n += d ? 0 : 1;
+    return n;
+}
+uint64_t Engine::device_bytes_in_use() const {
+    const Impl& I = *impl_;
+    return I.arena.bytes() + I.st_off.bytes() * 2 + I.st_ne.bytes() * 5 + I.edge_creator.bytes() +
+           I.ev_in.bytes() * 8 + I.ev_hash.bytes() + I.ev_cons.bytes() * 2 + I.tab_keys.bytes() +
+           I.tab_vals.bytes() + I.bpairs.bytes();
+}
+uint64_t Engine::estimate_bytes(const EvolutionSpec& spec) {
+    // Per state: record (~ 6 words/edge) + SoA (40 B); per event ~ 64 B + relations.
+    uint64_t edges = 0;
+    for (const auto& r : spec.roots) edges += r.size();
+    const uint64_t states = spec.max_states ? spec.max_states : 100000;
+    const uint64_t per_state = (edges + 4ull * spec.steps) * 24 + 40;
+    return states * per_state + states * 8 * 96 + states * 64;
+}
+cudaStream_t Engine::stream() const { return impl_->st; }
+void Engine::set_timing(bool on) { impl_->timing = on; }
+const StageTimes& Engine::times() const { return impl_->times; }
+void Engine::sync() { HGX_CUDA_CHECK(cudaStreamSynchronize(impl_->st)); }
+
+}  // namespace hgx

@@ -1,0 +1,113 @@
+// Host engine: device-resident multiway evolution over a batch of independent evolutions.
+//
+// This is the native runtime behind the C-ABI (include/hgx.h). It owns the device arrays,
+// drives the level-synchronous step kernels and reads results back. One Engine serves the three
+// ways the step is used:
+//   * one evolution per call      (the plain path; what ParallelEvolutionEngine::evolve and
+//                                  hg_gpu::evolve callers get)
+//   * a batch of evolutions       (every level of every evolution in one launch per stage)
+//   * a continuous request stream (admit between levels; finished evolutions are collected
+//                                  while others keep running)
+// No CPU fallback exists: without a CUDA device the constructor throws.
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace hgx {
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const char* expr, const char* file, int line)
+        : std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(c) + " at " + file +
+                             ":" + std::to_string(line) + " (" + expr + ")"),
+          code(c) {}
+};
+
+// A rule as pattern-variable edge lists (variables < 32, arity 1..16, <= 16 edges per side).
+struct RuleSpec {
+    std::vector<std::vector<uint8_t>> lhs, rhs;
+};
+
+struct EvolutionSpec {
+    std::vector<RuleSpec> rules;
+    std::vector<std::vector<std::vector<uint32_t>>> roots;   // one or more initial states
+    uint32_t steps = 0;
+    bool quotient = true;        // true: each WL class expanded once, at its shortest depth
+    uint64_t max_states = 0;     // 0 = unlimited; WL classes (quotient) or raw states (full)
+};
+
+struct EvolutionResult {
+    // States: in full multiway every raw state; in quotient mode one per WL class.
+    std::vector<uint64_t> state_hash;
+    std::vector<uint32_t> state_depth;
+    std::vector<uint32_t> state_event;          // creating event (kNone for roots)
+    std::vector<uint32_t> state_edge_off;       // [n+1] offsets into state_edge_ids (if kept)
+    std::vector<uint32_t> state_edge_ids;
+    std::vector<uint32_t> state_vert_off;       // [n+1] offsets into state_verts
+    std::vector<uint32_t> state_arity;          // per edge, parallel to state_edge_ids
+    std::vector<uint32_t> state_verts;
+    // Events (ids local to this evolution, in canonical order).
+    std::vector<uint32_t> ev_in, ev_out, ev_rule, ev_step;
+    std::vector<uint32_t> ev_cons_off;          // [n+1]
+    std::vector<uint32_t> ev_cons;              // consumed edge ids (pattern order)
+    std::vector<uint32_t> ev_prod_first, ev_prod_count;
+    // Relations over local event ids.
+    std::vector<uint32_t> causal;               // (producer, consumer, edge) triples
+    std::vector<uint32_t> branchial;            // (a, b) pairs, a < b
+    uint64_t num_classes = 0;
+    bool truncated = false;
+    std::vector<std::string> warnings;
+};
+
+struct RunOptions {
+    bool keep_state_edges = true;    // read back every state's edge record
+    bool causal = true;
+    bool branchial = true;
+};
+
+// Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.
+struct StageTimes {
+    double count = 0, scan = 0, expand = 0, select = 0, materialize = 0, branchial = 0,
+           roots = 0, total = 0;
+    uint64_t launches = 0;   // kernels this engine launched during the run
+    uint64_t expand_launches = 0;
+    uint64_t expand_bytes = 0;   // algorithmic bytes of the expand kernel (see DESIGN)
+};
+
+class Engine {
+public:
+    explicit Engine(int device = 0);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Run a batch of independent evolutions to completion; one result per spec.
+    std::vector<EvolutionResult> run(const std::vector<EvolutionSpec>& specs,
+                                     const RunOptions& opt = {});
+
+    // Continuous-batching interface.
+    void reset();                                   // drop everything, keep allocations
+    uint32_t admit(const EvolutionSpec& spec);      // returns the evolution id (engine-wide)
+    bool step(const RunOptions& opt = {});          // one level for every active evolution
+    std::vector<uint32_t> take_finished();          // evolutions that completed since last call
+    EvolutionResult collect(uint32_t evo, const RunOptions& opt = {});
+    uint32_t active() const;
+    uint64_t device_bytes_in_use() const;
+    static uint64_t estimate_bytes(const EvolutionSpec& spec);
+
+    cudaStream_t stream() const;
+    void set_timing(bool on);
+    const StageTimes& times() const;
+    void sync();
+
+private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
+
+}  // namespace hgx

@@ -1,0 +1,1089 @@
+// Kernels of one level-synchronous multiway step. See step_kernels.cuh for the stage list.
+//
+// Semantics restated from the reference (paths inside the reference project):
+//   binding / edge-injective join   common/include/hgcommon/match_core.hpp:32-49,
+//                                   common/include/hgcommon/join_core.hpp:144-208
+//   rewrite (fresh vertices in ascending variable order, RHS edge order)
+//                                   common/include/hgcommon/rewrite_core.hpp:53-87,
+//                                   hypergraph/src/rewriter.cpp:44-82
+//   WL canonical hash               common/include/hgcommon/wl_core.hpp:67-202 with the input
+//                                   convention of hypergraph/include/hypergraph/wl_hash.hpp:109-243
+//   causal producer of an edge      hypergraph/src/rewriter.cpp:138-191
+//   branchial pairs                 hypergraph/src/causal_graph.cpp:324-350
+//
+// Design (not a translation of the reference's GPU tree, which is one persistent launch per
+// evolution with a single-thread rewrite): every stage is a warp- or thread-granular kernel over
+// the whole frontier of every evolution in the batch; warps pull frontier states from a device
+// work counter so uneven state sizes balance across the 148 SMs; a state's edge record is
+// staged once in shared memory and every child of it is built and hashed there, so children are
+// never written to HBM unless they are new class representatives.
+#include "step_kernels.cuh"
+
+namespace hgx {
+
+namespace {
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+template <typename T>
+__device__ __forceinline__ T* smp(char* base, uint32_t off) {
+    return reinterpret_cast<T*>(base + off);
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x) {
+    const uint32_t lane = lane_id();
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= static_cast<uint32_t>(d)) x += y;
+    }
+    return x;
+}
+
+__device__ __forceinline__ uint64_t warp_sum64(uint64_t x) {
+#pragma unroll
+    for (int d = 16; d; d >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, d);
+    return x;
+}
+
+__device__ __forceinline__ uint32_t warp_sum32(uint32_t x) {
+#pragma unroll
+    for (int d = 16; d; d >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, d);
+    return x;
+}
+
+__device__ __forceinline__ uint32_t warp_max32(uint32_t x) {
+#pragma unroll
+    for (int d = 16; d; d >>= 1) x = max(x, __shfl_xor_sync(0xFFFFFFFFu, x, d));
+    return x;
+}
+
+__device__ __forceinline__ void isort64(uint64_t* a, uint32_t n) {
+    for (uint32_t i = 1; i < n; ++i) {
+        const uint64_t k = a[i];
+        uint32_t j = i;
+        while (j > 0 && a[j - 1] > k) { a[j] = a[j - 1]; --j; }
+        a[j] = k;
+    }
+}
+
+__device__ __forceinline__ void isort32(uint32_t* a, uint32_t n) {
+    for (uint32_t i = 1; i < n; ++i) {
+        const uint32_t k = a[i];
+        uint32_t j = i;
+        while (j > 0 && a[j - 1] > k) { a[j] = a[j - 1]; --j; }
+        a[j] = k;
+    }
+}
+
+// Warp-aggregated add of 1 to counter[key] for the lanes in `active`.
+__device__ __forceinline__ void warp_count(unsigned long long* counter, uint32_t key, bool active) {
+    const uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
+    if (!active) return;
+    const uint32_t peers = __match_any_sync(act, key);
+    if (lane_id() == static_cast<uint32_t>(__ffs(peers) - 1))
+        atomicAdd(&counter[key], static_cast<unsigned long long>(__popc(peers)));
+}
+
+// ------------------------------------------------------------------------------------------
+// Dedup table: open addressing, linear probing, per-evolution region. Key 0 is EMPTY; a WL hash
+// that is itself 0 lives in the extra slot after the region. The value is the smallest arrival
+// id (event id, or a root's pseudo-event id) that produced the key: the first arrival in
+// canonical order wins, whatever order the warps ran in.
+// ------------------------------------------------------------------------------------------
+__device__ void table_insert(const DevPtrs& P, const DevEvo& ev, uint64_t h, uint32_t arrival) {
+    const uint64_t base = ev.table_off, mask = ev.table_mask;
+    if (h == 0) { atomicMin(&P.tab_vals[base + mask + 1], arrival); return; }
+    uint64_t slot = smix(h) & mask;
+    for (uint64_t probe = 0; probe <= mask; ++probe) {
+        unsigned long long* kp = &P.tab_keys[base + slot];
+        unsigned long long k = *reinterpret_cast<volatile unsigned long long*>(kp);
+        if (k == 0ull) {
+            k = atomicCAS(kp, 0ull, static_cast<unsigned long long>(h));
+            if (k == 0ull) k = h;
+        }
+        if (k == h) { atomicMin(&P.tab_vals[base + slot], arrival); return; }
+        slot = (slot + 1) & mask;
+    }
+    atomicOr(P.err, kErrTableFull);
+}
+
+__device__ uint32_t table_lookup(const DevPtrs& P, const DevEvo& ev, uint64_t h) {
+    const uint64_t base = ev.table_off, mask = ev.table_mask;
+    if (h == 0) return P.tab_vals[base + mask + 1];
+    uint64_t slot = smix(h) & mask;
+    for (uint64_t probe = 0; probe <= mask; ++probe) {
+        const unsigned long long k = P.tab_keys[base + slot];
+        if (k == h) return P.tab_vals[base + slot];
+        if (k == 0ull) return kNone;
+        slot = (slot + 1) & mask;
+    }
+    return kNone;
+}
+
+// ------------------------------------------------------------------------------------------
+// Parent staging: the state's edge record is read once (coalesced) into shared memory, and its
+// vertices are renumbered to local ids by first occurrence. WL is invariant under the local
+// numbering, and the join only compares vertices for equality, so nothing downstream needs the
+// global vertex ids.
+// ------------------------------------------------------------------------------------------
+struct Parent {
+    uint32_t ne, nocc, nvp;
+};
+
+__device__ Parent load_parent(const DevPtrs& P, const Layout& L, char* sm, uint32_t sid) {
+    const uint32_t lane = lane_id();
+    Parent pa;
+    pa.ne = P.st_ne[sid];
+    pa.nocc = P.st_nocc[sid];
+    pa.nvp = 0;
+    if (pa.ne > L.NE || pa.nocc > L.NOCC) {
+        if (lane == 0) atomicOr(P.err, kErrStateTooLarge);
+        pa.ne = 0;
+        pa.nocc = 0;
+        return pa;
+    }
+    const uint32_t* rec = P.arena + P.st_off[sid];
+    uint32_t* peid = smp<uint32_t>(sm, L.o_peid);
+    uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+    uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    uint32_t* glob = smp<uint32_t>(sm, L.o_occ);    // aliases the WL occurrence list
+    uint32_t* first = smp<uint32_t>(sm, L.o_deg);   // aliases the WL degrees
+    const uint32_t aw = (pa.ne + 3) >> 2;
+    for (uint32_t i = lane; i < pa.ne; i += 32) {
+        peid[i] = rec[i];
+        pear[i] = static_cast<uint8_t>((rec[pa.ne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu);
+    }
+    for (uint32_t j = lane; j < pa.nocc; j += 32) glob[j] = rec[pa.ne + aw + j];
+    __syncwarp();
+    uint32_t run = 0;
+    for (uint32_t b = 0; b < pa.ne; b += 32) {
+        const uint32_t i = b + lane;
+        const uint32_t a = i < pa.ne ? pear[i] : 0u;
+        const uint32_t inc = warp_incl_scan(a);
+        if (i < pa.ne) pevo[i] = static_cast<uint16_t>(run + inc - a);
+        run += __shfl_sync(0xFFFFFFFFu, inc, 31);
+    }
+    run = 0;
+    for (uint32_t b = 0; b < pa.nocc; b += 32) {
+        const uint32_t j = b + lane;
+        uint32_t f = j;
+        if (j < pa.nocc) {
+            const uint32_t v = glob[j];
+            for (uint32_t i = 0; i < j; ++i)
+                if (glob[i] == v) { f = i; break; }
+            first[j] = f;
+        }
+        const bool rep = (j < pa.nocc) && f == j;
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, rep);
+        if (rep) vloc[j] = static_cast<uint16_t>(run + __popc(bal & ((1u << lane) - 1u)));
+        run += __popc(bal);
+    }
+    __syncwarp();
+    for (uint32_t j = lane; j < pa.nocc; j += 32) {
+        const uint32_t f = first[j];
+        if (f != j) vloc[j] = vloc[f];
+    }
+    __syncwarp();
+    pa.nvp = run;
+    return pa;
+}
+
+__device__ __forceinline__ void load_rule(char* sm, const Layout& L, const DevRule* src) {
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = smp<uint32_t>(sm, L.o_rule);
+    for (uint32_t i = lane_id(); i < sizeof(DevRule) / 4; i += 32) d[i] = s[i];
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
+// The join. One warp holds one partial match; at every depth the 32 lanes test the state's
+// edges against the next pattern edge in parallel and a ballot compacts the survivors into a
+// candidate bitmask. Candidates are taken in ascending state position, so matches come out in
+// lexicographic order of their positions in schedule order -- the canonical event order.
+// Edge-injective (a state edge serves one pattern edge), vertex-non-injective.
+// ------------------------------------------------------------------------------------------
+__device__ void compute_cands(const Layout& L, char* sm, const DevRule& R, uint32_t p,
+                              const Parent& pa, uint32_t mask, uint32_t* cand) {
+    const uint32_t lane = lane_id();
+    const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+    const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    const uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
+    const uint32_t* taken = smp<uint32_t>(sm, L.o_taken);
+    const uint32_t a = R.lhs_ar[p];
+    const uint8_t* pv = &R.lhs_vars[R.lhs_off[p]];
+    for (uint32_t b = 0; b < pa.ne; b += 32) {
+        const uint32_t i = b + lane;
+        bool ok = false;
+        if (i < pa.ne && pear[i] == a && !((taken[i >> 5] >> (i & 31u)) & 1u)) {
+            ok = true;
+            const uint32_t vo = pevo[i];
+            for (uint32_t q = 0; q < a && ok; ++q) {
+                const uint32_t var = pv[q];
+                const uint32_t x = vloc[vo + q];
+                if ((mask >> var) & 1u) {
+                    ok = (bind[var] == x);
+                } else {
+                    for (uint32_t r = 0; r < q; ++r)
+                        if (pv[r] == var) { ok = (vloc[vo + r] == x); break; }
+                }
+            }
+        }
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ok);
+        if (lane == 0) cand[b >> 5] = bal;
+    }
+    __syncwarp();
+}
+
+template <class F>
+__device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Parent& pa,
+                          F&& on_match) {
+    const uint32_t lane = lane_id();
+    const uint32_t n = R.n_lhs;
+    const uint32_t nw = (pa.ne + 31) >> 5;
+    if (n == 0 || pa.ne == 0) return;
+    uint32_t* cand = smp<uint32_t>(sm, L.o_cand);
+    uint32_t* taken = smp<uint32_t>(sm, L.o_taken);
+    uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
+    uint16_t* match = smp<uint16_t>(sm, L.o_match);
+    uint16_t* mdepth = smp<uint16_t>(sm, L.o_mdepth);
+    uint32_t* saved = smp<uint32_t>(sm, L.o_misc);
+    const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+    const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    (void)pear;
+    for (uint32_t w = lane; w < nw; w += 32) taken[w] = 0;
+    __syncwarp();
+    uint32_t mask = 0;
+    uint32_t d = 0;
+    compute_cands(L, sm, R, R.sched[0], pa, mask, cand);
+    while (true) {
+        int pick = -1;
+        for (uint32_t w = 0; w < nw; ++w) {
+            const uint32_t c = cand[d * L.W + w];
+            if (c) { pick = static_cast<int>(w * 32 + __ffs(c) - 1); break; }
+        }
+        __syncwarp();
+        if (pick < 0) {
+            if (d == 0) break;
+            --d;
+            const uint32_t e = mdepth[d];
+            mask = saved[d];
+            __syncwarp();
+            if (lane == 0) taken[e >> 5] &= ~(1u << (e & 31u));
+            __syncwarp();
+            continue;
+        }
+        const uint32_t p = R.sched[d];
+        if (lane == 0) {
+            cand[d * L.W + (pick >> 5)] &= ~(1u << (pick & 31));
+            taken[pick >> 5] |= 1u << (pick & 31);
+            match[p] = static_cast<uint16_t>(pick);
+            mdepth[d] = static_cast<uint16_t>(pick);
+            saved[d] = mask;
+        }
+        const uint32_t a = R.lhs_ar[p];
+        const uint8_t* pv = &R.lhs_vars[R.lhs_off[p]];
+        const uint32_t vo = pevo[pick];
+        uint32_t nm = mask;
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t var = pv[q];
+            if (!((nm >> var) & 1u)) {
+                if (lane == 0) bind[var] = vloc[vo + q];
+                nm |= 1u << var;
+            }
+        }
+        __syncwarp();
+        if (d + 1 == n) {
+            on_match(nm);
+            __syncwarp();
+            if (lane == 0) taken[pick >> 5] &= ~(1u << (pick & 31));
+            __syncwarp();
+        } else {
+            mask = nm;
+            ++d;
+            compute_cands(L, sm, R, R.sched[d], pa, mask, cand + d * L.W);
+        }
+    }
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
+// Child construction in shared memory: parent edges minus the matched ones (ascending, so the
+// reference's ascending edge-id order is kept) followed by the produced edges in RHS order.
+// Vertices stay local: a matched variable takes its bound local id, the n-th fresh variable
+// takes local id nvp + n.
+// ------------------------------------------------------------------------------------------
+__device__ uint32_t build_child(const Layout& L, char* sm, const DevRule& R, const Parent& pa,
+                                uint32_t nm) {
+    const uint32_t lane = lane_id();
+    const uint32_t* taken = smp<uint32_t>(sm, L.o_taken);
+    const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+    const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    const uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
+    uint8_t* car = smp<uint8_t>(sm, L.o_car);
+    uint16_t* cvo = smp<uint16_t>(sm, L.o_cvo);
+    uint32_t run = 0;
+    for (uint32_t b = 0; b < pa.ne; b += 32) {
+        const uint32_t i = b + lane;
+        const bool keep = i < pa.ne && !((taken[i >> 5] >> (i & 31u)) & 1u);
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+        if (keep) {
+            const uint32_t c = run + __popc(bal & ((1u << lane) - 1u));
+            car[c] = pear[i];
+            cvo[c] = pevo[i];
+        }
+        run += __popc(bal);
+    }
+    for (uint32_t k = lane; k < R.n_rhs; k += 32) {
+        car[run + k] = R.rhs_ar[k];
+        cvo[run + k] = static_cast<uint16_t>(pa.nocc + R.rhs_off[k]);
+    }
+    for (uint32_t t = lane; t < R.rhs_total; t += 32) {
+        const uint32_t var = R.rhs_vars[t];
+        vloc[pa.nocc + t] = ((nm >> var) & 1u) ? bind[var]
+                                                : static_cast<uint16_t>(pa.nvp + R.fresh_rank[var]);
+    }
+    __syncwarp();
+    return run + R.n_rhs;
+}
+
+// ------------------------------------------------------------------------------------------
+// WL canonical hash of the state held in shared memory (car/cvo/vloc, `ne` edges over local
+// vertex ids [0, V)), computed by one warp: lanes own vertices. Bit-identical to the reference
+// core: initial colour FNV(deg, sorted (arity,pos) of the first `cap` occurrences), rounds of
+// sorted neighbour folds until the distinct-colour count stops changing (<= 100), then the
+// component fold and the final FNV over (n_v, n_e, sums).
+// ------------------------------------------------------------------------------------------
+__device__ uint32_t wl_distinct(const uint64_t* cur, const uint32_t* deg, uint32_t V) {
+    uint32_t cnt = 0;
+    for (uint32_t v = lane_id(); v < V; v += 32) {
+        if (!deg[v]) continue;
+        const uint64_t c = cur[v];
+        bool first = true;
+        for (uint32_t u = 0; u < v; ++u)
+            if (deg[u] && cur[u] == c) { first = false; break; }
+        cnt += first ? 1u : 0u;
+    }
+    return warp_sum32(cnt);
+}
+
+__device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V) {
+    const uint32_t lane = lane_id();
+    const uint8_t* car = smp<uint8_t>(sm, L.o_car);
+    const uint16_t* cvo = smp<uint16_t>(sm, L.o_cvo);
+    const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    uint64_t* cur = smp<uint64_t>(sm, L.o_cur);
+    uint64_t* nxt = smp<uint64_t>(sm, L.o_nxt);
+    uint64_t* csum = smp<uint64_t>(sm, L.o_csum);
+    uint64_t* ccnt = smp<uint64_t>(sm, L.o_ccnt);
+    uint64_t* nbr = smp<uint64_t>(sm, L.o_nbr);
+    uint32_t* occ = smp<uint32_t>(sm, L.o_occ);
+    uint32_t* ooff = smp<uint32_t>(sm, L.o_ooff);
+    uint32_t* nbo = smp<uint32_t>(sm, L.o_nbo);
+    uint32_t* deg = smp<uint32_t>(sm, L.o_deg);
+    uint32_t* nn = smp<uint32_t>(sm, L.o_nn);
+    uint32_t* comp = smp<uint32_t>(sm, L.o_comp);
+
+    if (ne == 0) return kEmptyStateHash;
+
+    for (uint32_t v = lane; v < V; v += 32) { deg[v] = 0; nn[v] = 0; }
+    __syncwarp();
+    for (uint32_t e = lane; e < ne; e += 32) {
+        const uint32_t a = car[e], vo = cvo[e];
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t v = vloc[vo + q];
+            atomicAdd(&deg[v], 1u);
+            atomicAdd(&nn[v], a - 1u);
+        }
+    }
+    __syncwarp();
+    uint32_t run_o = 0, run_n = 0, nv = 0, cap = 1;
+    for (uint32_t b = 0; b < V; b += 32) {
+        const uint32_t v = b + lane;
+        const uint32_t dv = v < V ? deg[v] : 0u;
+        const uint32_t nnv = v < V ? nn[v] : 0u;
+        const uint32_t s = max(nnv, dv);
+        const uint32_t io = warp_incl_scan(dv);
+        const uint32_t is = warp_incl_scan(s);
+        if (v < V) {
+            ooff[v] = run_o + io - dv;
+            nbo[v] = run_n + is - s;
+            comp[v] = run_o + io - dv;
+        }
+        run_o += __shfl_sync(0xFFFFFFFFu, io, 31);
+        run_n += __shfl_sync(0xFFFFFFFFu, is, 31);
+        nv += __popc(__ballot_sync(0xFFFFFFFFu, dv > 0));
+        cap = max(cap, warp_max32(nnv));
+    }
+    if (nv == 0) return 0;   // only arity-0 edges: the reference core returns 0
+    __syncwarp();
+    for (uint32_t e = lane; e < ne; e += 32) {
+        const uint32_t a = car[e], vo = cvo[e];
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t slot = atomicAdd(&comp[vloc[vo + q]], 1u);
+            occ[slot] = (e << 8) | q;
+        }
+    }
+    __syncwarp();
+
+    // initial colours
+    for (uint32_t v = lane; v < V; v += 32) {
+        const uint32_t dv = deg[v];
+        if (!dv) continue;
+        uint32_t* o = occ + ooff[v];
+        if (dv > cap) isort32(o, dv);   // truncation keeps the first `cap` in edge order
+        uint64_t* kb = nbr + nbo[v];
+        const uint32_t n = min(dv, cap);
+        for (uint32_t j = 0; j < n; ++j) {
+            const uint32_t x = o[j];
+            kb[j] = (static_cast<uint64_t>(car[x >> 8]) << 8) | (x & 0xFFu);
+        }
+        isort64(kb, n);
+        uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(dv));
+        for (uint32_t j = 0; j < n; ++j) {
+            h = fnv(h, kb[j] >> 8);
+            h = fnv(h, kb[j] & 0xFFu);
+        }
+        cur[v] = h;
+    }
+    __syncwarp();
+    uint32_t prev = wl_distinct(cur, deg, V);
+    for (uint32_t it = 0; it < kWlMaxRounds; ++it) {
+        for (uint32_t v = lane; v < V; v += 32) {
+            const uint32_t dv = deg[v];
+            if (!dv) continue;
+            const uint32_t* o = occ + ooff[v];
+            uint64_t* kb = nbr + nbo[v];
+            uint32_t n = 0;
+            for (uint32_t j = 0; j < dv; ++j) {
+                const uint32_t x = o[j];
+                const uint32_t e = x >> 8, q = x & 0xFFu;
+                const uint32_t a = car[e], vo = cvo[e];
+                for (uint32_t k = 0; k < a; ++k)
+                    if (k != q && n < cap) kb[n++] = fnv(cur[vloc[vo + k]], k);
+            }
+            isort64(kb, n);
+            uint64_t h = cur[v];
+            for (uint32_t j = 0; j < n; ++j) h = fnv(h, kb[j]);
+            nxt[v] = h;
+        }
+        __syncwarp();
+        for (uint32_t v = lane; v < V; v += 32) cur[v] = nxt[v];
+        __syncwarp();
+        const uint32_t dd = wl_distinct(cur, deg, V);
+        if (dd == prev) break;
+        prev = dd;
+    }
+
+    // components (union-find on one lane; the partition is what enters the hash)
+    for (uint32_t v = lane; v < V; v += 32) { comp[v] = v; csum[v] = 0; ccnt[v] = 0; }
+    __syncwarp();
+    if (lane == 0) {
+        for (uint32_t e = 0; e < ne; ++e) {
+            const uint32_t a = car[e], vo = cvo[e];
+            if (!a) continue;
+            uint32_t r = vloc[vo];
+            while (comp[r] != r) { comp[r] = comp[comp[r]]; r = comp[r]; }
+            for (uint32_t q = 1; q < a; ++q) {
+                uint32_t x = vloc[vo + q];
+                while (comp[x] != x) { comp[x] = comp[comp[x]]; x = comp[x]; }
+                if (x != r) comp[x] = r;
+            }
+        }
+    }
+    __syncwarp();
+    uint64_t vs = 0, es = 0, cs = 0;
+    for (uint32_t v = lane; v < V; v += 32) {
+        if (!deg[v]) continue;
+        uint32_t r = v;
+        while (comp[r] != r) r = comp[r];
+        const uint64_t m = smix(cur[v]);
+        vs += m;
+        atomicAdd(reinterpret_cast<unsigned long long*>(&csum[r]), static_cast<unsigned long long>(m));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&ccnt[r]), 1ull);
+    }
+    for (uint32_t e = lane; e < ne; e += 32) {
+        const uint32_t a = car[e], vo = cvo[e];
+        uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(a));
+        for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[vloc[vo + q]]);
+        es += smix(h);
+        if (a) {
+            uint32_t r = vloc[vo];
+            while (comp[r] != r) r = comp[r];
+            atomicAdd(reinterpret_cast<unsigned long long*>(&ccnt[r]), 1ull << 32);
+        }
+    }
+    __syncwarp();
+    for (uint32_t v = lane; v < V; v += 32)
+        if (deg[v] && comp[v] == v) cs += smix(fnv(fnv(kFnvOffset, ccnt[v]), csum[v]));
+    vs = warp_sum64(vs);
+    es = warp_sum64(es);
+    cs = warp_sum64(cs);
+    uint64_t h = kFnvOffset;
+    h = fnv(h, nv);
+    h = fnv(h, ne);
+    h = fnv(h, vs);
+    h = fnv(h, es);
+    h = fnv(h, cs);
+    __syncwarp();
+    return h;
+}
+
+}  // namespace
+
+// ==========================================================================================
+// Kernels
+// ==========================================================================================
+
+// Root states: hash the uploaded records and seed the dedup tables.
+__global__ void k_roots(DevPtrs P, const uint32_t* sids, uint32_t n, uint32_t* work, Layout L) {
+    extern __shared__ __align__(16) char smem[];
+    char* sm = smem + (threadIdx.x >> 5) * L.bytes;
+    const uint32_t lane = lane_id();
+    while (true) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(work, 1u);
+        i = __shfl_sync(0xFFFFFFFFu, i, 0);
+        if (i >= n) break;
+        const uint32_t sid = sids[i];
+        const Parent pa = load_parent(P, L, sm, sid);
+        uint8_t* car = smp<uint8_t>(sm, L.o_car);
+        uint16_t* cvo = smp<uint16_t>(sm, L.o_cvo);
+        const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+        const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+        for (uint32_t e = lane; e < pa.ne; e += 32) { car[e] = pear[e]; cvo[e] = pevo[e]; }
+        __syncwarp();
+        const uint64_t h = warp_wl(L, sm, pa.ne, pa.nvp);
+        if (lane == 0) {
+            P.st_hash[sid] = h;
+            const uint32_t a = P.st_event[sid];
+            P.ev_hash[a] = h;
+            table_insert(P, P.evos[P.st_evo[sid]], h, a);
+        }
+        __syncwarp();
+    }
+}
+
+// Count the matches of every (frontier state, rule) item.
+__global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
+    extern __shared__ __align__(16) char smem[];
+    char* sm = smem + (threadIdx.x >> 5) * L.bytes;
+    const uint32_t lane = lane_id();
+    const DevRule& R = *smp<DevRule>(sm, L.o_rule);
+    while (true) {
+        uint32_t f = 0;
+        if (lane == 0) f = atomicAdd(&A.work[0], 1u);
+        f = __shfl_sync(0xFFFFFFFFu, f, 0);
+        if (f >= A.n_frontier) break;
+        const uint32_t sid = A.frontier[f];
+        const Parent pa = load_parent(P, L, sm, sid);
+        const DevEvo ev = P.evos[P.st_evo[sid]];
+        for (uint32_t r = 0; r < A.rules_stride; ++r) {
+            uint32_t cnt = 0;
+            if (r < ev.rule_count) {
+                load_rule(sm, L, &P.rules[ev.rule_begin + r]);
+                warp_join(L, sm, R, pa, [&](uint32_t) { ++cnt; });
+            }
+            if (lane == 0) A.counts[f * A.rules_stride + r] = cnt;
+            __syncwarp();
+        }
+    }
+}
+
+// Per-item counts scaled by the rule's consumed / produced / fresh sizes, for the scans.
+__global__ void k_item_sizes(DevPtrs P, LevelArgs A) {
+    const uint32_t n = A.n_frontier * A.rules_stride;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t f = t / A.rules_stride, r = t % A.rules_stride;
+        const uint32_t sid = A.frontier[f];
+        const DevEvo& ev = P.evos[P.st_evo[sid]];
+        const uint32_t c = A.counts[t];
+        uint32_t cons = 0, prod = 0, fresh = 0;
+        if (r < ev.rule_count && c) {
+            const DevRule& R = P.rules[ev.rule_begin + r];
+            cons = c * R.n_lhs;
+            prod = c * R.n_rhs;
+            fresh = c * R.n_fresh;
+        }
+        A.item_ev[t] = c;
+        A.item_cons[t] = cons;
+        A.item_prod[t] = prod;
+        A.item_fresh[t] = fresh;
+    }
+}
+
+// Enumerate again; mint events, produced edges and fresh vertices at the scanned offsets;
+// build and WL-hash every child in shared memory; insert the hash into the dedup table.
+__global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
+    extern __shared__ __align__(16) char smem[];
+    char* sm = smem + (threadIdx.x >> 5) * L.bytes;
+    const uint32_t lane = lane_id();
+    const DevRule& R = *smp<DevRule>(sm, L.o_rule);
+    const uint32_t* peid = smp<uint32_t>(sm, L.o_peid);
+    const uint16_t* match = smp<uint16_t>(sm, L.o_match);
+    while (true) {
+        uint32_t f = 0;
+        if (lane == 0) f = atomicAdd(&A.work[1], 1u);
+        f = __shfl_sync(0xFFFFFFFFu, f, 0);
+        if (f >= A.n_frontier) break;
+        const uint32_t sid = A.frontier[f];
+        const Parent pa = load_parent(P, L, sm, sid);
+        const uint32_t evo = P.st_evo[sid];
+        const DevEvo ev = P.evos[evo];
+        for (uint32_t r = 0; r < A.rules_stride && r < ev.rule_count; ++r) {
+            const uint32_t item = f * A.rules_stride + r;
+            if (A.counts[item] == 0) continue;
+            load_rule(sm, L, &P.rules[ev.rule_begin + r]);
+            const uint32_t ev0 = A.ev_base + A.item_ev[item];
+            const uint32_t cons0 = A.cons_base + A.item_cons[item];
+            const uint32_t prod0 = A.prod_base + A.item_prod[item];
+            const uint32_t fresh0 = A.fresh_base + A.item_fresh[item];
+            const uint32_t rule_g = ev.rule_begin + r;
+            uint32_t idx = 0;
+            warp_join(L, sm, R, pa, [&](uint32_t nm) {
+                const uint32_t e = ev0 + idx;
+                const uint32_t coff = cons0 + idx * R.n_lhs;
+                const uint32_t pid = prod0 + idx * R.n_rhs;
+                if (lane < R.n_lhs) {
+                    const uint32_t gid = peid[match[lane]];
+                    P.ev_cons[coff + lane] = gid;
+                    P.ev_cprod[coff + lane] = P.edge_creator[gid];
+                }
+                if (lane < R.n_rhs) P.edge_creator[pid + lane] = e;
+                if (lane == 0) {
+                    P.ev_in[e] = sid;
+                    P.ev_rule[e] = rule_g;
+                    P.ev_coff[e] = coff;
+                    P.ev_prod[e] = pid;
+                    P.ev_fresh[e] = fresh0 + idx * R.n_fresh;
+                }
+                const uint32_t nec = build_child(L, sm, R, pa, nm);
+                const uint64_t h = warp_wl(L, sm, nec, pa.nvp + R.n_fresh);
+                if (lane == 0) {
+                    P.ev_hash[e] = h;
+                    table_insert(P, ev, h, e);
+                }
+                ++idx;
+            });
+        }
+    }
+}
+
+// First / one-past-last event of every evolution in this level (the frontier is grouped by
+// evolution, so each evolution's items are contiguous); resets the evolution's cap cut.
+__global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last) {
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
+         f += gridDim.x * blockDim.x) {
+        const uint32_t evo = P.st_evo[A.frontier[f]];
+        if (f == 0 || P.st_evo[A.frontier[f - 1]] != evo) {
+            P.evo_first_ev[evo] = A.ev_base + A.item_ev[f * A.rules_stride];
+            P.evo_cut[evo] = kNone;
+        }
+        if (f + 1 == A.n_frontier || P.st_evo[A.frontier[f + 1]] != evo)
+            evo_last[evo] = A.ev_base + A.item_ev[(f + 1) * A.rules_stride];
+    }
+}
+
+// Largest edge count / occurrence count in the frontier (sizes the expand kernel's layout).
+__global__ void k_frontier_max(DevPtrs P, LevelArgs A) {
+    uint32_t mne = 0, mno = 0;
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
+         f += gridDim.x * blockDim.x) {
+        const uint32_t sid = A.frontier[f];
+        mne = max(mne, P.st_ne[sid]);
+        mno = max(mno, P.st_nocc[sid]);
+    }
+    mne = warp_max32(mne);
+    mno = warp_max32(mno);
+    if (lane_id() == 0) {
+        atomicMax(&A.level_max[2], mne);
+        atomicMax(&A.level_max[3], mno);
+    }
+}
+
+// Roots: count WL classes (first arrival of each hash) and states per evolution.
+__global__ void k_root_counts(DevPtrs P, const uint32_t* sids, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t sid = sids[i];
+        const uint32_t evo = P.st_evo[sid];
+        const uint32_t w = table_lookup(P, P.evos[evo], P.st_hash[sid]);
+        if (w == P.st_event[sid]) atomicAdd(&P.evo_classes[evo], 1ull);
+        atomicAdd(&P.evo_states[evo], 1ull);
+    }
+}
+
+// Move one evolution's table into a larger region (values are already the minimum arrival).
+__global__ void k_rehash(unsigned long long* keys, uint32_t* vals, uint64_t old_off,
+                         uint64_t old_mask, uint64_t new_off, uint64_t new_mask, uint32_t* err) {
+    for (uint64_t s = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; s <= old_mask + 1;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t v = vals[old_off + s];
+        if (s == old_mask + 1) {
+            if (v != kNone) atomicMin(&vals[new_off + new_mask + 1], v);
+            continue;
+        }
+        const unsigned long long k = keys[old_off + s];
+        if (k == 0ull) continue;
+        uint64_t slot = smix(k) & new_mask;
+        bool done = false;
+        for (uint64_t probe = 0; probe <= new_mask && !done; ++probe) {
+            unsigned long long* kp = &keys[new_off + slot];
+            unsigned long long cur = atomicCAS(kp, 0ull, k);
+            if (cur == 0ull || cur == k) {
+                atomicMin(&vals[new_off + slot], v);
+                done = true;
+            }
+            slot = (slot + 1) & new_mask;
+        }
+        if (!done) atomicOr(err, kErrTableFull);
+    }
+}
+
+// Mark the evolutions that still have states to expand.
+__global__ void k_mark_front(DevPtrs P, const uint32_t* front, uint32_t n, uint32_t* mark) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        mark[P.st_evo[front[i]]] = 1;
+}
+
+// Is the child the first arrival of its WL class? (winner stored in ev_out until resolved)
+__global__ void k_select(DevPtrs P, LevelArgs A) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
+         t += gridDim.x * blockDim.x) {
+        const uint32_t e = A.ev_base + t;
+        const uint32_t evo = P.st_evo[P.ev_in[e]];
+        const uint32_t w = table_lookup(P, P.evos[evo], P.ev_hash[e]);
+        P.ev_out[e] = w;
+        A.flag_new[t] = (w == e) ? 1u : 0u;
+    }
+}
+
+// State cap: the first event of an evolution that would take it past max_states cuts the level
+// there; that event and every later one of the evolution in this level are dropped and the
+// evolution stops expanding.
+__global__ void k_cut(DevPtrs P, LevelArgs A) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
+         t += gridDim.x * blockDim.x) {
+        const uint32_t e = A.ev_base + t;
+        const uint32_t evo = P.st_evo[P.ev_in[e]];
+        const DevEvo& ev = P.evos[evo];
+        if (!ev.max_states) continue;
+        const uint32_t first = P.evo_first_ev[evo] - A.ev_base;
+        if (ev.quotient) {
+            if (!A.flag_new[t]) continue;
+            const uint64_t rank = A.scan_new[t] - A.scan_new[first] + 1;
+            const uint64_t have = P.evo_classes[evo];
+            if (have + rank > ev.max_states) atomicMin(&P.evo_cut[evo], e);
+        } else {
+            const uint64_t rank = t - first + 1;
+            if (P.evo_states[evo] + rank > ev.max_states) atomicMin(&P.evo_cut[evo], e);
+        }
+    }
+}
+
+__global__ void k_rep(DevPtrs P, LevelArgs A) {
+    for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < A.n_events; t0 += gridDim.x * blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        const bool valid = t < A.n_events;
+        uint32_t evo = 0;
+        bool kept = false, fresh = false, rep = false;
+        if (valid) {
+            const uint32_t e = A.ev_base + t;
+            const uint32_t sid = P.ev_in[e];
+            evo = P.st_evo[sid];
+            const DevEvo& ev = P.evos[evo];
+            const uint32_t cut = P.evo_cut[evo];
+            kept = e < cut;
+            fresh = kept && A.flag_new[t];
+            rep = kept && (ev.quotient ? fresh : true);
+            const bool front = rep && (P.st_depth[sid] + 1 < ev.steps) && cut == kNone;
+            P.ev_kept[e] = kept ? 1 : 0;
+            A.flag_rep[t] = rep ? 1u : 0u;
+            A.flag_front[t] = front ? 1u : 0u;
+            if (e == cut) P.evo_stopped[evo] = 1;
+        }
+        warp_count(P.evo_classes, evo, fresh);
+        warp_count(P.evo_states, evo, rep);
+    }
+}
+
+// Representatives become states (ids in event order); eligible ones form the next frontier.
+__global__ void k_assign(DevPtrs P, LevelArgs A) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
+         t += gridDim.x * blockDim.x) {
+        const uint32_t e = A.ev_base + t;
+        const bool rep = A.flag_rep[t + 1] != A.flag_rep[t];
+        if (!rep) continue;
+        const uint32_t j = A.flag_rep[t];
+        const uint32_t sid = A.state_base + j;
+        const uint32_t in = P.ev_in[e];
+        P.state_of_arrival[e] = sid;
+        A.new_state_event[j] = e;
+        P.st_event[sid] = e;
+        P.st_evo[sid] = P.st_evo[in];
+        P.st_depth[sid] = P.st_depth[in] + 1;
+        P.st_hash[sid] = P.ev_hash[e];
+        if (A.flag_front[t + 1] != A.flag_front[t]) A.next_frontier[A.flag_front[t]] = sid;
+    }
+}
+
+__global__ void k_outstate(DevPtrs P, LevelArgs A) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
+         t += gridDim.x * blockDim.x) {
+        const uint32_t e = A.ev_base + t;
+        if (!P.ev_kept[e]) { P.ev_out[e] = kNone; continue; }
+        const uint32_t evo = P.st_evo[P.ev_in[e]];
+        const bool rep = A.flag_rep[t + 1] != A.flag_rep[t];
+        if (rep || !P.evos[evo].quotient) {
+            P.ev_out[e] = P.state_of_arrival[e];
+        } else {
+            const uint32_t w = P.ev_out[e];
+            if (w == kNone) { atomicOr(P.err, kErrTableFull); P.ev_out[e] = kNone; }
+            else P.ev_out[e] = P.state_of_arrival[w];
+        }
+    }
+}
+
+// Write the edge record of every new state: parent edges minus consumed, then produced.
+__global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
+    __shared__ uint32_t bind_sm[8][kMaxVars];
+    __shared__ uint32_t cons_sm[8][kMaxPatternEdges];
+    const uint32_t lane = lane_id();
+    const uint32_t w = threadIdx.x >> 5;
+    uint32_t* bind = bind_sm[w];
+    uint32_t* cons = cons_sm[w];
+    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < n_new;
+         j += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t e = A.new_state_event[j];
+        const uint32_t sid = A.state_base + j;
+        const uint32_t f = P.ev_in[e];
+        const DevRule& R = P.rules[P.ev_rule[e]];
+        const uint32_t pne = P.st_ne[f], pnocc = P.st_nocc[f];
+        const uint32_t* prec = P.arena + P.st_off[f];
+        const uint32_t paw = (pne + 3) >> 2;
+        const uint32_t ne = pne - R.n_lhs + R.n_rhs;
+        const uint32_t nocc = pnocc - R.lhs_total + R.rhs_total;
+        const uint32_t aw = (ne + 3) >> 2;
+        const uint32_t words = ne + aw + nocc;
+        unsigned long long off = 0;
+        if (lane == 0) off = atomicAdd(P.arena_top, static_cast<unsigned long long>(words));
+        off = __shfl_sync(0xFFFFFFFFu, off, 0);
+        if (off + words > P.arena_cap) {
+            if (lane == 0) atomicOr(P.err, kErrArenaFull);
+            continue;
+        }
+        uint32_t* rec = P.arena + off;
+        uint8_t* rar = reinterpret_cast<uint8_t*>(rec + ne);
+        uint32_t* rv = rec + ne + aw;
+        if (lane < R.n_lhs) cons[lane] = P.ev_cons[P.ev_coff[e] + lane];
+        for (uint32_t t = lane; t < aw; t += 32) rec[ne + t] = 0;   // arity padding bytes
+        __syncwarp();
+        // binding from the consumed edges (sorted parent ids -> binary search for positions)
+        if (lane < R.n_lhs) {
+            const uint32_t gid = cons[lane];
+            uint32_t lo = 0, hi = pne;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (prec[mid] < gid) lo = mid + 1; else hi = mid;
+            }
+            // vertex offset of parent edge `lo`: sum of the arities before it
+            uint32_t vo = 0;
+            for (uint32_t i = 0; i < lo; ++i) vo += (prec[pne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
+            const uint32_t a = R.lhs_ar[lane];
+            for (uint32_t q = 0; q < a; ++q) bind[R.lhs_vars[R.lhs_off[lane] + q]] = prec[pne + paw + vo + q];
+        }
+        __syncwarp();
+        // kept parent edges
+        uint32_t run_e = 0, run_pv = 0, run_cv = 0;
+        for (uint32_t b = 0; b < pne; b += 32) {
+            const uint32_t i = b + lane;
+            uint32_t id = 0, a = 0;
+            bool keep = false;
+            if (i < pne) {
+                id = prec[i];
+                a = (prec[pne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
+                keep = true;
+                for (uint32_t k = 0; k < R.n_lhs; ++k) keep &= (cons[k] != id);
+            }
+            const uint32_t pinc = warp_incl_scan(a);
+            const uint32_t ka = keep ? a : 0u;
+            const uint32_t kinc = warp_incl_scan(ka);
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+            if (keep) {
+                const uint32_t c = run_e + __popc(bal & ((1u << lane) - 1u));
+                rec[c] = id;
+                rar[c] = static_cast<uint8_t>(a);
+                const uint32_t src = run_pv + pinc - a, dst = run_cv + kinc - ka;
+                for (uint32_t q = 0; q < a; ++q) rv[dst + q] = prec[pne + paw + src + q];
+            }
+            run_e += __popc(bal);
+            run_pv += __shfl_sync(0xFFFFFFFFu, pinc, 31);
+            run_cv += __shfl_sync(0xFFFFFFFFu, kinc, 31);
+        }
+        // produced edges
+        const uint32_t pid = P.ev_prod[e], fid = P.ev_fresh[e];
+        for (uint32_t k = lane; k < R.n_rhs; k += 32) {
+            rec[run_e + k] = pid + k;
+            rar[run_e + k] = R.rhs_ar[k];
+        }
+        for (uint32_t t = lane; t < R.rhs_total; t += 32) {
+            const uint32_t var = R.rhs_vars[t];
+            rv[run_cv + t] = ((R.new_mask >> var) & 1u) ? fid + R.fresh_rank[var] : bind[var];
+        }
+        if (lane == 0) {
+            P.st_off[sid] = off;
+            P.st_ne[sid] = ne;
+            P.st_nocc[sid] = nocc;
+            atomicMax(&A.level_max[0], ne);
+            atomicMax(&A.level_max[1], nocc);
+        }
+        __syncwarp();
+    }
+}
+
+// Branchial pairs: events of one input state (contiguous ids) that consumed a common edge.
+template <bool kEmit>
+__device__ void branchial_state(const DevPtrs& P, const LevelArgs& A, uint32_t f) {
+    const uint32_t lane = lane_id();
+    const uint32_t lo = A.ev_base + A.item_ev[f * A.rules_stride];
+    const uint32_t hi = A.ev_base + A.item_ev[(f + 1) * A.rules_stride];
+    uint32_t total = 0;
+    uint32_t out = kEmit ? A.boff[f] : 0u;
+    for (uint32_t b = lo; b < hi; b += 32) {
+        const uint32_t a = b + lane;
+        uint32_t cnt = 0;
+        uint32_t ca[kMaxPatternEdges];
+        uint32_t na = 0;
+        const bool live = a < hi && P.ev_kept[a];
+        if (live) {
+            na = P.rules[P.ev_rule[a]].n_lhs;
+            const uint32_t co = P.ev_coff[a];
+            for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[co + k];
+        }
+        // pass 1: count (pass 2 writes at the warp-scanned offset)
+        for (int pass = 0; pass < (kEmit ? 2 : 1); ++pass) {
+            uint32_t pos = 0;
+            if (kEmit && pass == 1) {
+                const uint32_t inc = warp_incl_scan(cnt);
+                pos = out + inc - cnt;
+                out += __shfl_sync(0xFFFFFFFFu, inc, 31);
+            }
+            cnt = 0;
+            if (live) {
+                for (uint32_t c = a + 1; c < hi; ++c) {
+                    if (!P.ev_kept[c]) continue;
+                    const uint32_t nc = P.rules[P.ev_rule[c]].n_lhs;
+                    const uint32_t co = P.ev_coff[c];
+                    bool share = false;
+                    for (uint32_t k = 0; k < nc && !share; ++k) {
+                        const uint32_t x = P.ev_cons[co + k];
+                        for (uint32_t m = 0; m < na; ++m) share |= (ca[m] == x);
+                    }
+                    if (share) {
+                        if (kEmit && pass == 1) {
+                            A.bpairs[2ull * (pos + cnt)] = a;
+                            A.bpairs[2ull * (pos + cnt) + 1] = c;
+                        }
+                        ++cnt;
+                    }
+                }
+            }
+        }
+        total += cnt;
+    }
+    if (!kEmit) {
+        total = warp_sum32(total);
+        if (lane == 0) A.bcount[f] = total;
+    }
+}
+
+__global__ void k_bcount(DevPtrs P, LevelArgs A) {
+    for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < A.n_frontier;
+         f += (gridDim.x * blockDim.x) >> 5)
+        branchial_state<false>(P, A, f);
+}
+
+__global__ void k_bemit(DevPtrs P, LevelArgs A) {
+    for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < A.n_frontier;
+         f += (gridDim.x * blockDim.x) >> 5)
+        branchial_state<true>(P, A, f);
+}
+
+// ------------------------------------------------------------------------------------------
+// Exclusive scan of uint32 (in place allowed), writes the total at out[n]. Three phases:
+// per-block sums, one block scans the sums, per-block downsweep.
+// ------------------------------------------------------------------------------------------
+constexpr uint32_t kScanThreads = 1024;
+constexpr uint32_t kScanPer = 4;
+constexpr uint32_t kScanTile = kScanThreads * kScanPer;
+
+__device__ uint32_t block_excl_scan(uint32_t x, uint32_t* sh, uint32_t& total) {
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const uint32_t inc = warp_incl_scan(x);
+    if (lane == 31) sh[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        const uint32_t s = lane < (blockDim.x >> 5) ? sh[lane] : 0u;
+        const uint32_t si = warp_incl_scan(s);
+        sh[lane] = si - s;
+        if (lane == 31) sh[32] = si;
+    }
+    __syncthreads();
+    const uint32_t r = sh[w] + inc - x;
+    total = sh[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_reduce(const uint32_t* in, uint32_t n, uint32_t* sums) {
+    __shared__ uint32_t sh[33];
+    const uint32_t base = blockIdx.x * kScanTile;
+    uint32_t s = 0;
+    for (uint32_t k = 0; k < kScanPer; ++k) {
+        const uint32_t i = base + k * kScanThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    uint32_t total;
+    block_excl_scan(s, sh, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_sums(uint32_t* sums, uint32_t nb) {
+    __shared__ uint32_t sh[33];
+    uint32_t carry = 0;
+    for (uint32_t b = 0; b < nb; b += kScanThreads) {
+        const uint32_t i = b + threadIdx.x;
+        const uint32_t x = i < nb ? sums[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_excl_scan(x, sh, total);
+        if (i < nb) sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) sums[nb] = carry;
+}
+
+__global__ void k_scan_down(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_t* sums,
+                            uint32_t nb) {
+    __shared__ uint32_t sh[33];
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
+    uint32_t v[kScanPer];
+    uint32_t s = 0;
+    for (uint32_t k = 0; k < kScanPer; ++k) {
+        const uint32_t i = base + k;
+        v[k] = i < n ? in[i] : 0u;
+        s += v[k];
+    }
+    uint32_t total;
+    uint32_t ex = block_excl_scan(s, sh, total) + sums[blockIdx.x];
+    for (uint32_t k = 0; k < kScanPer; ++k) {
+        const uint32_t i = base + k;
+        if (i < n) out[i] = ex;
+        ex += v[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = sums[nb];
+}
+
+}  // namespace hgx

@@ -1,0 +1,106 @@
+// Kernels of one level-synchronous multiway step (sm_100a).
+//
+// A step takes the frontier (states to expand, from any number of independent evolutions) to
+// the next frontier:
+//
+//   count      warp per frontier state: enumerate every rule's matches, count them
+//   scan       exclusive scan of the per-(state, rule) counts -> event / edge / vertex ids
+//   expand     warp per frontier state: enumerate again; per match write the event, mint the
+//              produced edges, build the child in shared memory, WL-hash it and insert the
+//              hash into the evolution's dedup table (first arrival wins via atomicMin)
+//   select     thread per event: is the child the first arrival of its WL class? cap check
+//   assign     thread per event: representative children become states / next frontier
+//   materialize warp per new state: write its edge record (ids, arities, vertices)
+//   branchial  warp per frontier state: event pairs of one input state sharing a consumed edge
+//
+// Everything is integer; there is no floating point on this path.
+#pragma once
+#include "common.cuh"
+
+namespace hgx {
+
+// All device arrays of an engine, by value into every kernel.
+struct DevPtrs {
+    // rules / evolutions
+    const DevRule* rules;
+    const DevEvo* evos;
+    // states (SoA, indexed by global state id)
+    uint64_t* st_off;       // word offset of the state's edge record in `arena`
+    uint32_t* st_ne;        // edges
+    uint32_t* st_nocc;      // vertex occurrences (sum of arities)
+    uint32_t* st_evo;
+    uint32_t* st_depth;
+    uint32_t* st_event;     // arrival (event or root pseudo-event) that created it
+    uint64_t* st_hash;
+    uint32_t* arena;        // per-state records: ids[ne] | arity bytes[ceil(ne/4) words] | verts[nocc]
+    unsigned long long* arena_top;
+    uint64_t arena_cap;
+    // edges (global ids)
+    uint32_t* edge_creator; // producing event, kNone for initial edges
+    // events (arrival ids; roots occupy pseudo-event slots with ev_in == kNone)
+    uint32_t* ev_in;
+    uint32_t* ev_rule;
+    uint32_t* ev_coff;      // offset of the consumed-edge list in ev_cons / ev_cprod
+    uint32_t* ev_prod;      // id of the first produced edge (RHS order, consecutive)
+    uint32_t* ev_fresh;     // first fresh vertex id (consecutive, ascending variable order)
+    uint32_t* ev_out;       // output state (the class representative in quotient mode)
+    uint8_t*  ev_kept;      // 0 when a state cap cut the event off
+    uint64_t* ev_hash;      // WL hash of the output state
+    uint32_t* ev_cons;      // consumed edge ids, pattern order
+    uint32_t* ev_cprod;     // producer event of each consumed edge
+    uint32_t* state_of_arrival;
+    // dedup tables (all evolutions, each at its own offset)
+    unsigned long long* tab_keys;
+    uint32_t* tab_vals;
+    // per-evolution counters
+    unsigned long long* evo_classes;   // WL classes seen so far
+    unsigned long long* evo_states;    // states recorded so far
+    uint32_t* evo_cut;                 // first event cut off by the cap this level (kNone = none)
+    uint32_t* evo_first_ev;            // first event of the evolution in this level
+    uint32_t* evo_stopped;
+    // errors
+    uint32_t* err;
+};
+
+// Per-level parameters.
+struct LevelArgs {
+    const uint32_t* frontier;   // state ids
+    uint32_t n_frontier;
+    uint32_t rules_stride;      // R: item (f, r) = f * R + r
+    uint32_t* counts;           // [F*R] matches per item
+    uint32_t* item_ev;          // [F*R+1] exclusive scans
+    uint32_t* item_cons;
+    uint32_t* item_prod;
+    uint32_t* item_fresh;
+    uint32_t ev_base, cons_base, prod_base, fresh_base;   // level bases
+    uint32_t n_events;          // events minted this level
+    uint32_t* work;             // work-queue counters
+    // select / assign
+    uint32_t* flag_new;         // [n_events]
+    uint32_t* flag_rep;         // [n_events] then exclusive scan
+    uint32_t* flag_front;       // [n_events] then exclusive scan
+    uint32_t* scan_new;         // [n_events] exclusive scan of flag_new
+    uint32_t state_base;
+    uint32_t* new_state_event;  // [n_new] event of each new state
+    uint32_t* next_frontier;
+    uint32_t* level_max;        // [2] max ne, max nocc over new states
+    // branchial
+    uint32_t* bcount;           // [F]
+    uint32_t* boff;             // [F+1]
+    uint32_t* bpairs;           // output pairs (a, b)
+    uint32_t bbase;             // pair index base
+};
+
+// Per-warp shared-memory carve-up, sized on the host from the level's largest state.
+struct Layout {
+    uint32_t NE, NOCC, CNE, CNOCC, V, W, NBR;
+    uint32_t o_cur, o_nxt, o_csum, o_ccnt, o_nbr;                  // u64
+    uint32_t o_peid, o_occ, o_ooff, o_nbo, o_deg, o_nn, o_comp;     // u32
+    uint32_t o_cand, o_taken, o_misc;                               // u32
+    uint32_t o_pevo, o_vloc, o_cvo, o_bind, o_match, o_mdepth;      // u16
+    uint32_t o_pear, o_car;                                         // u8
+    uint32_t o_rule;                                                // DevRule
+    uint32_t bytes;
+};
+
+}  // namespace hgx

@@ -1,0 +1,171 @@
+/*
+ * hgx.h -- C ABI of the B200-native multiway evolution step.
+ *
+ * Plain pointers and sizes only; no C++ or torch types cross this boundary, and no exception
+ * does either: every entry point returns an hgx_status, and hgx_last_error() gives the
+ * message of the last failure on the calling thread.
+ *
+ * Each entry point names the reference interface it replaces (paths inside the reference
+ * project). The evolution it computes is the reference engine's multiway step in WL mode:
+ * states are identified by the shared WL canonical hash, events are every rule application
+ * of every expanded state, causal edges are (producer, consumer, edge) triples, branchial
+ * edges are event pairs of one input state that consumed a common edge.
+ *
+ * Blob encodings (uint32 arrays):
+ *   rule   [n_lhs, (arity, var...)*n_lhs, n_rhs, (arity, var...)*n_rhs]   vars < 32, arity 1..16
+ *   rules  [n_rules, rule...]
+ *   roots  [n_roots, per root: n_edges, (arity, vertex...)*n_edges]
+ *
+ * Threading: one host thread drives one engine at a time; distinct engines are independent.
+ */
+#ifndef HGX_H
+#define HGX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HGX_API __attribute__((visibility("default")))
+#else
+#define HGX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hgx_status {
+    HGX_OK = 0,
+    HGX_ERR_INVALID = 1,    /* malformed rule / state / argument (reference: std::length_error,
+                               std::invalid_argument from RuleBuilder and evolve) */
+    HGX_ERR_CUDA = 2,       /* CUDA driver/runtime failure (reference: HG_CUDA_CHECK throw) */
+    HGX_ERR_CAPACITY = 3,   /* a device capacity was exceeded (reference: ErrorKind overflow) */
+    HGX_ERR_NO_DEVICE = 4,  /* no CUDA device: there is no CPU fallback */
+    HGX_ERR_INTERNAL = 5
+} hgx_status;
+
+typedef struct hgx_engine hgx_engine;
+typedef struct hgx_result hgx_result;
+
+/* Options (hgx_engine_set_option). */
+typedef enum hgx_option {
+    /* ParallelEvolutionEngine::set_explore_from_canonical_states_only
+       (hypergraph/include/hypergraph/parallel_evolution.hpp:926): 1 = expand each WL class
+       once, at its shortest depth; 0 = full multiway (every raw state expanded). */
+    HGX_OPT_QUOTIENT = 0,
+    /* set_max_states (parallel_evolution.hpp:764): 0 = unlimited. */
+    HGX_OPT_MAX_STATES = 1,
+    /* set_transitive_reduction (parallel_evolution.hpp:781). Only 0 is accepted. */
+    HGX_OPT_TRANSITIVE_REDUCTION = 2,
+    /* RecordSet::causal / ::branchial (common/include/hgcommon/core.hpp:128-155). */
+    HGX_OPT_RECORD_CAUSAL = 3,
+    HGX_OPT_RECORD_BRANCHIAL = 4,
+    /* EvolveInput::edge_identity (gpu/include/hg_gpu/evolve.hpp:36): read back every state's
+       edge record (ids, arities, vertices). */
+    HGX_OPT_KEEP_STATE_EDGES = 5,
+    /* 1 = record per-stage device times (CUDA events on the engine stream). */
+    HGX_OPT_TIMING = 6
+} hgx_option;
+
+/* One evolution of a batch or a served request. */
+typedef struct hgx_job {
+    const uint32_t* rules;     /* rules blob */
+    size_t rules_len;
+    const uint32_t* roots;     /* roots blob */
+    size_t roots_len;
+    uint32_t steps;
+    uint32_t quotient;         /* as HGX_OPT_QUOTIENT */
+    uint64_t max_states;       /* as HGX_OPT_MAX_STATES */
+} hgx_job;
+
+/* Counts (hgx_result_count). */
+typedef enum hgx_count {
+    HGX_COUNT_STATES = 0,        /* states recorded: raw states (full) / class reps (quotient) */
+    HGX_COUNT_EVENTS = 1,        /* Hypergraph::num_events (hypergraph.hpp:749) */
+    HGX_COUNT_CLASSES = 2,       /* distinct WL canonical hashes (num_canonical_states, :694) */
+    HGX_COUNT_CAUSAL = 3,        /* causal triples (CausalGraph::get_causal_edges) */
+    HGX_COUNT_BRANCHIAL = 4,     /* branchial pairs (CausalGraph::get_branchial_edges) */
+    HGX_COUNT_TRUNCATED = 5,     /* 1 when a state cap stopped the evolution */
+    HGX_COUNT_CONSUMED = 6,      /* total consumed-edge entries over all events */
+    HGX_COUNT_STATE_EDGES = 7,   /* total edge entries over all state records */
+    HGX_COUNT_STATE_VERTS = 8,   /* total vertex entries over all state records */
+    HGX_COUNT_RAW_STATES = 9     /* Hypergraph::num_states (hypergraph.hpp:567): roots + events */
+} hgx_count;
+
+/* Arrays (hgx_result_copy); element type and length in brackets. */
+typedef enum hgx_array {
+    HGX_ARR_STATE_HASH = 0,      /* [u64 x STATES] WL canonical hash (CanonicalState::canonical_hash) */
+    HGX_ARR_STATE_DEPTH = 1,     /* [u32 x STATES] */
+    HGX_ARR_EVENTS = 2,          /* [u32 x EVENTS*4] (input state, output state, rule, step) */
+    HGX_ARR_CAUSAL = 3,          /* [u32 x CAUSAL*3] (producer event, consumer event, edge) */
+    HGX_ARR_BRANCHIAL = 4,       /* [u32 x BRANCHIAL*2] (event a, event b), a < b */
+    HGX_ARR_EVENT_CONS_OFF = 5,  /* [u32 x EVENTS+1] */
+    HGX_ARR_EVENT_CONS = 6,      /* [u32 x CONSUMED] consumed edge ids, pattern order */
+    HGX_ARR_EVENT_PROD = 7,      /* [u32 x EVENTS*2] (first produced edge id, count) */
+    HGX_ARR_STATE_EDGE_OFF = 8,  /* [u32 x STATES+1] (needs HGX_OPT_KEEP_STATE_EDGES) */
+    HGX_ARR_STATE_EDGE_IDS = 9,  /* [u32 x STATE_EDGES] */
+    HGX_ARR_STATE_ARITY = 10,    /* [u32 x STATE_EDGES] */
+    HGX_ARR_STATE_VERT_OFF = 11, /* [u32 x STATES+1] */
+    HGX_ARR_STATE_VERTS = 12     /* [u32 x STATE_VERTS] */
+} hgx_array;
+
+/* Message of the last failure on this thread ("" if none). */
+HGX_API const char* hgx_last_error(void);
+
+/* Library version string. */
+HGX_API const char* hgx_version(void);
+
+/* Replaces ParallelEvolutionEngine(Hypergraph*, num_threads)
+   (hypergraph/include/hypergraph/parallel_evolution.hpp:743) and
+   hg_gpu::Engine(EngineConfig) / PersistentEvolver (gpu/include/hg_gpu/evolve.hpp:435, :466):
+   device state that persists across evolve calls. */
+HGX_API hgx_status hgx_engine_create(int device, hgx_engine** out);
+HGX_API void hgx_engine_destroy(hgx_engine* engine);
+
+/* Replaces make_rule(i).lhs(...).rhs(...).build() (hypergraph/include/hypergraph/pattern.hpp:213)
+   followed by ParallelEvolutionEngine::add_rule (parallel_evolution.hpp:756). */
+HGX_API hgx_status hgx_engine_add_rule(hgx_engine* engine, const uint32_t* rule, size_t len);
+HGX_API hgx_status hgx_engine_clear_rules(hgx_engine* engine);
+
+/* Replaces the ParallelEvolutionEngine setters named on each hgx_option. */
+HGX_API hgx_status hgx_engine_set_option(hgx_engine* engine, hgx_option opt, uint64_t value);
+
+/* Replaces ParallelEvolutionEngine::evolve(initial_edges, steps) and its multi-root overload
+   (parallel_evolution.hpp:1009, :1041), and hg_gpu::evolve(EvolveInput) (evolve.hpp:368). */
+HGX_API hgx_status hgx_evolve(hgx_engine* engine, const uint32_t* roots, size_t roots_len, uint32_t steps,
+                      hgx_result** out);
+
+/* Many independent evolutions in one level-synchronous pipeline: one launch per stage per
+   level for all of them. The batched form of hg_gpu::evolve (evolve.hpp:368); results are
+   identical to evolving each job alone. out[i] receives job i's result. */
+HGX_API hgx_status hgx_evolve_batch(hgx_engine* engine, const hgx_job* jobs, uint32_t n_jobs,
+                            hgx_result** out);
+
+/* Continuous batching. Replaces the strictly serial request loop of
+   paclet_source/hg_evolve_main.cpp:99 (run_serve): requests are admitted between levels and
+   advance together, each at its own depth. */
+HGX_API hgx_status hgx_serve_reset(hgx_engine* engine);
+HGX_API hgx_status hgx_serve_admit(hgx_engine* engine, const hgx_job* job, uint32_t* evolution_id);
+HGX_API hgx_status hgx_serve_step(hgx_engine* engine, int* still_active);
+HGX_API hgx_status hgx_serve_take_finished(hgx_engine* engine, uint32_t* ids, uint32_t cap, uint32_t* n);
+HGX_API hgx_status hgx_serve_collect(hgx_engine* engine, uint32_t evolution_id, hgx_result** out);
+HGX_API hgx_status hgx_serve_device_bytes(hgx_engine* engine, uint64_t* bytes);
+
+/* Result accessors. Replace Hypergraph::num_states / num_events / num_canonical_states
+   (hypergraph/include/hypergraph/hypergraph.hpp:567, :749, :694),
+   CausalGraph::get_causal_edges / get_branchial_edges and the hg_gpu::EvolveResult vectors
+   (gpu/include/hg_gpu/evolve.hpp:161-173). */
+HGX_API uint64_t hgx_result_count(const hgx_result* result, hgx_count what);
+HGX_API hgx_status hgx_result_copy(const hgx_result* result, hgx_array what, void* dst, size_t dst_bytes);
+HGX_API void hgx_result_free(hgx_result* result);
+
+/* Device time per stage of the last evolve call, in milliseconds (HGX_OPT_TIMING must be on):
+   out[0..7] = count, scan, expand, select, materialize, branchial, roots, total.
+   launches: kernels launched by the call. */
+HGX_API hgx_status hgx_engine_stage_times(hgx_engine* engine, double* out_ms, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HGX_H */

@@ -1,0 +1,106 @@
+"""Parity of the CUDA path (through the C-ABI) with the oracle and the reference's fixtures.
+
+Integer work throughout: every comparison is exact (WL hashes bit for bit, key multisets equal).
+"""
+import random
+
+import numpy as np
+import pytest
+
+import cases
+from hypergraphrewritingengine_b200 import workloads as W
+from oracle import pyoracle
+from parity import assert_matches_golden, assert_same, norm_gpu, norm_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_state(rng, n_edges, n_verts, arities):
+    return [[rng.randint(1, n_verts) for _ in range(rng.choice(arities))] for _ in range(n_edges)]
+
+
+def test_root_wl_hashes_match_oracle(engine):
+    """steps=0: the device hashes the roots only (several roots per call, uneven sizes)."""
+    rng = random.Random(11)
+    roots = []
+    for i in range(300):
+        ne = rng.choice([1, 2, 3, 5, 8, 13, 20, 40, 90, 200])
+        roots.append(_random_state(rng, ne, max(2, ne // 2 + rng.randint(0, 4)),
+                                   arities=rng.choice([(2,), (3,), (2, 3), (1, 2, 4), (4, 5)])))
+    res = engine.evolve([([[0, 1]], [[0, 1]])], roots, 0, quotient=False)
+    want = [pyoracle.wl_hash(r) for r in roots]
+    assert [int(h) for h in res.state_hash] == want
+
+
+FULL = {name: (rules, roots, steps) for name, rules, roots, steps in cases.all_full_cases()}
+
+
+@pytest.mark.parametrize("name", sorted(FULL))
+def test_full_multiway_matches_reference_fixtures(engine, golden, name):
+    rules, roots, steps = FULL[name]
+    res = engine.evolve(rules, roots, steps, quotient=False)
+    assert_matches_golden(norm_gpu(res), golden["full"][name], name)
+
+
+QUOT = {name: (rules, roots, steps) for name, rules, roots, steps in cases.all_quotient_cases()}
+
+
+@pytest.mark.parametrize("name", sorted(QUOT))
+def test_quotient_matches_oracle(engine, name):
+    rules, roots, steps = QUOT[name]
+    res = engine.evolve(rules, roots, steps, quotient=True)
+    ref = pyoracle.evolve(rules, roots, steps, quotient=True)
+    assert_same(norm_gpu(res), norm_oracle(ref), name)
+
+
+@pytest.mark.parametrize("ev", [W.config2(6), W.config2(7), W.config3(5)], ids=lambda e: e.name)
+def test_named_quotient_workloads_match_oracle(engine, ev):
+    res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+    ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+    assert_same(norm_gpu(res), norm_oracle(ref), ev.name)
+    assert res.num_classes == ref["classes"]
+
+
+def test_state_cap_matches_oracle(engine):
+    for cap in (1, 7, 100, 1000):
+        res = engine.evolve([cases.C2_RULE], [cases.C2_INIT], 6, quotient=True, max_states=cap)
+        ref = pyoracle.evolve([cases.C2_RULE], [cases.C2_INIT], 6, quotient=True, max_states=cap)
+        assert res.truncated == ref["truncated"]
+        assert_same(norm_gpu(res), norm_oracle(ref), f"cap {cap}")
+    for cap in (5, 300):
+        res = engine.evolve([cases.C1_RULE], [cases.C1_INIT], 4, quotient=False, max_states=cap)
+        ref = pyoracle.evolve([cases.C1_RULE], [cases.C1_INIT], 4, quotient=False, max_states=cap)
+        assert_same(norm_gpu(res), norm_oracle(ref), f"full cap {cap}")
+
+
+def test_batch_matches_single_and_oracle(engine):
+    evs = W.config4(n=48, max_states=512)
+    batch = engine.evolve_batch(evs)
+    for ev, res in zip(evs, batch):
+        single = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+        ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+        a, b, c = norm_gpu(res), norm_gpu(single), norm_oracle(ref)
+        assert_same(a, b, ev.name)
+        assert_same(a, c, ev.name)
+        assert res.truncated == ref["truncated"]
+
+
+def test_state_edge_records_are_the_oracle_states(engine):
+    """Every recorded state's edges hash (on the CPU) to the WL hash the device reported."""
+    res = engine.evolve([cases.C3_RULE], [cases.C3_INIT], 4, quotient=True)
+    for s in range(0, res.num_states, 7):
+        assert pyoracle.wl_hash(res.state_edges(s)) == int(res.state_hash[s])
+
+
+def test_reference_shaped_api(engine):
+    from hypergraphrewritingengine_b200 import Hypergraph, ParallelEvolutionEngine, make_rule
+    hg = Hypergraph()
+    eng = ParallelEvolutionEngine(hg, 8)
+    eng.add_rule(make_rule(0).lhs([0, 1]).lhs([1, 2]).rhs([0, 1]).rhs([1, 2]).rhs([2, 0]).build())
+    eng.set_transitive_reduction(False)
+    eng.evolve([[1, 2], [2, 3], [3, 1]], 5)
+    assert hg.num_states() == 22204
+    assert hg.num_events() == 22203
+    assert hg.num_canonical_states() == 20
+    assert hg.causal_graph().num_causal_edges() == 42816
+    assert hg.causal_graph().num_branchial_edges() == 78045
