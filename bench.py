@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the multiway evolution step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A "step" is one complete WL-quotient evolution of the single large workload: rule
+{{x,y},{x,z}} -> {{x,z},{x,w},{y,w},{z,w}} (w fresh) from {{1,1},{1,1}}, 8 levels, WL dedup, capped
+at 2,000,000 unique states, causal + branchial relations recorded.  Inputs are synthetic (the
+rule and the initial state), generated in-process.
+
+* value   events/s over all ranks, device-resident (the result stays in HBM; counts read back),
+          timed with CUDA events on the engine's stream, L2 flushed (256 MB write) before each step.
+* e2e     the same metric through the C-ABI call a user makes (hgx_evolve with host buffers):
+          rule/state blobs copied in and the whole result (states, events, causal, branchial)
+          copied out every step, timed on the host clock around the call.
+* roofline  the dominant kernel (k_expand: join + rewrite + WL hash + dedup insert, fused), its
+          algorithmic bytes per launch over its CUDA-event launch time, against the measured HBM
+          copy bandwidth (MEASURED_PEAKS.json).
+* cpu_baseline  the reference CPU engine (oracle/_ref/hgref, compiled from the reference's own
+          sources) on a bounded sample of the same workload: its quotient exploration (IR-keyed;
+          the reference has no WL-keyed quotient) to 6 levels, all host threads.
+* batched  1024 random evolutions (seeded generator) in one batched pipeline vs. the plain path
+          (one evolution per call), same GPU, identical per-evolution outputs.
+
+Multi-GPU: the path does not shard (one evolution per device); --gpus N runs N replicas under
+torchrun and reports the aggregate with the max-over-ranks time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "events/s (WL-quotient multiway evolution; unique states/s alongside)"
+WORKLOAD = ("c2: {{x,y},{x,z}}->{{x,z},{x,w},{y,w},{z,w}} from {{1,1},{1,1}}, 8 steps, WL dedup, "
+            "cap 2,000,000 unique states, causal+branchial recorded")
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def profile_traffic():
+    """dram bytes per k_expand launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "k_expand.c2-8step.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_per_launch_bytes"):
+            return float(line.split("=")[1].split()[0])
+    return None
+
+
+def cpu_baseline_reference(threads: int | None = None, levels: int = 6):
+    """Reference CPU engine on a bounded sample (quotient exploration to `levels` levels)."""
+    from hypergraphrewritingengine_b200 import workloads as W
+    from oracle import pyoracle
+    ev = W.config2(levels)
+    threads = threads or os.cpu_count() or 1
+    if os.path.exists(pyoracle.REF_BIN):
+        r = pyoracle.run_reference(ev.rules, ev.roots, ev.steps, quotient=True, threads=threads,
+                                   timeout=600)
+        return {"value": r["events"] / (r["ms"] / 1e3), "unit": "events/s", "cores": threads,
+                "kind": "reference",
+                "sample": f"reference engine (oracle/_ref) quotient exploration (IR-keyed) of the "
+                          f"same rule/state to {levels} levels: {r['events']} events, "
+                          f"{r['canonical_states']} classes in {r['ms']:.0f} ms"}
+    t = time.perf_counter()
+    r = pyoracle.evolve(ev.rules, ev.roots, 7, quotient=True)
+    dt = time.perf_counter() - t
+    return {"value": len(r["events"]) / dt, "unit": "events/s", "cores": 1, "kind": "port",
+            "sample": f"oracle restatement, WL quotient to 7 levels: {len(r['events'])} events in {dt:.1f} s"}
+
+
+def run_reference_arm(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline_reference(cores)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.mean(vals)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "events/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " (reference: bounded 6-level sample, IR-keyed quotient)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched comparison")
+    ap.add_argument("--levels", type=int, default=8)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from hypergraphrewritingengine_b200 import Engine, encode_roots, encode_rules
+    from hypergraphrewritingengine_b200 import workloads as W
+
+    ev = W.config2(args.levels)
+    eng = Engine(local)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", local))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")   # 256 MB > 126 MB L2
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        counts = eng.counts(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+
+    # ---- timed region (device-resident), stage timing on (event records, no syncs)
+    from hypergraphrewritingengine_b200 import api
+    eng.set_option(api.OPT_TIMING, 1)
+    expand_ms = 0.0
+    expand_launches = 0
+    stage_bytes = hbm_bytes = children = rounds = 0
+    launches = 0
+    step_ms = []
+    with ClockSampler(local) as clocks:
+        barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            counts = eng.counts(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            st, nl = eng.stage_times()
+            xs = eng.expand_stats()
+            expand_ms += st["expand"]
+            expand_launches += xs["launches"]
+            stage_bytes += xs["stage_bytes"]
+            hbm_bytes += xs["hbm_bytes"]
+            children += xs["children"]
+            rounds += xs["wl_rounds"]
+            launches += nl
+        barrier()
+    eng.set_option(api.OPT_TIMING, 0)
+    t_ms = sum(step_ms) / len(step_ms)
+    if dist is not None:
+        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    events = counts["events"]
+    states = counts["states"]
+    value = world * events / (t_ms / 1e3)
+
+    # ---- e2e through the C-ABI with host buffers
+    rb, sb = encode_rules(ev.rules), encode_roots(ev.roots)
+    h2d = rb.nbytes + sb.nbytes
+    e2e_s = []
+    d2h = 0
+    for i in range(1 + max(1, args.steps // 2)):
+        barrier()
+        t0 = time.perf_counter()
+        res = eng.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+        dt = time.perf_counter() - t0
+        if i:
+            e2e_s.append(dt)
+        d2h = res.bytes()
+        assert res.num_events == events and res.num_states == states
+    e2e_t = max(e2e_s) if dist is None else e2e_s[-1]
+    if dist is not None:
+        t = torch.tensor([statistics.mean(e2e_s)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    else:
+        e2e_t = statistics.mean(e2e_s)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = peaks()
+    per_launch_bytes = stage_bytes / max(expand_launches, 1)
+    per_launch_s = expand_ms / 1e3 / max(expand_launches, 1)
+    achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else None
+    traffic = profile_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded rule and initial state; no dataset)",
+        "config": {"workload": WORKLOAD, "levels": args.levels, "parallelism": f"replicas x{world}",
+                   "l2": "flushed before every step (256 MB device write)",
+                   "events_per_step": events, "unique_states_per_step": states,
+                   "classes": counts["classes"], "causal_per_step": counts["causal"],
+                   "branchial_per_step": counts["branchial"], "truncated_at_cap": counts["truncated"]},
+        "unique_states_per_s": world * states / (t_ms / 1e3),
+        "e2e": {"value": world * events / e2e_t, "unit": "events/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},
+        "roofline": {"bound": "hbm", "kernel": "k_expand", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "traffic": traffic, "peak_kind": f"{peak_kind} (copy bandwidth)",
+                     "algorithmic_bytes_per_launch": per_launch_bytes,
+                     "fused_hbm_bytes_per_launch": hbm_bytes / max(expand_launches, 1),
+                     "launch_ms": per_launch_s * 1e3, "launches": expand_launches,
+                     "children_hashed": children, "wl_rounds": rounds,
+                     "stage_ms_last_step": {k: round(v, 3) for k, v in st.items()}},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if world == 1:
+        line["cpu_baseline"] = cpu_baseline_reference()
+        if not args.no_extras:
+            line["batched"] = batched_vs_plain(eng)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def batched_vs_plain(eng, n=1024):
+    """1024 random evolutions: one batched pipeline vs. one call per evolution (device-resident,
+    counts read back), same outputs required."""
+    import torch
+    from hypergraphrewritingengine_b200 import api
+    from hypergraphrewritingengine_b200 import workloads as W
+    evs = W.config4(n=n)
+    jobs, keep = eng.make_jobs(evs)
+    eng.set_option(api.OPT_READBACK, 0)
+    try:
+        # warm-up both paths
+        out = (api.ctypes.c_void_p * n)()
+        api._check(eng._L.hgx_evolve_batch(eng._h, jobs, n, out))
+        for i in range(n):
+            eng._L.hgx_result_free(out[i])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        api._check(eng._L.hgx_evolve_batch(eng._h, jobs, n, out))
+        t_batch = time.perf_counter() - t0
+        batch_counts = []
+        for i in range(n):
+            batch_counts.append(tuple(int(eng._L.hgx_result_count(out[i], w)) for w in range(6)))
+            eng._L.hgx_result_free(out[i])
+        t0 = time.perf_counter()
+        plain_counts = []
+        for i in range(n):
+            one = (api.ctypes.c_void_p * 1)()
+            api._check(eng._L.hgx_evolve_batch(eng._h, api.ctypes.byref(jobs[i]), 1, one))
+            plain_counts.append(tuple(int(eng._L.hgx_result_count(one[0], w)) for w in range(6)))
+            eng._L.hgx_result_free(one[0])
+        t_plain = time.perf_counter() - t0
+    finally:
+        eng.set_option(api.OPT_READBACK, 1)
+    events = sum(c[1] for c in batch_counts)
+    states = sum(c[0] for c in batch_counts)
+    return {"workload": f"c4: {n} random evolutions (seed 0x5EED; LHS 2-3, RHS 3-4, arity 2|3, "
+                        "0-2 fresh, 4-64 initial edges, 3-7 steps, WL quotient, cap 4096 states each)",
+            "events": events, "unique_states": states,
+            "batched_events_per_s": events / t_batch, "plain_events_per_s": events / t_plain,
+            "batched_ms": t_batch * 1e3, "plain_ms": t_plain * 1e3,
+            "speedup_vs_plain": t_plain / t_batch,
+            "identical_outputs": batch_counts == plain_counts}
+
+
+if __name__ == "__main__":
+    main()

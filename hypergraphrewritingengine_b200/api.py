@@ -32,7 +32,7 @@ LIB_PATH = os.path.join(HERE, "libhgx.so")
 
 HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_ERR_INTERNAL = range(6)
 (OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
- OPT_KEEP_STATE_EDGES, OPT_TIMING) = range(7)
+ OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK) = range(8)
 (COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
  COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES) = range(10)
 (ARR_STATE_HASH, ARR_STATE_DEPTH, ARR_EVENTS, ARR_CAUSAL, ARR_BRANCHIAL, ARR_EVENT_CONS_OFF,
@@ -45,7 +45,8 @@ EXPORTS = (
     "hgx_engine_add_rule", "hgx_engine_clear_rules", "hgx_engine_set_option", "hgx_evolve",
     "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_step",
     "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_device_bytes", "hgx_result_count",
-    "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times",
+    "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
+    "hgx_engine_stream",
 )
 
 
@@ -95,6 +96,8 @@ def load_library(path: str = LIB_PATH):
         "hgx_result_copy": ([vp, ctypes.c_int, vp, ctypes.c_size_t], ctypes.c_int),
         "hgx_result_free": ([vp], None),
         "hgx_engine_stage_times": ([vp, ctypes.POINTER(ctypes.c_double), u64p], ctypes.c_int),
+        "hgx_engine_expand_stats": ([vp, u64p], ctypes.c_int),
+        "hgx_engine_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -328,6 +331,40 @@ class Engine:
         b = ctypes.c_uint64()
         _check(self._L.hgx_serve_device_bytes(self._h, ctypes.byref(b)))
         return int(b.value)
+
+    def expand_stats(self):
+        out = (ctypes.c_uint64 * 5)()
+        _check(self._L.hgx_engine_expand_stats(self._h, out))
+        return dict(zip(("stage_bytes", "hbm_bytes", "children", "wl_rounds", "launches"), list(out)))
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(self._L.hgx_engine_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def counts(self, rules, roots, steps, quotient=True, max_states=0):
+        """Evolve with the result left on the device; returns the counts only."""
+        self.set_option(OPT_READBACK, 0)
+        try:
+            L = self._L
+            _check(L.hgx_engine_clear_rules(self._h))
+            for lhs, rhs in rules:
+                b = encode_rule(lhs, rhs)
+                _check(L.hgx_engine_add_rule(self._h, _u32p(b), len(b)))
+            self.set_option(OPT_QUOTIENT, quotient)
+            self.set_option(OPT_MAX_STATES, max_states)
+            rb = encode_roots(roots)
+            out = ctypes.c_void_p()
+            _check(L.hgx_evolve(self._h, _u32p(rb), len(rb), int(steps), ctypes.byref(out)))
+            try:
+                cnt = lambda w: int(L.hgx_result_count(out, w))  # noqa: E731
+                return {"states": cnt(COUNT_STATES), "events": cnt(COUNT_EVENTS),
+                        "classes": cnt(COUNT_CLASSES), "causal": cnt(COUNT_CAUSAL),
+                        "branchial": cnt(COUNT_BRANCHIAL), "truncated": bool(cnt(COUNT_TRUNCATED))}
+            finally:
+                L.hgx_result_free(out)
+        finally:
+            self.set_option(OPT_READBACK, 1)
 
     def stage_times(self):
         out = (ctypes.c_double * 8)()

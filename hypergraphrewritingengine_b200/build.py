@@ -18,6 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhgx.so")
 SOURCES = ["engine.cu", "capi.cpp"]
 DEPS = ["engine.cu", "capi.cpp", "engine.hpp", "step_kernels.cu", "step_kernels.cuh", "common.cuh",
+        "lane_wl.cuh",
         os.path.join("..", "..", "include", "hgx.h")]
 
 

@@ -202,6 +202,7 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
         case HGX_OPT_RECORD_BRANCHIAL: e->opt.branchial = value != 0; return HGX_OK;
         case HGX_OPT_KEEP_STATE_EDGES: e->opt.keep_state_edges = value != 0; return HGX_OK;
         case HGX_OPT_TIMING: e->engine.set_timing(value != 0); return HGX_OK;
+        case HGX_OPT_READBACK: e->opt.readback = value != 0; return HGX_OK;
     }
     return fail(HGX_ERR_INVALID, "unknown option");
 }
@@ -288,6 +289,17 @@ hgx_status hgx_serve_device_bytes(hgx_engine* e, uint64_t* bytes) {
 uint64_t hgx_result_count(const hgx_result* res, hgx_count what) {
     if (!res) return 0;
     const auto& r = res->r;
+    if (r.counts_only) {
+        switch (what) {
+            case HGX_COUNT_STATES: return r.n_states;
+            case HGX_COUNT_EVENTS: return r.n_events;
+            case HGX_COUNT_CLASSES: return r.num_classes;
+            case HGX_COUNT_CAUSAL: return r.n_causal;
+            case HGX_COUNT_BRANCHIAL: return r.n_branchial;
+            case HGX_COUNT_TRUNCATED: return r.truncated ? 1 : 0;
+            default: return 0;
+        }
+    }
     switch (what) {
         case HGX_COUNT_STATES: return r.state_hash.size();
         case HGX_COUNT_EVENTS: return r.ev_in.size();
@@ -342,6 +354,23 @@ hgx_status hgx_engine_stage_times(hgx_engine* e, double* out, uint64_t* launches
     out[6] = t.roots;
     out[7] = t.count + t.scan + t.expand + t.select + t.materialize + t.branchial + t.roots;
     if (launches) *launches = t.launches;
+    return HGX_OK;
+}
+
+hgx_status hgx_engine_expand_stats(hgx_engine* e, uint64_t* out) {
+    if (!e || !out) return fail(HGX_ERR_INVALID, "null argument");
+    const auto& t = e->engine.times();
+    out[0] = t.expand_bytes;
+    out[1] = t.expand_hbm_bytes;
+    out[2] = t.children;
+    out[3] = t.wl_rounds;
+    out[4] = t.expand_launches;
+    return HGX_OK;
+}
+
+hgx_status hgx_engine_stream(hgx_engine* e, void** stream) {
+    if (!e || !stream) return fail(HGX_ERR_INVALID, "null argument");
+    *stream = reinterpret_cast<void*>(e->engine.stream());
     return HGX_OK;
 }
 

@@ -28,6 +28,11 @@ constexpr int kMaxArity = 16;
 constexpr int kMaxVars = 32;
 constexpr int kMaxSideVars = 64;   // total positions over one rule side (16 edges x 4 avg)
 
+// Lane-per-child WL: a parent with at most kLaneEMax edges whose children have at most
+// kLaneVMax vertices is expanded with one child per lane.
+constexpr int kLaneVMax = 32;
+constexpr int kLaneEMax = 64;
+
 HGX_HD uint64_t fnv(uint64_t h, uint64_t x) { return (h ^ x) * kFnvPrime; }
 
 HGX_HD uint64_t smix(uint64_t z) {

@@ -48,7 +48,8 @@ struct DVec {
 };
 
 struct RuleMax {
-    uint32_t rhs = 0, rhs_total = 0, fresh = 0, arity = 1, grow_e = 0, grow_o = 0, stride = 1;
+    uint32_t rhs = 0, rhs_total = 0, fresh = 0, arity = 1, grow_e = 0, grow_o = 0, stride = 1,
+             lhs = 1;
 };
 
 DevRule pack_rule(const RuleSpec& r) {
@@ -162,6 +163,14 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, bool wl) {
     L.o_pear = take(NE, 1);
     if (wl) L.o_car = take(L.CNE, 1);
     L.o_rule = take(sizeof(DevRule), 4);
+    if (wl) {
+        L.SB = rm.lhs + rm.rhs_total;
+        L.o_poff = take(2 * (kLaneVMax + 1), 2);
+        L.o_pocc = take(2 * NOCC, 2);
+        L.o_pnn = take(2 * kLaneVMax, 2);
+        L.o_pdeg = take(2 * kLaneVMax, 2);
+        L.o_batch = take(32 * L.SB, 1);
+    }
     L.bytes = align_up(off, 16);
     return L;
 }
@@ -202,6 +211,7 @@ struct Engine::Impl {
     DVec<uint32_t> frontier, next_frontier, counts, item_ev, item_cons, item_prod, item_fresh;
     DVec<uint32_t> work, flag_new, scan_new, flag_rep, flag_front, new_state_event, level_max;
     DVec<uint32_t> bcount, boff, bpairs, scan_sums, sync_buf, root_ids;
+    DVec<unsigned long long> stats, totals;
 
     // host mirrors
     std::vector<DevRule> h_rules;
@@ -235,6 +245,7 @@ struct Engine::Impl {
         work.ensure(8, 0, st);
         level_max.ensure(4, 0, st);
         sync_buf.ensure(16, 0, st);
+        stats.ensure(4, 0, st);
         reset();
     }
 
@@ -258,11 +269,14 @@ struct Engine::Impl {
         tab_keys.release(st);
         evo_classes.release(st);
         evo_states.release(st);
+        stats.release(st);
+        totals.release(st);
         rules.release(st);
         evos.release(st);
         cudaStreamSynchronize(st);
         cudaEventDestroy(ev_a);
         cudaEventDestroy(ev_b);
+        for (auto e : ev_pool) cudaEventDestroy(e);
         cudaStreamDestroy(st);
     }
 
@@ -281,6 +295,9 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
         times = StageTimes{};
         launches = 0;
+        pending.clear();
+        ev_used = 0;
+        HGX_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 4 * sizeof(unsigned long long), st));
     }
 
     DevPtrs ptrs() const {
@@ -317,20 +334,47 @@ struct Engine::Impl {
         P.evo_first_ev = evo_first_ev.p;
         P.evo_stopped = evo_stopped.p;
         P.err = err.p;
+        P.stats = stats.p;
         return P;
     }
 
     // ---- small helpers ------------------------------------------------------------------
+    // Stage timing: CUDA events recorded on the engine stream, no host synchronisation; the
+    // pairs are resolved after the run's final synchronise (flush_times).
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    struct Pending { cudaEvent_t a, b; double* acc; };
+    std::vector<Pending> pending;
+    cudaEvent_t cur_a = nullptr;
+    cudaEvent_t next_event() {
+        if (ev_used == ev_pool.size()) {
+            cudaEvent_t e;
+            HGX_CUDA_CHECK(cudaEventCreate(&e));
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
     void tic() {
-        if (timing) HGX_CUDA_CHECK(cudaEventRecord(ev_a, st));
+        if (!timing) return;
+        cur_a = next_event();
+        HGX_CUDA_CHECK(cudaEventRecord(cur_a, st));
     }
     void toc(double& acc) {
         if (!timing) return;
-        HGX_CUDA_CHECK(cudaEventRecord(ev_b, st));
-        HGX_CUDA_CHECK(cudaEventSynchronize(ev_b));
-        float ms = 0;
-        HGX_CUDA_CHECK(cudaEventElapsedTime(&ms, ev_a, ev_b));
-        acc += ms;
+        cudaEvent_t b = next_event();
+        HGX_CUDA_CHECK(cudaEventRecord(b, st));
+        pending.push_back({cur_a, b, &acc});
+    }
+    void flush_times() {
+        if (pending.empty()) return;
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        for (const auto& p : pending) {
+            float ms = 0;
+            HGX_CUDA_CHECK(cudaEventElapsedTime(&ms, p.a, p.b));
+            *p.acc += ms;
+        }
+        pending.clear();
+        ev_used = 0;
     }
     void check_launch() {
         ++launches;
@@ -392,6 +436,7 @@ struct Engine::Impl {
             rm.rhs = std::max<uint32_t>(rm.rhs, pr.n_rhs);
             rm.rhs_total = std::max<uint32_t>(rm.rhs_total, pr.rhs_total);
             rm.fresh = std::max<uint32_t>(rm.fresh, pr.n_fresh);
+            rm.lhs = std::max<uint32_t>(rm.lhs, pr.n_lhs);
             for (uint32_t i = 0; i < pr.n_rhs; ++i) rm.arity = std::max<uint32_t>(rm.arity, pr.rhs_ar[i]);
             rm.grow_e = std::max<int>(rm.grow_e, int(pr.n_rhs) - int(pr.n_lhs));
             rm.grow_o = std::max<int>(rm.grow_o, int(pr.rhs_total) - int(pr.lhs_total));
@@ -579,6 +624,47 @@ struct Engine::Impl {
     void read_results(const std::vector<uint32_t>& which, const RunOptions& opt,
                       std::vector<EvolutionResult>& out);
 
+    // Counts only (results stay on the device).
+    void read_counts(const std::vector<uint32_t>& which, std::vector<EvolutionResult>& out) {
+        const size_t nevo = h_evos.size();
+        totals.ensure(3 * nevo, 0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(totals.p, 0, 3 * nevo * sizeof(unsigned long long), st));
+        k_evo_totals<<<grid_for(std::max<uint64_t>(n_events, n_bpairs), 256), 256, 0, st>>>(
+            ptrs(), static_cast<uint32_t>(n_events), bpairs.p, n_bpairs, totals.p);
+        check_launch();
+        std::vector<unsigned long long> tot(3 * nevo), cls(nevo), sts(nevo);
+        std::vector<uint32_t> stop(nevo);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(tot.data(), totals.p, tot.size() * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(cls.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(sts.data(), evo_states.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(stop.data(), evo_stopped.p, nevo * 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        out.assign(which.size(), EvolutionResult{});
+        for (size_t i = 0; i < which.size(); ++i) {
+            const uint32_t e = which[i];
+            EvolutionResult& r = out[i];
+            r.counts_only = true;
+            r.num_classes = cls[e];
+            r.n_states = sts[e];
+            r.n_events = tot[3 * e];
+            r.n_causal = tot[3 * e + 1];
+            r.n_branchial = tot[3 * e + 2];
+            r.truncated = stop[e] != 0;
+        }
+    }
+
+    void finish_times() {
+        flush_times();
+        unsigned long long sv[4];
+        HGX_CUDA_CHECK(cudaMemcpyAsync(sv, stats.p, sizeof(sv), cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        times.expand_bytes = sv[0];
+        times.expand_hbm_bytes = sv[1];
+        times.children = sv[2];
+        times.wl_rounds = sv[3];
+        times.launches = launches;
+    }
+
     // ---- one level for every evolution in the frontier ---------------------------------------
     bool level(const RunOptions& opt) {
         const uint32_t F = frontier_size;
@@ -691,6 +777,10 @@ struct Engine::Impl {
             tic();
             k_expand<<<se.grid, se.block, se.smem, st>>>(ptrs(), A, Le);
             check_launch();
+            if (n_cons_lv) {
+                k_cprod<<<grid_for(n_cons_lv, 256), 256, 0, st>>>(ptrs(), A.cons_base, n_cons_lv);
+                check_launch();
+            }
             toc(times.expand);
             ++times.expand_launches;
 
@@ -942,8 +1032,9 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
     for (const auto& s : specs) ids.push_back(I.admit(s));
     while (I.level(opt)) {}
     std::vector<EvolutionResult> out;
-    I.read_results(ids, opt, out);
-    I.times.launches = I.launches;
+    if (opt.readback) I.read_results(ids, opt, out);
+    else I.read_counts(ids, out);
+    I.finish_times();
     return out;
 }
 
@@ -957,7 +1048,8 @@ std::vector<uint32_t> Engine::take_finished() {
 }
 EvolutionResult Engine::collect(uint32_t evo, const RunOptions& opt) {
     std::vector<EvolutionResult> out;
-    impl_->read_results({evo}, opt, out);
+    if (opt.readback) impl_->read_results({evo}, opt, out);
+    else impl_->read_counts({evo}, out);
     return std::move(out[0]);
 }
 uint32_t Engine::active() const {

@@ -62,10 +62,15 @@ struct EvolutionResult {
     uint64_t num_classes = 0;
     bool truncated = false;
     std::vector<std::string> warnings;
+    // Set when the run kept its results on the device (RunOptions::readback == false): the
+    // arrays above are empty and only these counts are filled.
+    bool counts_only = false;
+    uint64_t n_states = 0, n_events = 0, n_causal = 0, n_branchial = 0;
 };
 
 struct RunOptions {
     bool keep_state_edges = true;    // read back every state's edge record
+    bool readback = true;            // false: leave results on the device, return counts
     bool causal = true;
     bool branchial = true;
 };
@@ -76,7 +81,10 @@ struct StageTimes {
            roots = 0, total = 0;
     uint64_t launches = 0;   // kernels this engine launched during the run
     uint64_t expand_launches = 0;
-    uint64_t expand_bytes = 0;   // algorithmic bytes of the expand kernel (see DESIGN)
+    uint64_t expand_bytes = 0;       // per-stage algorithmic bytes of the expand kernel
+    uint64_t expand_hbm_bytes = 0;   // bytes the fused expand kernel must move to/from HBM
+    uint64_t children = 0;           // children built and WL-hashed
+    uint64_t wl_rounds = 0;          // refinement rounds over all children
 };
 
 class Engine {

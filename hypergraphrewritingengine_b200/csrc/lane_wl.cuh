@@ -1,0 +1,219 @@
+// Lane-per-child WL canonical hash (one thread hashes one child against its parent).
+//
+// Host and device: the same function runs in the expand kernel and in the native unit test
+// (tests/native/lane_wl_test.cpp), which checks it against the oracle's WL hash on random
+// parents and matches.
+//
+// A child is given relative to its parent: the parent's edges (arity pear[e], vertex offset
+// pevo[e] into vloc), the parent's per-vertex occurrence lists in edge order (poff/pocc, entries
+// e << 4 | position), per-vertex degree pdeg and neighbour count pnn (sum of arity - 1), and a
+// slot holding the parent positions the match removes (pattern order) followed by the local
+// vertex ids of the produced edges (RHS order). Local ids: parent vertices [0, nvp), the n-th
+// fresh variable nvp + n. The child's edge order is the parent's minus the removed edges,
+// then the produced ones -- the order the reference hashes a state's edges in.
+//
+// The arithmetic restates common/include/hgcommon/wl_core.hpp:67-202 of the reference: initial
+// colour FNV(degree, sorted (arity, position) of the first `cap` occurrences), refinement by the
+// sorted multiset of fnv(colour(u), k) until the distinct-colour count stops changing (at most
+// 100 rounds), then the connected-component fold and FNV(n_v, n_e, vsum, esum, csum).
+#pragma once
+#include "common.cuh"
+
+namespace hgx {
+
+struct WlInfo {
+    uint32_t rounds, nv, nocc, nbr;   // refinement rounds run, vertices, occurrences, sum a(a-1)
+};
+
+HGX_HD void lane_isort64(uint64_t* a, uint32_t n) {
+    for (uint32_t i = 1; i < n; ++i) {
+        const uint64_t k = a[i];
+        uint32_t j = i;
+        while (j > 0 && a[j - 1] > k) { a[j] = a[j - 1]; --j; }
+        a[j] = k;
+    }
+}
+
+template <int VM>
+HGX_HD uint32_t lane_distinct(const uint64_t* cur, const uint16_t* deg, uint32_t V) {
+    uint32_t d = 0;
+    for (uint32_t v = 0; v < V; ++v) {
+        if (!deg[v]) continue;
+        bool first = true;
+        for (uint32_t u = 0; u < v && first; ++u)
+            if (deg[u] && cur[u] == cur[v]) first = false;
+        d += first ? 1u : 0u;
+    }
+    return d;
+}
+
+template <int VM, int NM>
+HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const uint16_t* vloc,
+                             const uint16_t* poff, const uint16_t* pocc, const uint16_t* pdeg,
+                             const uint16_t* pnn, uint32_t pne, uint32_t nvp, const DevRule& R,
+                             const uint8_t* slot, WlInfo& info) {
+    const uint8_t* rpos = slot;
+    const uint8_t* prodv = slot + R.n_lhs;
+    const uint32_t V = nvp + R.n_fresh;
+    const uint32_t ne = pne - R.n_lhs + R.n_rhs;
+    info.rounds = info.nv = info.nocc = info.nbr = 0;
+    if (ne == 0) return kEmptyStateHash;
+
+    uint64_t rmask = 0;
+    for (uint32_t k = 0; k < R.n_lhs; ++k) rmask |= 1ull << rpos[k];
+    uint16_t deg[VM], nn[VM];
+    for (uint32_t v = 0; v < V; ++v) {
+        deg[v] = v < nvp ? pdeg[v] : 0;
+        nn[v] = v < nvp ? pnn[v] : 0;
+    }
+    for (uint32_t k = 0; k < R.n_lhs; ++k) {
+        const uint32_t e = rpos[k], a = pear[e], vo = pevo[e];
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t v = vloc[vo + q];
+            deg[v] -= 1;
+            nn[v] -= static_cast<uint16_t>(a - 1);
+        }
+    }
+    for (uint32_t k = 0; k < R.n_rhs; ++k) {
+        const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t v = prodv[o + q];
+            deg[v] += 1;
+            nn[v] += static_cast<uint16_t>(a - 1);
+        }
+    }
+    uint32_t nv = 0, cap = 1, nocc = 0, nbr = 0;
+    for (uint32_t v = 0; v < V; ++v) {
+        nv += deg[v] ? 1u : 0u;
+        cap = nn[v] > cap ? nn[v] : cap;
+        nocc += deg[v];
+        nbr += nn[v];
+    }
+    info.nv = nv;
+    info.nocc = nocc;
+    info.nbr = nbr;
+    if (nv == 0) return 0;
+
+    uint64_t cur[VM], nxt[VM], buf[NM];
+    // initial colours
+    for (uint32_t v = 0; v < V; ++v) {
+        cur[v] = 0;
+        if (!deg[v]) continue;
+        uint32_t n = 0;
+        const uint32_t j0 = v < nvp ? poff[v] : 0u, j1 = v < nvp ? poff[v + 1] : 0u;
+        for (uint32_t j = j0; j < j1 && n < cap; ++j) {
+            const uint32_t x = pocc[j], e = x >> 4;
+            if ((rmask >> e) & 1ull) continue;
+            buf[n++] = (static_cast<uint64_t>(pear[e]) << 8) | (x & 15u);
+        }
+        for (uint32_t k = 0; k < R.n_rhs; ++k) {
+            const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+            for (uint32_t q = 0; q < a && n < cap; ++q)
+                if (prodv[o + q] == v) buf[n++] = (static_cast<uint64_t>(a) << 8) | q;
+        }
+        lane_isort64(buf, n);
+        uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(deg[v]));
+        for (uint32_t j = 0; j < n; ++j) {
+            h = fnv(h, buf[j] >> 8);
+            h = fnv(h, buf[j] & 0xFFu);
+        }
+        cur[v] = h;
+    }
+    uint32_t prev = lane_distinct<VM>(cur, deg, V);
+    for (uint32_t it = 0; it < kWlMaxRounds; ++it) {
+        for (uint32_t v = 0; v < V; ++v) {
+            if (!deg[v]) { nxt[v] = 0; continue; }
+            uint32_t n = 0;
+            const uint32_t j0 = v < nvp ? poff[v] : 0u, j1 = v < nvp ? poff[v + 1] : 0u;
+            for (uint32_t j = j0; j < j1; ++j) {
+                const uint32_t x = pocc[j], e = x >> 4;
+                if ((rmask >> e) & 1ull) continue;
+                const uint32_t q = x & 15u, a = pear[e], vo = pevo[e];
+                for (uint32_t k = 0; k < a; ++k)
+                    if (k != q && n < cap) buf[n++] = fnv(cur[vloc[vo + k]], k);
+            }
+            for (uint32_t kk = 0; kk < R.n_rhs; ++kk) {
+                const uint32_t a = R.rhs_ar[kk], o = R.rhs_off[kk];
+                for (uint32_t q = 0; q < a; ++q) {
+                    if (prodv[o + q] != v) continue;
+                    for (uint32_t t = 0; t < a; ++t)
+                        if (t != q && n < cap) buf[n++] = fnv(cur[prodv[o + t]], t);
+                }
+            }
+            lane_isort64(buf, n);
+            uint64_t h = cur[v];
+            for (uint32_t j = 0; j < n; ++j) h = fnv(h, buf[j]);
+            nxt[v] = h;
+        }
+        for (uint32_t v = 0; v < V; ++v) cur[v] = nxt[v];
+        const uint32_t d = lane_distinct<VM>(cur, deg, V);
+        ++info.rounds;
+        if (d == prev) break;
+        prev = d;
+    }
+
+    // components (partition), then the commutative folds
+    uint8_t comp[VM];
+    for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(v);
+    auto find = [&](uint32_t x) -> uint32_t {
+        while (comp[x] != x) { comp[x] = comp[comp[x]]; x = comp[x]; }
+        return x;
+    };
+    for (uint32_t e = 0; e < pne; ++e) {
+        if ((rmask >> e) & 1ull) continue;
+        const uint32_t a = pear[e], vo = pevo[e];
+        const uint32_t r = find(vloc[vo]);
+        for (uint32_t q = 1; q < a; ++q) {
+            const uint32_t x = find(vloc[vo + q]);
+            if (x != r) comp[x] = static_cast<uint8_t>(r);
+        }
+    }
+    for (uint32_t k = 0; k < R.n_rhs; ++k) {
+        const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+        const uint32_t r = find(prodv[o]);
+        for (uint32_t q = 1; q < a; ++q) {
+            const uint32_t x = find(prodv[o + q]);
+            if (x != r) comp[x] = static_cast<uint8_t>(r);
+        }
+    }
+    for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(find(v));
+    uint64_t vs = 0, es = 0, cs = 0;
+    for (uint32_t v = 0; v < V; ++v) {
+        nxt[v] = deg[v] ? smix(cur[v]) : 0;
+        vs += nxt[v];
+    }
+    for (uint32_t e = 0; e < pne; ++e) {
+        if ((rmask >> e) & 1ull) continue;
+        const uint32_t a = pear[e], vo = pevo[e];
+        uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(a));
+        for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[vloc[vo + q]]);
+        es += smix(h);
+    }
+    for (uint32_t k = 0; k < R.n_rhs; ++k) {
+        const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+        uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(a));
+        for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[prodv[o + q]]);
+        es += smix(h);
+    }
+    for (uint32_t r = 0; r < V; ++r) {
+        if (!deg[r] || comp[r] != r) continue;
+        uint64_t col = 0, vc = 0, ec = 0;
+        for (uint32_t v = 0; v < V; ++v)
+            if (deg[v] && comp[v] == r) { col += nxt[v]; ++vc; }
+        for (uint32_t e = 0; e < pne; ++e)
+            if (!((rmask >> e) & 1ull) && comp[vloc[pevo[e]]] == r) ++ec;
+        for (uint32_t k = 0; k < R.n_rhs; ++k)
+            if (comp[prodv[R.rhs_off[k]]] == r) ++ec;
+        cs += smix(fnv(fnv(kFnvOffset, (ec << 32) | vc), col));
+    }
+    uint64_t h = kFnvOffset;
+    h = fnv(h, nv);
+    h = fnv(h, ne);
+    h = fnv(h, vs);
+    h = fnv(h, es);
+    h = fnv(h, cs);
+    return h;
+}
+
+
+}  // namespace hgx

@@ -18,6 +18,7 @@
 // staged once in shared memory and every child of it is built and hashed there, so children are
 // never written to HBM unless they are new class representatives.
 #include "step_kernels.cuh"
+#include "lane_wl.cuh"
 
 namespace hgx {
 
@@ -371,7 +372,7 @@ __device__ uint32_t wl_distinct(const uint64_t* cur, const uint32_t* deg, uint32
     return warp_sum32(cnt);
 }
 
-__device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V) {
+__device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, WlInfo& info) {
     const uint32_t lane = lane_id();
     const uint8_t* car = smp<uint8_t>(sm, L.o_car);
     const uint16_t* cvo = smp<uint16_t>(sm, L.o_cvo);
@@ -388,6 +389,10 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V) 
     uint32_t* nn = smp<uint32_t>(sm, L.o_nn);
     uint32_t* comp = smp<uint32_t>(sm, L.o_comp);
 
+    info.rounds = 0;
+    info.nv = 0;
+    info.nocc = 0;
+    info.nbr = 0;
     if (ne == 0) return kEmptyStateHash;
 
     for (uint32_t v = lane; v < V; v += 32) { deg[v] = 0; nn[v] = 0; }
@@ -401,7 +406,7 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V) 
         }
     }
     __syncwarp();
-    uint32_t run_o = 0, run_n = 0, nv = 0, cap = 1;
+    uint32_t run_o = 0, run_n = 0, run_nn = 0, nv = 0, cap = 1;
     for (uint32_t b = 0; b < V; b += 32) {
         const uint32_t v = b + lane;
         const uint32_t dv = v < V ? deg[v] : 0u;
@@ -418,7 +423,11 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V) 
         run_n += __shfl_sync(0xFFFFFFFFu, is, 31);
         nv += __popc(__ballot_sync(0xFFFFFFFFu, dv > 0));
         cap = max(cap, warp_max32(nnv));
+        run_nn += warp_sum32(nnv);
     }
+    info.nv = nv;
+    info.nocc = run_o;
+    info.nbr = run_nn;   // sum over edges of a(a-1): neighbour entries per refinement round
     if (nv == 0) return 0;   // only arity-0 edges: the reference core returns 0
     __syncwarp();
     for (uint32_t e = lane; e < ne; e += 32) {
@@ -475,6 +484,7 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V) 
         for (uint32_t v = lane; v < V; v += 32) cur[v] = nxt[v];
         __syncwarp();
         const uint32_t dd = wl_distinct(cur, deg, V);
+        ++info.rounds;
         if (dd == prev) break;
         prev = dd;
     }
@@ -533,6 +543,60 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V) 
     return h;
 }
 
+
+// ------------------------------------------------------------------------------------------
+// Lane-per-child WL. For the small states that dominate deep evolutions (a handful of
+// vertices, tens of edges) one warp per child leaves most lanes idle; instead the warp stages
+// the parent once, enumerates up to 32 matches into a batch, and every lane hashes one child
+// against the shared parent. A child is described by the parent positions it removes and the
+// local vertex ids of its produced edges; its occurrence lists are the parent's (edge order)
+// minus removed edges, followed by the produced occurrences (RHS order) -- the child's edge
+// order, so the initial-colour truncation sees occurrences in the same order as the reference.
+// ------------------------------------------------------------------------------------------
+__device__ uint32_t build_parent_csr(const Layout& L, char* sm, const Parent& pa) {
+    const uint32_t lane = lane_id();
+    const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+    const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    uint16_t* poff = smp<uint16_t>(sm, L.o_poff);
+    uint16_t* pocc = smp<uint16_t>(sm, L.o_pocc);
+    uint16_t* pdeg = smp<uint16_t>(sm, L.o_pdeg);
+    uint16_t* pnn = smp<uint16_t>(sm, L.o_pnn);
+    const uint32_t v = lane;
+    uint32_t d = 0, nn = 0;
+    if (v < pa.nvp)
+        for (uint32_t e = 0; e < pa.ne; ++e) {
+            const uint32_t a = pear[e], vo = pevo[e];
+            for (uint32_t q = 0; q < a; ++q)
+                if (vloc[vo + q] == v) { ++d; nn += a - 1; }
+        }
+    const uint32_t inc = warp_incl_scan(d);
+    if (v < pa.nvp) {
+        poff[v] = static_cast<uint16_t>(inc - d);
+        pdeg[v] = static_cast<uint16_t>(d);
+        pnn[v] = static_cast<uint16_t>(nn);
+        uint32_t w = inc - d;
+        for (uint32_t e = 0; e < pa.ne; ++e) {
+            const uint32_t a = pear[e], vo = pevo[e];
+            for (uint32_t q = 0; q < a; ++q)
+                if (vloc[vo + q] == v) pocc[w++] = static_cast<uint16_t>((e << 4) | q);
+        }
+    }
+    if (lane == 31) poff[pa.nvp] = static_cast<uint16_t>(inc);
+    const uint32_t nnmax = warp_max32(nn);
+    __syncwarp();
+    return nnmax;
+}
+
+template <int VM, int NM>
+__device__ __forceinline__ uint64_t lane_wl(const Layout& L, char* sm, const Parent& pa,
+                                            const DevRule& R, const uint8_t* slot, WlInfo& info) {
+    return lane_wl_core<VM, NM>(smp<uint8_t>(sm, L.o_pear), smp<uint16_t>(sm, L.o_pevo),
+                                smp<uint16_t>(sm, L.o_vloc), smp<uint16_t>(sm, L.o_poff),
+                                smp<uint16_t>(sm, L.o_pocc), smp<uint16_t>(sm, L.o_pdeg),
+                                smp<uint16_t>(sm, L.o_pnn), pa.ne, pa.nvp, R, slot, info);
+}
+
 }  // namespace
 
 // ==========================================================================================
@@ -557,7 +621,8 @@ __global__ void k_roots(DevPtrs P, const uint32_t* sids, uint32_t n, uint32_t* w
         const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
         for (uint32_t e = lane; e < pa.ne; e += 32) { car[e] = pear[e]; cvo[e] = pevo[e]; }
         __syncwarp();
-        const uint64_t h = warp_wl(L, sm, pa.ne, pa.nvp);
+        WlInfo info;
+        const uint64_t h = warp_wl(L, sm, pa.ne, pa.nvp, info);
         if (lane == 0) {
             P.st_hash[sid] = h;
             const uint32_t a = P.st_event[sid];
@@ -625,6 +690,9 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
     const DevRule& R = *smp<DevRule>(sm, L.o_rule);
     const uint32_t* peid = smp<uint32_t>(sm, L.o_peid);
     const uint16_t* match = smp<uint16_t>(sm, L.o_match);
+    const uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
+    uint8_t* batch = smp<uint8_t>(sm, L.o_batch);
+    uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
     while (true) {
         uint32_t f = 0;
         if (lane == 0) f = atomicAdd(&A.work[1], 1u);
@@ -634,8 +702,12 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
         const Parent pa = load_parent(P, L, sm, sid);
         const uint32_t evo = P.st_evo[sid];
         const DevEvo ev = P.evos[evo];
+        if (lane == 0) b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
+        const bool lane_ok = pa.nvp <= kLaneVMax && pa.ne <= kLaneEMax && pa.ne > 0;
+        const uint32_t pnn_max = lane_ok ? build_parent_csr(L, sm, pa) : 0u;
         for (uint32_t r = 0; r < A.rules_stride && r < ev.rule_count; ++r) {
             const uint32_t item = f * A.rules_stride + r;
+            if (lane == 0) b_stage += 4ull * pa.ne + 4ull * pa.nocc;   // join: ids and vertices
             if (A.counts[item] == 0) continue;
             load_rule(sm, L, &P.rules[ev.rule_begin + r]);
             const uint32_t ev0 = A.ev_base + A.item_ev[item];
@@ -643,33 +715,122 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
             const uint32_t prod0 = A.prod_base + A.item_prod[item];
             const uint32_t fresh0 = A.fresh_base + A.item_fresh[item];
             const uint32_t rule_g = ev.rule_begin + r;
-            uint32_t idx = 0;
-            warp_join(L, sm, R, pa, [&](uint32_t nm) {
+            // neighbour-count bound of any child vertex under this rule
+            uint32_t gain = 0;
+            for (uint32_t k = 0; k < R.n_rhs; ++k) gain += uint32_t(R.rhs_ar[k]) * (R.rhs_ar[k] - 1u);
+            const uint32_t vneed = pa.nvp + R.n_fresh;
+            const int mode = !lane_ok ? 0
+                           : (vneed <= 16 && pnn_max + gain <= 48) ? 1
+                           : (vneed <= 32 && pnn_max + gain <= 64) ? 2 : 0;
+            // per-child work shared by both paths: the event record and the table insert
+            auto finish = [&](uint32_t idx, uint64_t h, const WlInfo& info, const uint8_t* rpos) {
                 const uint32_t e = ev0 + idx;
                 const uint32_t coff = cons0 + idx * R.n_lhs;
                 const uint32_t pid = prod0 + idx * R.n_rhs;
-                if (lane < R.n_lhs) {
-                    const uint32_t gid = peid[match[lane]];
-                    P.ev_cons[coff + lane] = gid;
-                    P.ev_cprod[coff + lane] = P.edge_creator[gid];
-                }
-                if (lane < R.n_rhs) P.edge_creator[pid + lane] = e;
-                if (lane == 0) {
-                    P.ev_in[e] = sid;
-                    P.ev_rule[e] = rule_g;
-                    P.ev_coff[e] = coff;
-                    P.ev_prod[e] = pid;
-                    P.ev_fresh[e] = fresh0 + idx * R.n_fresh;
-                }
-                const uint32_t nec = build_child(L, sm, R, pa, nm);
-                const uint64_t h = warp_wl(L, sm, nec, pa.nvp + R.n_fresh);
-                if (lane == 0) {
-                    P.ev_hash[e] = h;
-                    table_insert(P, ev, h, e);
-                }
-                ++idx;
-            });
+                P.ev_in[e] = sid;
+                P.ev_rule[e] = rule_g;
+                P.ev_coff[e] = coff;
+                P.ev_prod[e] = pid;
+                P.ev_fresh[e] = fresh0 + idx * R.n_fresh;
+                P.ev_hash[e] = h;
+                for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = peid[rpos[k]];
+                for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
+                table_insert(P, ev, h, e);
+                const uint64_t k = R.n_lhs, rr = R.n_rhs;
+                const uint32_t nec = pa.ne - R.n_lhs + R.n_rhs;
+                b_stage += 4 * k + 8;
+                b_stage += 4ull * pa.ne + 4ull * nec + 4ull * R.rhs_total + 12 * rr + 16 + 4 * k + 4 * rr;
+                b_stage += 5ull * info.nocc + 8ull * info.nv +
+                           uint64_t(info.rounds) * (8ull * info.nbr + 5ull * info.nocc + 16ull * info.nv) +
+                           8ull * info.nv + 8ull * info.nocc;
+                b_stage += 16;
+                b_hbm += 20 + 8 + 8 * k + 4 * rr + 16;
+                n_child += 1;
+                n_rounds += info.rounds;
+            };
+            if (mode) {
+                uint32_t nb = 0, done = 0;
+                auto flush = [&]() {
+                    if (lane < nb) {
+                        const uint8_t* slot = batch + lane * L.SB;
+                        WlInfo info;
+                        const uint64_t h = (mode == 1) ? lane_wl<16, 48>(L, sm, pa, R, slot, info)
+                                                       : lane_wl<32, 64>(L, sm, pa, R, slot, info);
+                        finish(done + lane, h, info, slot);
+                    }
+                    __syncwarp();
+                    done += nb;
+                    nb = 0;
+                };
+                warp_join(L, sm, R, pa, [&](uint32_t nm) {
+                    uint8_t* slot = batch + nb * L.SB;
+                    if (lane < R.n_lhs) slot[lane] = static_cast<uint8_t>(match[lane]);
+                    for (uint32_t t = lane; t < R.rhs_total; t += 32) {
+                        const uint32_t var = R.rhs_vars[t];
+                        slot[R.n_lhs + t] = static_cast<uint8_t>(((nm >> var) & 1u) ? bind[var]
+                                                                 : pa.nvp + R.fresh_rank[var]);
+                    }
+                    __syncwarp();
+                    if (++nb == 32) flush();
+                });
+                if (nb) flush();
+            } else {
+                uint32_t idx = 0;
+                uint8_t rpos[kMaxPatternEdges];
+                warp_join(L, sm, R, pa, [&](uint32_t nm) {
+                    for (uint32_t k = 0; k < R.n_lhs; ++k) rpos[k] = static_cast<uint8_t>(match[k]);
+                    const uint32_t nec = build_child(L, sm, R, pa, nm);
+                    WlInfo info;
+                    const uint64_t h = warp_wl(L, sm, nec, pa.nvp + R.n_fresh, info);
+                    if (lane == 0) finish(idx, h, info, rpos);
+                    __syncwarp();
+                    ++idx;
+                });
+            }
         }
+    }
+    b_stage = warp_sum64(b_stage);
+    b_hbm = warp_sum64(b_hbm);
+    n_child = warp_sum64(n_child);
+    n_rounds = warp_sum64(n_rounds);
+    if (lane == 0 && b_hbm) {
+        atomicAdd(&P.stats[0], static_cast<unsigned long long>(b_stage));
+        atomicAdd(&P.stats[1], static_cast<unsigned long long>(b_hbm));
+        atomicAdd(&P.stats[2], static_cast<unsigned long long>(n_child));
+        atomicAdd(&P.stats[3], static_cast<unsigned long long>(n_rounds));
+    }
+}
+
+// Producer event of every consumed edge of this level (the causal relation's gather).
+__global__ void k_cprod(DevPtrs P, uint32_t base, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        P.ev_cprod[base + i] = P.edge_creator[P.ev_cons[base + i]];
+}
+
+// Per-evolution totals without reading the result back: kept events, causal triples,
+// branchial pairs. out[evo * 3 + {0,1,2}].
+__global__ void k_evo_totals(DevPtrs P, uint32_t n_events, const uint32_t* bpairs, uint64_t n_bpairs,
+                             unsigned long long* out) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < n_events; t0 += stride) {
+        const uint64_t e = t0 + threadIdx.x;
+        bool live = false;
+        uint32_t evo = 0, nc = 0;
+        if (e < n_events && P.ev_in[e] != kNone && P.ev_kept[e]) {
+            live = true;
+            evo = P.st_evo[P.ev_in[e]];
+            const DevRule& R = P.rules[P.ev_rule[e]];
+            const uint32_t co = P.ev_coff[e];
+            for (uint32_t k = 0; k < R.n_lhs; ++k) nc += P.ev_cprod[co + k] != kNone ? 1u : 0u;
+        }
+        warp_count(out, live ? evo * 3 : 0, live);
+        if (live && nc) atomicAdd(&out[evo * 3 + 1], static_cast<unsigned long long>(nc));
+    }
+    for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < n_bpairs; t0 += stride) {
+        const uint64_t i = t0 + threadIdx.x;
+        const bool live = i < n_bpairs;
+        const uint32_t evo = live ? P.st_evo[P.ev_in[bpairs[2 * i]]] : 0;
+        warp_count(out, evo * 3 + 2, live);
     }
 }
 

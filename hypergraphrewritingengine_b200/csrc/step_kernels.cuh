@@ -60,6 +60,10 @@ struct DevPtrs {
     uint32_t* evo_stopped;
     // errors
     uint32_t* err;
+    // expand-kernel counters: [0] bytes by the per-stage figures (join + rewrite + WL + dedup
+    // as separate streams), [1] bytes the fused kernel must move to/from HBM, [2] children
+    // hashed, [3] WL refinement rounds run
+    unsigned long long* stats;
 };
 
 // Per-level parameters.
@@ -100,6 +104,10 @@ struct Layout {
     uint32_t o_pevo, o_vloc, o_cvo, o_bind, o_match, o_mdepth;      // u16
     uint32_t o_pear, o_car;                                         // u8
     uint32_t o_rule;                                                // DevRule
+    // lane-per-child path: parent occurrence lists by vertex, per-vertex degree / neighbour
+    // counts, and a batch of up to 32 matches (removed positions + produced local vertices)
+    uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_batch;
+    uint32_t SB;                                                    // bytes per batch slot
     uint32_t bytes;
 };
 

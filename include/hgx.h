@@ -64,7 +64,10 @@ typedef enum hgx_option {
        edge record (ids, arities, vertices). */
     HGX_OPT_KEEP_STATE_EDGES = 5,
     /* 1 = record per-stage device times (CUDA events on the engine stream). */
-    HGX_OPT_TIMING = 6
+    HGX_OPT_TIMING = 6,
+    /* 1 (default) = copy the result to host memory; 0 = keep it on the device and report the
+       counts only (hgx_result_count works, hgx_result_copy returns empty arrays). */
+    HGX_OPT_READBACK = 7
 } hgx_option;
 
 /* One evolution of a batch or a served request. */
@@ -163,6 +166,16 @@ HGX_API void hgx_result_free(hgx_result* result);
    out[0..7] = count, scan, expand, select, materialize, branchial, roots, total.
    launches: kernels launched by the call. */
 HGX_API hgx_status hgx_engine_stage_times(hgx_engine* engine, double* out_ms, uint64_t* launches);
+
+/* Counters of the last evolve call's expand kernel (the fused join + rewrite + WL + dedup
+   kernel): out[0] bytes by the per-stage figures (join + rewrite + WL + dedup counted as
+   separate HBM streams), out[1] bytes the fused kernel itself must move to or from HBM,
+   out[2] children hashed, out[3] WL refinement rounds, out[4] expand launches. */
+HGX_API hgx_status hgx_engine_expand_stats(hgx_engine* engine, uint64_t* out);
+
+/* The CUDA stream (cudaStream_t) the engine launches on, for callers that time or order
+   work against it. */
+HGX_API hgx_status hgx_engine_stream(hgx_engine* engine, void** stream);
 
 #ifdef __cplusplus
 }
