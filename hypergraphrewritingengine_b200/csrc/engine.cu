@@ -735,11 +735,13 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[4], level_max.p + 2, 8, cudaMemcpyDeviceToHost, st));
         const size_t nevo = h_evos.size();
         std::vector<uint32_t> h_first(nevo), h_last(nevo);
-        std::vector<unsigned long long> h_classes(nevo);
+        std::vector<unsigned long long> h_classes(nevo), h_states_ev(nevo);
         HGX_CUDA_CHECK(cudaMemcpyAsync(h_first.data(), evo_first_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(h_last.data(), evo_last_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(h_classes.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(h_states_ev.data(), evo_states.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        auto h_states_now = [&](uint32_t e) { return static_cast<uint64_t>(h_states_ev[e]); };
         const uint32_t n_ev = tot[0], n_cons_lv = tot[1], n_prod = tot[2], n_fresh = tot[3];
         const uint32_t fmax_ne = tot[4], fmax_nocc = tot[5];
         if (uint64_t(n_events) + n_ev >= 0xFFFFFFF0ull || uint64_t(n_edges) + n_prod >= 0xFFFFFFF0ull ||
@@ -771,52 +773,108 @@ struct Engine::Impl {
         }
 
         // ---- expand: events, produced edges, children's WL hashes, table inserts
+        //
+        // A level that a state cap may cut is expanded in chunks of the frontier, in frontier
+        // (= canonical event) order, stopping after the chunk that holds the cut: every event
+        // after the cut is dropped anyway, so the result is identical and the dropped tail is
+        // never built. Dedup stays exact because a chunk's events are selected only after every
+        // earlier event has been inserted.
+        uint32_t F_eff = F;
         if (n_ev) {
             const Layout Le = make_layout(std::max<uint32_t>(fmax_ne, 1), std::max<uint32_t>(fmax_nocc, 1), rm, true);
             LaunchShape se = warp_shape(k_expand, Le, F);
-            tic();
-            k_expand<<<se.grid, se.block, se.smem, st>>>(ptrs(), A, Le);
-            check_launch();
-            if (n_cons_lv) {
-                k_cprod<<<grid_for(n_cons_lv, 256), 256, 0, st>>>(ptrs(), A.cons_base, n_cons_lv);
+            // chunking applies to a level holding one evolution whose cap this level can reach
+            uint32_t only = kNone, n_in_level = 0;
+            for (size_t e = 0; e < nevo; ++e)
+                if (!evo_done[e] && h_first[e] != kNone) { only = static_cast<uint32_t>(e); ++n_in_level; }
+            uint64_t remaining = 0;
+            bool chunked = false;
+            if (n_in_level == 1 && h_evos[only].max_states) {
+                const uint64_t have = h_evos[only].quotient ? h_classes[only] : h_states_now(only);
+                remaining = h_evos[only].max_states > have ? h_evos[only].max_states - have : 0;
+                chunked = uint64_t(n_ev) > remaining && F >= 4096;
+            }
+            std::vector<uint32_t> h_item;
+            if (chunked) {
+                h_item.resize(NI + 1);
+                HGX_CUDA_CHECK(cudaMemcpyAsync(h_item.data(), item_ev.p, (NI + 1) * 4, cudaMemcpyDeviceToHost, st));
+                HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            }
+            const uint32_t chunk = chunked ? std::max<uint32_t>(1024, (F + 31) / 32) : F;
+            uint64_t cum = 0;
+            uint32_t f0 = 0;
+            while (f0 < F) {
+                const uint32_t f1 = std::min<uint64_t>(F, uint64_t(f0) + chunk);
+                A.f_begin = f0;
+                A.f_end = f1;
+                HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, sizeof(uint32_t), st));
+                tic();
+                k_expand<<<se.grid, se.block, se.smem, st>>>(ptrs(), A, Le);
+                check_launch();
+                toc(times.expand);
+                ++times.expand_launches;
+                const uint32_t t0 = chunked ? h_item[uint64_t(f0) * R] : 0u;
+                const uint32_t t1 = chunked ? h_item[uint64_t(f1) * R] : n_ev;
+                tic();
+                k_select<<<grid_for(t1 - t0, 256), 256, 0, st>>>(ptrs(), A, t0, t1);
+                check_launch();
+                toc(times.select);
+                f0 = f1;
+                if (!chunked) break;
+                uint32_t cnt = t1 - t0;
+                if (h_evos[only].quotient) {
+                    HGX_CUDA_CHECK(cudaMemsetAsync(sync_buf.p, 0, 4, st));
+                    k_sum_flags<<<grid_for(t1 - t0, 256), 256, 0, st>>>(flag_new.p + t0, t1 - t0, sync_buf.p);
+                    check_launch();
+                    HGX_CUDA_CHECK(cudaMemcpyAsync(&cnt, sync_buf.p, 4, cudaMemcpyDeviceToHost, st));
+                    HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+                }
+                cum += cnt;
+                if (cum > remaining) break;   // the cut event lies in the chunk just processed
+            }
+            F_eff = f0;
+            const uint32_t n_ev_eff = chunked ? h_item[uint64_t(F_eff) * R] : n_ev;
+            A.n_events = n_ev_eff;
+            if (n_ev_eff) {
+                k_cprod<<<grid_for(n_ev_eff, 256), 256, 0, st>>>(ptrs(), A.ev_base, n_ev_eff);
                 check_launch();
             }
-            toc(times.expand);
-            ++times.expand_launches;
 
-            // ---- select / cap / representatives
+            // ---- cap / representatives over the events actually built
+            const uint32_t ne2 = A.n_events;
             tic();
-            k_select<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
-            check_launch();
             if (any_cap) {
-                scan(flag_new.p, scan_new.p, n_ev);
-                k_cut<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+                scan(flag_new.p, scan_new.p, ne2);
+                k_cut<<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
                 check_launch();
             }
-            k_rep<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+            k_rep<<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
-            scan(flag_rep.p, flag_rep.p, n_ev);
-            scan(flag_front.p, flag_front.p, n_ev);
+            scan(flag_rep.p, flag_rep.p, ne2);
+            scan(flag_front.p, flag_front.p, ne2);
             toc(times.select);
         } else {
             HGX_CUDA_CHECK(cudaMemsetAsync(flag_rep.p, 0, 4, st));
             HGX_CUDA_CHECK(cudaMemsetAsync(flag_front.p, 0, 4, st));
         }
-        if (opt.branchial && n_ev) {
+        // frontier states whose events were built (all of them unless a chunked cut stopped early)
+        A.n_frontier = F_eff;
+        const uint32_t ne2 = A.n_events;
+        if (opt.branchial && ne2) {
             tic();
-            k_bcount<<<grid_for(uint64_t(F) * 32, 256), 256, 0, st>>>(ptrs(), A);
+            k_bcount<<<grid_for(uint64_t(F_eff) * 32, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
-            scan(bcount.p, boff.p, F);
+            scan(bcount.p, boff.p, F_eff);
             toc(times.branchial);
         } else {
-            HGX_CUDA_CHECK(cudaMemsetAsync(boff.p + F, 0, 4, st));
+            HGX_CUDA_CHECK(cudaMemsetAsync(boff.p + F_eff, 0, 4, st));
         }
 
         // ---- sync 2: new states, next frontier, branchial pairs, errors
         uint32_t s2[4];
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[0], flag_rep.p + n_ev, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[1], flag_front.p + n_ev, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + F, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[0], flag_rep.p + ne2, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[1], flag_front.p + ne2, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + F_eff, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[3], err.p, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         if (s2[3]) throw std::runtime_error("hgx: device error flags 0x" + std::to_string(s2[3]));
@@ -834,11 +892,11 @@ struct Engine::Impl {
         A.next_frontier = next_frontier.p;
         A.bpairs = bpairs.p;
         A.bbase = static_cast<uint32_t>(n_bpairs);
-        if (n_ev) {
+        if (ne2) {
             tic();
-            k_assign<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+            k_assign<<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
-            k_outstate<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A);
+            k_outstate<<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
             if (n_new) {
                 k_materialize<<<grid_for(uint64_t(n_new) * 32, 256), 256, 0, st>>>(ptrs(), A, n_new);
@@ -851,7 +909,7 @@ struct Engine::Impl {
             // pair offsets are absolute: shift by the running total
             A.boff = boff.p;
             A.bpairs = bpairs.p + 2ull * n_bpairs;
-            k_bemit<<<grid_for(uint64_t(F) * 32, 256), 256, 0, st>>>(ptrs(), A);
+            k_bemit<<<grid_for(uint64_t(F_eff) * 32, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
             toc(times.branchial);
         }
@@ -874,8 +932,9 @@ struct Engine::Impl {
                 finished.push_back(static_cast<uint32_t>(e));
             }
 
-        // advance
-        n_events += n_ev;
+        // advance (id ranges of produced edges / fresh vertices / consumed lists were reserved for
+        // the whole level; a chunked cut leaves the unbuilt tail of those ranges unused)
+        n_events += ne2;
         n_cons += n_cons_lv;
         n_edges += n_prod;
         next_vertex += n_fresh;

@@ -695,9 +695,9 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
     uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
     while (true) {
         uint32_t f = 0;
-        if (lane == 0) f = atomicAdd(&A.work[1], 1u);
+        if (lane == 0) f = A.f_begin + atomicAdd(&A.work[1], 1u);
         f = __shfl_sync(0xFFFFFFFFu, f, 0);
-        if (f >= A.n_frontier) break;
+        if (f >= A.f_end) break;
         const uint32_t sid = A.frontier[f];
         const Parent pa = load_parent(P, L, sm, sid);
         const uint32_t evo = P.st_evo[sid];
@@ -801,10 +801,14 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
     }
 }
 
-// Producer event of every consumed edge of this level (the causal relation's gather).
-__global__ void k_cprod(DevPtrs P, uint32_t base, uint32_t n) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        P.ev_cprod[base + i] = P.edge_creator[P.ev_cons[base + i]];
+// Producer event of every consumed edge of the level's built events (the causal relation's
+// gather: an edge has exactly one producer, recorded when it was minted).
+__global__ void k_cprod(DevPtrs P, uint32_t ev_base, uint32_t n) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t e = ev_base + t;
+        const uint32_t co = P.ev_coff[e], k = P.rules[P.ev_rule[e]].n_lhs;
+        for (uint32_t i = 0; i < k; ++i) P.ev_cprod[co + i] = P.edge_creator[P.ev_cons[co + i]];
+    }
 }
 
 // Per-evolution totals without reading the result back: kept events, causal triples,
@@ -911,8 +915,8 @@ __global__ void k_mark_front(DevPtrs P, const uint32_t* front, uint32_t n, uint3
 }
 
 // Is the child the first arrival of its WL class? (winner stored in ev_out until resolved)
-__global__ void k_select(DevPtrs P, LevelArgs A) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
+__global__ void k_select(DevPtrs P, LevelArgs A, uint32_t t_begin, uint32_t t_end) {
+    for (uint32_t t = t_begin + blockIdx.x * blockDim.x + threadIdx.x; t < t_end;
          t += gridDim.x * blockDim.x) {
         const uint32_t e = A.ev_base + t;
         const uint32_t evo = P.st_evo[P.ev_in[e]];
@@ -920,6 +924,15 @@ __global__ void k_select(DevPtrs P, LevelArgs A) {
         P.ev_out[e] = w;
         A.flag_new[t] = (w == e) ? 1u : 0u;
     }
+}
+
+// Sum of flags[0, n) into *out.
+__global__ void k_sum_flags(const uint32_t* flags, uint32_t n, uint32_t* out) {
+    uint32_t c = 0;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        c += flags[t];
+    c = warp_sum32(c);
+    if (lane_id() == 0 && c) atomicAdd(out, c);
 }
 
 // State cap: the first event of an evolution that would take it past max_states cuts the level

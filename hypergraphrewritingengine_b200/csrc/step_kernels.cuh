@@ -78,6 +78,7 @@ struct LevelArgs {
     uint32_t* item_fresh;
     uint32_t ev_base, cons_base, prod_base, fresh_base;   // level bases
     uint32_t n_events;          // events minted this level
+    uint32_t f_begin, f_end;    // frontier range the expand kernel works on
     uint32_t* work;             // work-queue counters
     // select / assign
     uint32_t* flag_new;         // [n_events]

@@ -104,3 +104,25 @@ def test_reference_shaped_api(engine):
     assert hg.num_canonical_states() == 20
     assert hg.causal_graph().num_causal_edges() == 42816
     assert hg.causal_graph().num_branchial_edges() == 78045
+
+
+@pytest.mark.parametrize("quotient,rule,init,steps,cap", [
+    (True, cases.C2_RULE, cases.C2_INIT, 7, 100_000),      # cut inside a chunked level
+    (True, cases.C2_RULE, cases.C2_INIT, 7, 26_700),       # cut right after the previous level
+    (False, cases.C1_RULE, cases.C1_INIT, 6, 100_000),     # full multiway: raw-state cap
+])
+def test_chunked_cap_matches_oracle(engine, quotient, rule, init, steps, cap):
+    res = engine.evolve([rule], [init], steps, quotient=quotient, max_states=cap)
+    ref = pyoracle.evolve([rule], [init], steps, quotient=quotient, max_states=cap)
+    assert res.truncated == ref["truncated"]
+    assert_same(norm_gpu(res), norm_oracle(ref), f"cap {cap}")
+
+
+@pytest.mark.parametrize("ev", [W.config2(8), W.config3(6)], ids=lambda e: e.name)
+def test_full_size_workloads_match_oracle(engine, ev):
+    """The benchmarked sizes themselves (C2: 8 levels, 2M-state cap; C3: 6 levels)."""
+    res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+    ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+    assert res.truncated == ref["truncated"]
+    assert res.num_classes == ref["classes"]
+    assert_same(norm_gpu(res), norm_oracle(ref), ev.name)
