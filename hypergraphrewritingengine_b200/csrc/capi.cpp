@@ -352,7 +352,7 @@ hgx_status hgx_engine_stage_times(hgx_engine* e, double* out, uint64_t* launches
     out[4] = t.materialize;
     out[5] = t.branchial;
     out[6] = t.roots;
-    out[7] = t.count + t.scan + t.expand + t.select + t.materialize + t.branchial + t.roots;
+    out[7] = t.count + t.scan + t.expand + t.expand_warp + t.select + t.materialize + t.branchial + t.roots;
     if (launches) *launches = t.launches;
     return HGX_OK;
 }
@@ -365,6 +365,11 @@ hgx_status hgx_engine_expand_stats(hgx_engine* e, uint64_t* out) {
     out[2] = t.children;
     out[3] = t.wl_rounds;
     out[4] = t.expand_launches;
+    out[5] = t.warp_bytes;
+    out[6] = t.warp_hbm_bytes;
+    out[7] = t.warp_children;
+    out[8] = t.warp_rounds;
+    out[9] = static_cast<uint64_t>(t.expand_warp * 1e6);   // warp kernel time, ns
     return HGX_OK;
 }
 

@@ -32,6 +32,7 @@ constexpr int kMaxSideVars = 64;   // total positions over one rule side (16 edg
 // kLaneVMax vertices is expanded with one child per lane.
 constexpr int kLaneVMax = 32;
 constexpr int kLaneEMax = 64;
+constexpr int kLaneNMax = 64;    // neighbour entries a lane sorts for one vertex
 
 HGX_HD uint64_t fnv(uint64_t h, uint64_t x) { return (h ^ x) * kFnvPrime; }
 

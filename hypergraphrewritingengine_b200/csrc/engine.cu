@@ -116,7 +116,13 @@ DevRule pack_rule(const RuleSpec& r) {
 
 uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
-Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, bool wl) {
+enum class LayoutKind { Count, Lane, Warp };
+
+// Shared-memory carve-up per warp. Count: the parent and the join. Lane: plus the parent's
+// per-vertex occurrence lists and a 32-match batch. Warp: plus the warp-per-child WL arrays.
+Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kind) {
+    const bool wl = kind == LayoutKind::Warp;
+    const bool lane = kind == LayoutKind::Lane;
     Layout L;
     std::memset(&L, 0, sizeof(L));
     NE = std::max<uint32_t>(NE, 1);
@@ -163,7 +169,7 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, bool wl) {
     L.o_pear = take(NE, 1);
     if (wl) L.o_car = take(L.CNE, 1);
     L.o_rule = take(sizeof(DevRule), 4);
-    if (wl) {
+    if (lane) {
         L.SB = rm.lhs + rm.rhs_total;
         L.o_poff = take(2 * (kLaneVMax + 1), 2);
         L.o_pocc = take(2 * NOCC, 2);
@@ -212,6 +218,7 @@ struct Engine::Impl {
     DVec<uint32_t> work, flag_new, scan_new, flag_rep, flag_front, new_state_event, level_max;
     DVec<uint32_t> bcount, boff, bpairs, scan_sums, sync_buf, root_ids;
     DVec<unsigned long long> stats, totals;
+    DVec<uint8_t> fmode;
 
     // host mirrors
     std::vector<DevRule> h_rules;
@@ -237,7 +244,8 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-        for (const void* k : {(const void*)k_count, (const void*)k_expand, (const void*)k_roots})
+        for (const void* k : {(const void*)k_count, (const void*)k_expand<true>,
+                              (const void*)k_expand<false>, (const void*)k_roots})
             HGX_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 static_cast<int>(kMaxDynSmem)));
         arena_top.ensure(1, 0, st);
@@ -245,7 +253,7 @@ struct Engine::Impl {
         work.ensure(8, 0, st);
         level_max.ensure(4, 0, st);
         sync_buf.ensure(16, 0, st);
-        stats.ensure(4, 0, st);
+        stats.ensure(8, 0, st);
         reset();
     }
 
@@ -271,6 +279,7 @@ struct Engine::Impl {
         evo_states.release(st);
         stats.release(st);
         totals.release(st);
+        fmode.release(st);
         rules.release(st);
         evos.release(st);
         cudaStreamSynchronize(st);
@@ -297,7 +306,7 @@ struct Engine::Impl {
         launches = 0;
         pending.clear();
         ev_used = 0;
-        HGX_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 4 * sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(stats.p, 0, 8 * sizeof(unsigned long long), st));
     }
 
     DevPtrs ptrs() const {
@@ -555,7 +564,7 @@ struct Engine::Impl {
         none.arity = rm.arity;
         uint32_t mne = *std::max_element(nes.begin(), nes.end());
         uint32_t mno = *std::max_element(noccs.begin(), noccs.end());
-        Layout L = make_layout(mne, mno, none, true);
+        Layout L = make_layout(mne, mno, none, LayoutKind::Warp);
         HGX_CUDA_CHECK(cudaMemsetAsync(work.p, 0, 8 * sizeof(uint32_t), st));
         LaunchShape s = warp_shape(k_roots, L, nr);
         tic();
@@ -655,13 +664,17 @@ struct Engine::Impl {
 
     void finish_times() {
         flush_times();
-        unsigned long long sv[4];
+        unsigned long long sv[8];
         HGX_CUDA_CHECK(cudaMemcpyAsync(sv, stats.p, sizeof(sv), cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         times.expand_bytes = sv[0];
         times.expand_hbm_bytes = sv[1];
         times.children = sv[2];
         times.wl_rounds = sv[3];
+        times.warp_bytes = sv[4];
+        times.warp_hbm_bytes = sv[5];
+        times.warp_children = sv[6];
+        times.warp_rounds = sv[7];
         times.launches = launches;
     }
 
@@ -704,7 +717,9 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemsetAsync(level_max.p, 0, 4 * sizeof(uint32_t), st));
 
         // ---- count
-        const Layout Lc = make_layout(ne_bound, nocc_bound, rm, false);
+        const Layout Lc = make_layout(ne_bound, nocc_bound, rm, LayoutKind::Count);
+        fmode.ensure(F, 0, st);
+        A.fmode = fmode.p;
         LaunchShape sc = warp_shape(k_count, Lc, F);
         tic();
         k_count<<<sc.grid, sc.block, sc.smem, st>>>(ptrs(), A, Lc);
@@ -781,8 +796,11 @@ struct Engine::Impl {
         // earlier event has been inserted.
         uint32_t F_eff = F;
         if (n_ev) {
-            const Layout Le = make_layout(std::max<uint32_t>(fmax_ne, 1), std::max<uint32_t>(fmax_nocc, 1), rm, true);
-            LaunchShape se = warp_shape(k_expand, Le, F);
+            const uint32_t mne = std::max<uint32_t>(fmax_ne, 1), mno = std::max<uint32_t>(fmax_nocc, 1);
+            const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane);
+            const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp);
+            LaunchShape sl = warp_shape(k_expand<true>, Ll, F);
+            LaunchShape sw = warp_shape(k_expand<false>, Lw, F);
             // chunking applies to a level holding one evolution whose cap this level can reach
             uint32_t only = kNone, n_in_level = 0;
             for (size_t e = 0; e < nevo; ++e)
@@ -807,12 +825,16 @@ struct Engine::Impl {
                 const uint32_t f1 = std::min<uint64_t>(F, uint64_t(f0) + chunk);
                 A.f_begin = f0;
                 A.f_end = f1;
-                HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, sizeof(uint32_t), st));
+                HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, 2 * sizeof(uint32_t), st));
                 tic();
-                k_expand<<<se.grid, se.block, se.smem, st>>>(ptrs(), A, Le);
+                k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 check_launch();
                 toc(times.expand);
                 ++times.expand_launches;
+                tic();
+                k_expand<false><<<sw.grid, sw.block, sw.smem, st>>>(ptrs(), A, Lw);
+                check_launch();
+                toc(times.expand_warp);
                 const uint32_t t0 = chunked ? h_item[uint64_t(f0) * R] : 0u;
                 const uint32_t t1 = chunked ? h_item[uint64_t(f1) * R] : n_ev;
                 tic();

@@ -77,14 +77,17 @@ struct RunOptions {
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.
 struct StageTimes {
-    double count = 0, scan = 0, expand = 0, select = 0, materialize = 0, branchial = 0,
-           roots = 0, total = 0;
+    double count = 0, scan = 0, expand = 0, expand_warp = 0, select = 0, materialize = 0,
+           branchial = 0, roots = 0, total = 0;
     uint64_t launches = 0;   // kernels this engine launched during the run
     uint64_t expand_launches = 0;
-    uint64_t expand_bytes = 0;       // per-stage algorithmic bytes of the expand kernel
-    uint64_t expand_hbm_bytes = 0;   // bytes the fused expand kernel must move to/from HBM
+    // lane-per-child expand kernel (k_expand<true>)
+    uint64_t expand_bytes = 0;       // per-stage algorithmic bytes
+    uint64_t expand_hbm_bytes = 0;   // bytes the fused kernel must move to/from HBM
     uint64_t children = 0;           // children built and WL-hashed
     uint64_t wl_rounds = 0;          // refinement rounds over all children
+    // warp-per-child expand kernel (k_expand<false>), same four figures
+    uint64_t warp_bytes = 0, warp_hbm_bytes = 0, warp_children = 0, warp_rounds = 0;
 };
 
 class Engine {

@@ -26,6 +26,7 @@ struct WlInfo {
 };
 
 HGX_HD void lane_isort64(uint64_t* a, uint32_t n) {
+        #pragma unroll 1
     for (uint32_t i = 1; i < n; ++i) {
         const uint64_t k = a[i];
         uint32_t j = i;
@@ -37,9 +38,11 @@ HGX_HD void lane_isort64(uint64_t* a, uint32_t n) {
 template <int VM>
 HGX_HD uint32_t lane_distinct(const uint64_t* cur, const uint16_t* deg, uint32_t V) {
     uint32_t d = 0;
+        #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         if (!deg[v]) continue;
         bool first = true;
+                #pragma unroll 1
         for (uint32_t u = 0; u < v && first; ++u)
             if (deg[u] && cur[u] == cur[v]) first = false;
         d += first ? 1u : 0u;
@@ -60,22 +63,28 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
     if (ne == 0) return kEmptyStateHash;
 
     uint64_t rmask = 0;
+        #pragma unroll 1
     for (uint32_t k = 0; k < R.n_lhs; ++k) rmask |= 1ull << rpos[k];
     uint16_t deg[VM], nn[VM];
+        #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         deg[v] = v < nvp ? pdeg[v] : 0;
         nn[v] = v < nvp ? pnn[v] : 0;
     }
+        #pragma unroll 1
     for (uint32_t k = 0; k < R.n_lhs; ++k) {
         const uint32_t e = rpos[k], a = pear[e], vo = pevo[e];
+                #pragma unroll 1
         for (uint32_t q = 0; q < a; ++q) {
             const uint32_t v = vloc[vo + q];
             deg[v] -= 1;
             nn[v] -= static_cast<uint16_t>(a - 1);
         }
     }
+        #pragma unroll 1
     for (uint32_t k = 0; k < R.n_rhs; ++k) {
         const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+                #pragma unroll 1
         for (uint32_t q = 0; q < a; ++q) {
             const uint32_t v = prodv[o + q];
             deg[v] += 1;
@@ -83,6 +92,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         }
     }
     uint32_t nv = 0, cap = 1, nocc = 0, nbr = 0;
+        #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         nv += deg[v] ? 1u : 0u;
         cap = nn[v] > cap ? nn[v] : cap;
@@ -96,23 +106,28 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
 
     uint64_t cur[VM], nxt[VM], buf[NM];
     // initial colours
+        #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         cur[v] = 0;
         if (!deg[v]) continue;
         uint32_t n = 0;
         const uint32_t j0 = v < nvp ? poff[v] : 0u, j1 = v < nvp ? poff[v + 1] : 0u;
+                #pragma unroll 1
         for (uint32_t j = j0; j < j1 && n < cap; ++j) {
             const uint32_t x = pocc[j], e = x >> 4;
             if ((rmask >> e) & 1ull) continue;
             buf[n++] = (static_cast<uint64_t>(pear[e]) << 8) | (x & 15u);
         }
+                #pragma unroll 1
         for (uint32_t k = 0; k < R.n_rhs; ++k) {
             const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+                        #pragma unroll 1
             for (uint32_t q = 0; q < a && n < cap; ++q)
                 if (prodv[o + q] == v) buf[n++] = (static_cast<uint64_t>(a) << 8) | q;
         }
         lane_isort64(buf, n);
         uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(deg[v]));
+                #pragma unroll 1
         for (uint32_t j = 0; j < n; ++j) {
             h = fnv(h, buf[j] >> 8);
             h = fnv(h, buf[j] & 0xFFu);
@@ -120,31 +135,40 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         cur[v] = h;
     }
     uint32_t prev = lane_distinct<VM>(cur, deg, V);
+        #pragma unroll 1
     for (uint32_t it = 0; it < kWlMaxRounds; ++it) {
+                #pragma unroll 1
         for (uint32_t v = 0; v < V; ++v) {
             if (!deg[v]) { nxt[v] = 0; continue; }
             uint32_t n = 0;
             const uint32_t j0 = v < nvp ? poff[v] : 0u, j1 = v < nvp ? poff[v + 1] : 0u;
+                        #pragma unroll 1
             for (uint32_t j = j0; j < j1; ++j) {
                 const uint32_t x = pocc[j], e = x >> 4;
                 if ((rmask >> e) & 1ull) continue;
                 const uint32_t q = x & 15u, a = pear[e], vo = pevo[e];
+                                #pragma unroll 1
                 for (uint32_t k = 0; k < a; ++k)
                     if (k != q && n < cap) buf[n++] = fnv(cur[vloc[vo + k]], k);
             }
+                        #pragma unroll 1
             for (uint32_t kk = 0; kk < R.n_rhs; ++kk) {
                 const uint32_t a = R.rhs_ar[kk], o = R.rhs_off[kk];
+                                #pragma unroll 1
                 for (uint32_t q = 0; q < a; ++q) {
                     if (prodv[o + q] != v) continue;
+                                        #pragma unroll 1
                     for (uint32_t t = 0; t < a; ++t)
                         if (t != q && n < cap) buf[n++] = fnv(cur[prodv[o + t]], t);
                 }
             }
             lane_isort64(buf, n);
             uint64_t h = cur[v];
+                        #pragma unroll 1
             for (uint32_t j = 0; j < n; ++j) h = fnv(h, buf[j]);
             nxt[v] = h;
         }
+                #pragma unroll 1
         for (uint32_t v = 0; v < V; ++v) cur[v] = nxt[v];
         const uint32_t d = lane_distinct<VM>(cur, deg, V);
         ++info.rounds;
@@ -154,54 +178,69 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
 
     // components (partition), then the commutative folds
     uint8_t comp[VM];
+        #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(v);
     auto find = [&](uint32_t x) -> uint32_t {
         while (comp[x] != x) { comp[x] = comp[comp[x]]; x = comp[x]; }
         return x;
     };
+        #pragma unroll 1
     for (uint32_t e = 0; e < pne; ++e) {
         if ((rmask >> e) & 1ull) continue;
         const uint32_t a = pear[e], vo = pevo[e];
         const uint32_t r = find(vloc[vo]);
+                #pragma unroll 1
         for (uint32_t q = 1; q < a; ++q) {
             const uint32_t x = find(vloc[vo + q]);
             if (x != r) comp[x] = static_cast<uint8_t>(r);
         }
     }
+        #pragma unroll 1
     for (uint32_t k = 0; k < R.n_rhs; ++k) {
         const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
         const uint32_t r = find(prodv[o]);
+                #pragma unroll 1
         for (uint32_t q = 1; q < a; ++q) {
             const uint32_t x = find(prodv[o + q]);
             if (x != r) comp[x] = static_cast<uint8_t>(r);
         }
     }
+        #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(find(v));
     uint64_t vs = 0, es = 0, cs = 0;
+        #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         nxt[v] = deg[v] ? smix(cur[v]) : 0;
         vs += nxt[v];
     }
+        #pragma unroll 1
     for (uint32_t e = 0; e < pne; ++e) {
         if ((rmask >> e) & 1ull) continue;
         const uint32_t a = pear[e], vo = pevo[e];
         uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(a));
+                #pragma unroll 1
         for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[vloc[vo + q]]);
         es += smix(h);
     }
+        #pragma unroll 1
     for (uint32_t k = 0; k < R.n_rhs; ++k) {
         const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
         uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(a));
+                #pragma unroll 1
         for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[prodv[o + q]]);
         es += smix(h);
     }
+        #pragma unroll 1
     for (uint32_t r = 0; r < V; ++r) {
         if (!deg[r] || comp[r] != r) continue;
         uint64_t col = 0, vc = 0, ec = 0;
+                #pragma unroll 1
         for (uint32_t v = 0; v < V; ++v)
             if (deg[v] && comp[v] == r) { col += nxt[v]; ++vc; }
+                #pragma unroll 1
         for (uint32_t e = 0; e < pne; ++e)
             if (!((rmask >> e) & 1ull) && comp[vloc[pevo[e]]] == r) ++ec;
+                #pragma unroll 1
         for (uint32_t k = 0; k < R.n_rhs; ++k)
             if (comp[prodv[R.rhs_off[k]]] == r) ++ec;
         cs += smix(fnv(fnv(kFnvOffset, (ec << 32) | vc), col));

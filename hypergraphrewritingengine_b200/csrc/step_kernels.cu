@@ -647,15 +647,33 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
         const uint32_t sid = A.frontier[f];
         const Parent pa = load_parent(P, L, sm, sid);
         const DevEvo ev = P.evos[P.st_evo[sid]];
+        // lane-per-child eligibility: few enough vertices and a bounded neighbour count
+        bool lane_ok = pa.nvp <= kLaneVMax && pa.ne <= kLaneEMax && pa.ne > 0;
+        uint32_t pnn_max = 0;
+        if (lane_ok) {
+            const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+            const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+            const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+            uint32_t nn = 0;
+            if (lane < pa.nvp)
+                for (uint32_t e = 0; e < pa.ne; ++e)
+                    for (uint32_t q = 0; q < pear[e]; ++q)
+                        if (vloc[pevo[e] + q] == lane) nn += pear[e] - 1u;
+            pnn_max = warp_max32(nn);
+        }
         for (uint32_t r = 0; r < A.rules_stride; ++r) {
             uint32_t cnt = 0;
             if (r < ev.rule_count) {
                 load_rule(sm, L, &P.rules[ev.rule_begin + r]);
+                uint32_t gain = 0;
+                for (uint32_t k = 0; k < R.n_rhs; ++k) gain += uint32_t(R.rhs_ar[k]) * (R.rhs_ar[k] - 1u);
+                lane_ok = lane_ok && pa.nvp + R.n_fresh <= kLaneVMax && pnn_max + gain <= kLaneNMax;
                 warp_join(L, sm, R, pa, [&](uint32_t) { ++cnt; });
             }
             if (lane == 0) A.counts[f * A.rules_stride + r] = cnt;
             __syncwarp();
         }
+        if (lane == 0) A.fmode[f] = lane_ok ? 1 : 0;
     }
 }
 
@@ -682,8 +700,11 @@ __global__ void k_item_sizes(DevPtrs P, LevelArgs A) {
 }
 
 // Enumerate again; mint events, produced edges and fresh vertices at the scanned offsets;
-// build and WL-hash every child in shared memory; insert the hash into the dedup table.
-__global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
+// hash every child; insert the hash into the dedup table. Two instantiations over the same
+// frontier range: kLane hashes the children of the states flagged by k_count one per lane,
+// the other one child per warp (states too large for a lane's private arrays).
+template <bool kLane>
+__global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layout L) {
     extern __shared__ __align__(16) char smem[];
     char* sm = smem + (threadIdx.x >> 5) * L.bytes;
     const uint32_t lane = lane_id();
@@ -693,18 +714,19 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
     const uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
     uint8_t* batch = smp<uint8_t>(sm, L.o_batch);
     uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
+    uint32_t* work = &A.work[kLane ? 1 : 2];
     while (true) {
         uint32_t f = 0;
-        if (lane == 0) f = A.f_begin + atomicAdd(&A.work[1], 1u);
+        if (lane == 0) f = A.f_begin + atomicAdd(work, 1u);
         f = __shfl_sync(0xFFFFFFFFu, f, 0);
         if (f >= A.f_end) break;
+        if ((A.fmode[f] != 0) != kLane) continue;
         const uint32_t sid = A.frontier[f];
         const Parent pa = load_parent(P, L, sm, sid);
         const uint32_t evo = P.st_evo[sid];
         const DevEvo ev = P.evos[evo];
         if (lane == 0) b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
-        const bool lane_ok = pa.nvp <= kLaneVMax && pa.ne <= kLaneEMax && pa.ne > 0;
-        const uint32_t pnn_max = lane_ok ? build_parent_csr(L, sm, pa) : 0u;
+        if (kLane) build_parent_csr(L, sm, pa);
         for (uint32_t r = 0; r < A.rules_stride && r < ev.rule_count; ++r) {
             const uint32_t item = f * A.rules_stride + r;
             if (lane == 0) b_stage += 4ull * pa.ne + 4ull * pa.nocc;   // join: ids and vertices
@@ -715,13 +737,6 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
             const uint32_t prod0 = A.prod_base + A.item_prod[item];
             const uint32_t fresh0 = A.fresh_base + A.item_fresh[item];
             const uint32_t rule_g = ev.rule_begin + r;
-            // neighbour-count bound of any child vertex under this rule
-            uint32_t gain = 0;
-            for (uint32_t k = 0; k < R.n_rhs; ++k) gain += uint32_t(R.rhs_ar[k]) * (R.rhs_ar[k] - 1u);
-            const uint32_t vneed = pa.nvp + R.n_fresh;
-            const int mode = !lane_ok ? 0
-                           : (vneed <= 16 && pnn_max + gain <= 48) ? 1
-                           : (vneed <= 32 && pnn_max + gain <= 64) ? 2 : 0;
             // per-child work shared by both paths: the event record and the table insert
             auto finish = [&](uint32_t idx, uint64_t h, const WlInfo& info, const uint8_t* rpos) {
                 const uint32_t e = ev0 + idx;
@@ -748,14 +763,13 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
                 n_child += 1;
                 n_rounds += info.rounds;
             };
-            if (mode) {
+            if constexpr (kLane) {
                 uint32_t nb = 0, done = 0;
                 auto flush = [&]() {
                     if (lane < nb) {
                         const uint8_t* slot = batch + lane * L.SB;
                         WlInfo info;
-                        const uint64_t h = (mode == 1) ? lane_wl<16, 48>(L, sm, pa, R, slot, info)
-                                                       : lane_wl<32, 64>(L, sm, pa, R, slot, info);
+                        const uint64_t h = lane_wl<kLaneVMax, kLaneNMax>(L, sm, pa, R, slot, info);
                         finish(done + lane, h, info, slot);
                     }
                     __syncwarp();
@@ -794,10 +808,11 @@ __global__ void k_expand(DevPtrs P, LevelArgs A, Layout L) {
     n_child = warp_sum64(n_child);
     n_rounds = warp_sum64(n_rounds);
     if (lane == 0 && b_hbm) {
-        atomicAdd(&P.stats[0], static_cast<unsigned long long>(b_stage));
-        atomicAdd(&P.stats[1], static_cast<unsigned long long>(b_hbm));
-        atomicAdd(&P.stats[2], static_cast<unsigned long long>(n_child));
-        atomicAdd(&P.stats[3], static_cast<unsigned long long>(n_rounds));
+        unsigned long long* st = P.stats + (kLane ? 0 : 4);
+        atomicAdd(&st[0], static_cast<unsigned long long>(b_stage));
+        atomicAdd(&st[1], static_cast<unsigned long long>(b_hbm));
+        atomicAdd(&st[2], static_cast<unsigned long long>(n_child));
+        atomicAdd(&st[3], static_cast<unsigned long long>(n_rounds));
     }
 }
 

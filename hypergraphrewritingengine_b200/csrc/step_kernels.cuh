@@ -60,9 +60,9 @@ struct DevPtrs {
     uint32_t* evo_stopped;
     // errors
     uint32_t* err;
-    // expand-kernel counters: [0] bytes by the per-stage figures (join + rewrite + WL + dedup
-    // as separate streams), [1] bytes the fused kernel must move to/from HBM, [2] children
-    // hashed, [3] WL refinement rounds run
+    // expand-kernel counters, [0..3] lane-per-child kernel, [4..7] warp-per-child kernel:
+    // bytes by the per-stage figures (join + rewrite + WL + dedup as separate streams), bytes the
+    // fused kernel must move to/from HBM, children hashed, WL refinement rounds run
     unsigned long long* stats;
 };
 
@@ -79,6 +79,7 @@ struct LevelArgs {
     uint32_t ev_base, cons_base, prod_base, fresh_base;   // level bases
     uint32_t n_events;          // events minted this level
     uint32_t f_begin, f_end;    // frontier range the expand kernel works on
+    uint8_t* fmode;             // [F] 1 = the state's children are hashed lane-per-child
     uint32_t* work;             // work-queue counters
     // select / assign
     uint32_t* flag_new;         // [n_events]

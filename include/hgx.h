@@ -167,10 +167,11 @@ HGX_API void hgx_result_free(hgx_result* result);
    launches: kernels launched by the call. */
 HGX_API hgx_status hgx_engine_stage_times(hgx_engine* engine, double* out_ms, uint64_t* launches);
 
-/* Counters of the last evolve call's expand kernel (the fused join + rewrite + WL + dedup
-   kernel): out[0] bytes by the per-stage figures (join + rewrite + WL + dedup counted as
-   separate HBM streams), out[1] bytes the fused kernel itself must move to or from HBM,
-   out[2] children hashed, out[3] WL refinement rounds, out[4] expand launches. */
+/* Counters of the last evolve call's expand kernels (the fused join + rewrite + WL + dedup
+   kernels). out[0..4], lane-per-child kernel: bytes by the per-stage figures (join + rewrite +
+   WL + dedup counted as separate HBM streams), bytes the fused kernel itself must move to or
+   from HBM, children hashed, WL refinement rounds, launches. out[5..8], warp-per-child kernel:
+   the same first four figures; out[9] its total device time in nanoseconds. */
 HGX_API hgx_status hgx_engine_expand_stats(hgx_engine* engine, uint64_t* out);
 
 /* The CUDA stream (cudaStream_t) the engine launches on, for callers that time or order
