@@ -46,7 +46,7 @@ EXPORTS = (
     "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_step",
     "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_device_bytes", "hgx_result_count",
     "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
-    "hgx_engine_stream",
+    "hgx_engine_stream", "hgx_hash_states_noalloc",
 )
 
 
@@ -98,6 +98,8 @@ def load_library(path: str = LIB_PATH):
         "hgx_engine_stage_times": ([vp, ctypes.POINTER(ctypes.c_double), u64p], ctypes.c_int),
         "hgx_engine_expand_stats": ([vp, u64p], ctypes.c_int),
         "hgx_engine_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
+        "hgx_hash_states_noalloc": ([vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_uint32, vp, vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

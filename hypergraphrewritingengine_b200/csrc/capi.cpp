@@ -154,6 +154,8 @@ hgx_status copy_out(const std::vector<T>& v, void* dst, size_t bytes) {
 
 }  // namespace
 
+void hgx::set_last_error(const std::string& msg) { g_err = msg; }
+
 extern "C" {
 
 const char* hgx_last_error(void) { return g_err.c_str(); }

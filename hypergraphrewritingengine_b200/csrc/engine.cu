@@ -5,7 +5,10 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+
+#include "../../include/hgx.h"
 
 #include "step_kernels.cu"
 
@@ -1158,3 +1161,159 @@ const StageTimes& Engine::times() const { return impl_->times; }
 void Engine::sync() { HGX_CUDA_CHECK(cudaStreamSynchronize(impl_->st)); }
 
 }  // namespace hgx
+
+// ==========================================================================================
+// Allocation-free state hashing (hgx_hash_states_noalloc).
+//
+// For callers that cannot call cudaMalloc: code running under a runtime that owns the device's
+// memory (a framework's caching allocator, a database or serving process with a fixed device
+// budget) where a foreign allocation breaks its accounting or fails outright, and code on a
+// latency-critical path where cudaMalloc's implicit device synchronisation is not acceptable.
+// They pass their own device buffers for inputs and outputs; the only scratch this needs -- the
+// dedup table, a work counter and an error word -- lives in the file-scope array below, which
+// every GPU that loads this library holds (kNoAllocScratchBytes) until the process exits.
+// ==========================================================================================
+
+namespace hgx {
+namespace {
+
+constexpr uint32_t kNoAllocMaxStates = 1u << 19;               // table load factor <= 1/2
+constexpr uint64_t kNoAllocSlots = 1ull << 20;                 // table capacity (power of two)
+constexpr uint64_t kNoAllocKeyBytes = (kNoAllocSlots + 1) * 8;
+constexpr uint64_t kNoAllocValBytes = (kNoAllocSlots + 1) * 4;
+constexpr uint64_t kNoAllocScratchBytes = kNoAllocKeyBytes + kNoAllocValBytes + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// The device address of g_noalloc_scratch, per device. In host code the symbol's name is only a
+// host-side handle, not a device address, so it is resolved once per device (with that device
+// current) through cudaGetSymbolAddress and the kernels are given the resolved pointer.
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+
+hgx_status noalloc_fail(hgx_status s, const std::string& msg) {
+    set_last_error(msg);
+    return s;
+}
+
+__global__ void k_noalloc_classes(DevPtrs P, DevEvo ev, const uint64_t* hash, uint32_t n,
+                                  uint32_t* cls) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        cls[i] = table_lookup(P, ev, hash[i]);
+}
+
+// Warp per state: WL hash into hash[i], then insert (hash, i) into the table (smallest i wins).
+__global__ void __launch_bounds__(256) k_noalloc_hash(DevPtrs P, DevEvo ev, uint32_t n,
+                                                     uint32_t* work, uint64_t* hash, Layout L) {
+    extern __shared__ __align__(16) char smem[];
+    char* sm = smem + (threadIdx.x >> 5) * L.bytes;
+    const uint32_t lane = lane_id();
+    while (true) {
+        uint32_t i = 0;
+        if (lane == 0) i = atomicAdd(work, 1u);
+        i = __shfl_sync(0xFFFFFFFFu, i, 0);
+        if (i >= n) break;
+        const Parent pa = load_parent(P, L, sm, i);
+        uint8_t* car = smp<uint8_t>(sm, L.o_car);
+        uint16_t* cvo = smp<uint16_t>(sm, L.o_cvo);
+        const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+        const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+        for (uint32_t e = lane; e < pa.ne; e += 32) { car[e] = pear[e]; cvo[e] = pevo[e]; }
+        __syncwarp();
+        WlInfo info;
+        const uint64_t h = warp_wl(L, sm, pa.ne, pa.nvp, info);
+        if (lane == 0) {
+            hash[i] = h;
+            table_insert(P, ev, h, i);
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+}  // namespace hgx
+
+extern "C" HGX_API hgx_status hgx_hash_states_noalloc(
+    const uint32_t* d_records, const uint64_t* d_offsets, const uint32_t* d_num_edges,
+    const uint32_t* d_num_occ, uint32_t n_states, uint32_t max_edges, uint32_t max_occ,
+    uint64_t* d_hash, uint32_t* d_class, void* stream) {
+    using namespace hgx;
+    try {
+        if (n_states > kNoAllocMaxStates)
+            return noalloc_fail(HGX_ERR_CAPACITY,
+                                "hgx_hash_states_noalloc: " + std::to_string(n_states) +
+                                    " states exceed the maximum of " +
+                                    std::to_string(kNoAllocMaxStates) + " per call");
+        if (n_states == 0) return HGX_OK;
+        if (!d_records || !d_offsets || !d_num_edges || !d_num_occ || !d_hash || !d_class)
+            return noalloc_fail(HGX_ERR_INVALID, "hgx_hash_states_noalloc: null device pointer");
+        if (max_edges == 0 || max_occ == 0)
+            return noalloc_fail(HGX_ERR_INVALID, "hgx_hash_states_noalloc: max_edges and max_occ must be > 0");
+        RuleMax rm;
+        rm.arity = kMaxArity;
+        const Layout L = make_layout(max_edges, max_occ, rm, LayoutKind::Warp);
+        if (L.bytes > kMaxDynSmem)
+            return noalloc_fail(HGX_ERR_CAPACITY,
+                                "hgx_hash_states_noalloc: states of this size exceed shared memory");
+        int dev = 0;
+        HGX_CUDA_CHECK(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return noalloc_fail(HGX_ERR_INVALID, "device index out of range");
+        unsigned char* base = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(g_noalloc_mu);
+            if (!g_noalloc_ptr[dev]) {   // first call on this device: resolve the scratch address
+                void* p = nullptr;
+                const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+                if (e != cudaSuccess || !p)
+                    return noalloc_fail(HGX_ERR_CUDA, std::string("cudaGetSymbolAddress failed: ") +
+                                                          cudaGetErrorString(e));
+                HGX_CUDA_CHECK(cudaFuncSetAttribute(k_noalloc_hash,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    static_cast<int>(kMaxDynSmem)));
+                g_noalloc_ptr[dev] = p;
+            }
+            base = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+        }
+        unsigned long long* keys = reinterpret_cast<unsigned long long*>(base);
+        uint32_t* vals = reinterpret_cast<uint32_t*>(base + kNoAllocKeyBytes);
+        uint32_t* counters = reinterpret_cast<uint32_t*>(base + kNoAllocKeyBytes + kNoAllocValBytes);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        // a table of at least twice the states; the array keeps the previous call's contents,
+        // so the used region and the counters are cleared first
+        uint64_t cap = 256;
+        while (cap < 2ull * n_states) cap <<= 1;
+        DevEvo ev;
+        std::memset(&ev, 0, sizeof(ev));
+        ev.table_off = 0;
+        ev.table_mask = cap - 1;
+        // slots [0, cap) plus the key-0 slot at index cap
+        HGX_CUDA_CHECK(cudaMemsetAsync(keys, 0, (cap + 1) * 8, st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(vals, 0xFF, (cap + 1) * 4, st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(counters, 0, 8, st));
+        DevPtrs P;
+        std::memset(&P, 0, sizeof(P));
+        P.arena = const_cast<uint32_t*>(d_records);
+        P.st_off = const_cast<uint64_t*>(d_offsets);
+        P.st_ne = const_cast<uint32_t*>(d_num_edges);
+        P.st_nocc = const_cast<uint32_t*>(d_num_occ);
+        P.tab_keys = keys;
+        P.tab_vals = vals;
+        P.err = counters + 1;
+        const uint32_t wpb = static_cast<uint32_t>(std::min<size_t>(8, std::max<size_t>(1, (96 * 1024) / L.bytes)));
+        const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((n_states + wpb - 1) / wpb, kNumSMs * 4));
+        k_noalloc_hash<<<grid, 32 * wpb, L.bytes * wpb, st>>>(P, ev, n_states, counters, d_hash, L);
+        HGX_CUDA_CHECK(cudaGetLastError());
+        k_noalloc_classes<<<(n_states + 255) / 256, 256, 0, st>>>(P, ev, d_hash, n_states, d_class);
+        HGX_CUDA_CHECK(cudaGetLastError());
+        uint32_t err = 0;
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&err, counters + 1, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (err)
+            return noalloc_fail(HGX_ERR_CAPACITY, "hgx_hash_states_noalloc: a state exceeds max_edges / "
+                                                  "max_occ, or the table overflowed (flags " +
+                                                  std::to_string(err) + ")");
+        return HGX_OK;
+    } catch (const std::exception& e) {
+        return noalloc_fail(HGX_ERR_CUDA, e.what());
+    }
+}

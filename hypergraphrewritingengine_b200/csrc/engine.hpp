@@ -90,6 +90,9 @@ struct StageTimes {
     uint64_t warp_bytes = 0, warp_hbm_bytes = 0, warp_children = 0, warp_rounds = 0;
 };
 
+// Message returned by hgx_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
+
 class Engine {
 public:
     explicit Engine(int device = 0);

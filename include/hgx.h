@@ -178,6 +178,35 @@ HGX_API hgx_status hgx_engine_expand_stats(hgx_engine* engine, uint64_t* out);
    work against it. */
 HGX_API hgx_status hgx_engine_stream(hgx_engine* engine, void** stream);
 
+/* Allocation-free WL hashing and deduplication of a batch of states that are already on the
+   device. No counterpart in the reference: it exists for callers that cannot call cudaMalloc --
+   code running under a runtime that owns the device's memory (a framework's caching allocator,
+   a database or serving process with a fixed device budget) and code on a latency-critical path
+   that cannot take cudaMalloc's implicit device synchronisation. It allocates nothing: the caller
+   passes device buffers for the inputs and the outputs, and the scratch it needs (a dedup table
+   of 2^20 slots, a work counter, an error word; about 12 MB) is a fixed array inside the library
+   that every GPU which loads the library holds until the process exits.
+
+   Inputs (device memory): states in the engine's record layout, concatenated in d_records; for
+   state i, its record starts at word d_offsets[i] and holds d_num_edges[i] edge ids (any values;
+   they only fix the edge order), then the edge arities packed four per 32-bit word (edge k in
+   byte k % 4 of word k / 4), then the d_num_occ[i] vertex ids of the edges in order. max_edges /
+   max_occ bound d_num_edges / d_num_occ and size the per-warp shared memory.
+   Outputs (device memory): d_hash[i] = WL canonical hash of state i (bit-identical to the
+   evolve path's state hashes); d_class[i] = the smallest index j with d_hash[j] == d_hash[i].
+
+   At most 524,288 states per call (larger n_states is rejected with HGX_ERR_CAPACITY before any
+   GPU work). The first call on a device resolves the array's device address (and sets the
+   kernel's shared-memory limit) with that device current; make that first call before any stream
+   capture. Every call clears and reuses the same array, so calls that overlap on the GPU (from
+   two streams or two threads) race: serialise them. The call runs on `stream` (a cudaStream_t,
+   NULL = legacy default stream) and synchronises it before returning, to report device-side
+   errors (a state larger than the declared bounds). */
+HGX_API hgx_status hgx_hash_states_noalloc(const uint32_t* d_records, const uint64_t* d_offsets,
+                                           const uint32_t* d_num_edges, const uint32_t* d_num_occ,
+                                           uint32_t n_states, uint32_t max_edges, uint32_t max_occ,
+                                           uint64_t* d_hash, uint32_t* d_class, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
