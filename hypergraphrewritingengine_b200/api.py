@@ -46,7 +46,7 @@ EXPORTS = (
     "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_step",
     "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_device_bytes", "hgx_result_count",
     "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
-    "hgx_engine_stream", "hgx_hash_states_noalloc",
+    "hgx_engine_stream", "hgx_hash_states_noalloc", "hgx_result_view",
 )
 
 
@@ -95,6 +95,7 @@ def load_library(path: str = LIB_PATH):
         "hgx_result_count": ([vp, ctypes.c_int], ctypes.c_uint64),
         "hgx_result_copy": ([vp, ctypes.c_int, vp, ctypes.c_size_t], ctypes.c_int),
         "hgx_result_free": ([vp], None),
+        "hgx_result_view": ([vp, ctypes.c_int, ctypes.POINTER(vp), u64p], ctypes.c_int),
         "hgx_engine_stage_times": ([vp, ctypes.POINTER(ctypes.c_double), u64p], ctypes.c_int),
         "hgx_engine_expand_stats": ([vp, u64p], ctypes.c_int),
         "hgx_engine_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
@@ -202,24 +203,44 @@ class EvolveResult:
             "state_vert_off", "state_verts"))
 
 
+class _ResultOwner:
+    """Frees an hgx_result once no numpy view of its memory is left."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def __del__(self):
+        try:
+            load_library().hgx_result_free(self.handle)
+        except Exception:
+            pass
+
+
+_ARR_TYPES = {ARR_STATE_HASH: np.uint64}
+_ARR_SHAPES = {ARR_EVENTS: 4, ARR_CAUSAL: 3, ARR_BRANCHIAL: 2, ARR_EVENT_PROD: 2}
+
+
 def _read_result(handle) -> EvolveResult:
+    """Zero-copy: every array is a numpy view of the result's host memory (page-locked for a
+    single-evolution result); the handle is freed when the last view is released."""
     L = load_library()
+    owner = _ResultOwner(handle)
     cnt = lambda w: int(L.hgx_result_count(handle, w))  # noqa: E731
-    ns, ne, nc, nb = cnt(COUNT_STATES), cnt(COUNT_EVENTS), cnt(COUNT_CAUSAL), cnt(COUNT_BRANCHIAL)
-    ncons, nse, nsv = cnt(COUNT_CONSUMED), cnt(COUNT_STATE_EDGES), cnt(COUNT_STATE_VERTS)
-    has_edges = nse > 0
-    arrays = {
-        ARR_STATE_HASH: np.empty(ns, np.uint64), ARR_STATE_DEPTH: np.empty(ns, np.uint32),
-        ARR_EVENTS: np.empty((ne, 4), np.uint32), ARR_CAUSAL: np.empty((nc, 3), np.uint32),
-        ARR_BRANCHIAL: np.empty((nb, 2), np.uint32), ARR_EVENT_CONS_OFF: np.empty(ne + 1, np.uint32),
-        ARR_EVENT_CONS: np.empty(ncons, np.uint32), ARR_EVENT_PROD: np.empty((ne, 2), np.uint32),
-        ARR_STATE_EDGE_OFF: np.empty(ns + 1 if has_edges else 1, np.uint32),
-        ARR_STATE_EDGE_IDS: np.empty(nse, np.uint32), ARR_STATE_ARITY: np.empty(nse, np.uint32),
-        ARR_STATE_VERT_OFF: np.empty(ns + 1 if has_edges else 1, np.uint32),
-        ARR_STATE_VERTS: np.empty(nsv, np.uint32),
-    }
-    for what, a in arrays.items():
-        _check(L.hgx_result_copy(handle, what, a.ctypes.data_as(ctypes.c_void_p), a.nbytes))
+    arrays = {}
+    for what in range(13):
+        ptr = ctypes.c_void_p()
+        n = ctypes.c_uint64()
+        _check(L.hgx_result_view(handle, what, ctypes.byref(ptr), ctypes.byref(n)))
+        dt = _ARR_TYPES.get(what, np.uint32)
+        n = int(n.value)
+        if n == 0 or not ptr.value:
+            a = np.zeros(0, dt)
+        else:
+            buf = (ctypes.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr.value)
+            buf._owner = owner
+            a = np.frombuffer(buf, dtype=dt)
+        w = _ARR_SHAPES.get(what)
+        arrays[what] = a.reshape(-1, w) if w else a
     return EvolveResult(
         state_hash=arrays[ARR_STATE_HASH], state_depth=arrays[ARR_STATE_DEPTH],
         events=arrays[ARR_EVENTS], causal=arrays[ARR_CAUSAL], branchial=arrays[ARR_BRANCHIAL],
@@ -270,10 +291,7 @@ class Engine:
         rb = encode_roots(roots)
         out = ctypes.c_void_p()
         _check(L.hgx_evolve(self._h, _u32p(rb), len(rb), int(steps), ctypes.byref(out)))
-        try:
-            return _read_result(out)
-        finally:
-            L.hgx_result_free(out)
+        return _read_result(out.value)
 
     @staticmethod
     def make_jobs(evolutions):
@@ -293,13 +311,7 @@ class Engine:
         n = len(jobs)
         outs = (ctypes.c_void_p * n)()
         _check(self._L.hgx_evolve_batch(self._h, jobs, n, outs))
-        res = []
-        for i in range(n):
-            try:
-                res.append(_read_result(outs[i]))
-            finally:
-                self._L.hgx_result_free(outs[i])
-        return res
+        return [_read_result(outs[i]) for i in range(n)]
 
     # --- serving ---
     def serve_reset(self):
@@ -324,10 +336,7 @@ class Engine:
     def serve_collect(self, evo: int) -> EvolveResult:
         out = ctypes.c_void_p()
         _check(self._L.hgx_serve_collect(self._h, int(evo), ctypes.byref(out)))
-        try:
-            return _read_result(out)
-        finally:
-            self._L.hgx_result_free(out)
+        return _read_result(out.value)
 
     def device_bytes(self) -> int:
         b = ctypes.c_uint64()

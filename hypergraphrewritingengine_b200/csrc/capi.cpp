@@ -19,8 +19,10 @@ struct hgx_engine {
 
 struct hgx_result {
     hgx::EvolutionResult r;
-    std::vector<uint32_t> events_flat;   // (in, out, rule, step)
+    std::vector<uint32_t> events_flat;   // (in, out, rule, step) for vector-held results
     std::vector<uint32_t> prod_flat;     // (first, count)
+    const void* ptr[13] = {};            // every array, indexed by hgx_array
+    uint64_t count[13] = {};             // elements
 };
 
 namespace {
@@ -127,7 +129,14 @@ hgx::EvolutionSpec spec_of(const hgx_job& j) {
 hgx_result* wrap(hgx::EvolutionResult&& r) {
     auto* out = new hgx_result;
     out->r = std::move(r);
-    const auto& x = out->r;
+    auto& x = out->r;
+    if (x.flat) {
+        for (int i = 0; i < 13; ++i) {
+            out->ptr[i] = x.flat->ptr[i];
+            out->count[i] = x.flat->count[i];
+        }
+        return out;
+    }
     out->events_flat.resize(4 * x.ev_in.size());
     out->prod_flat.resize(2 * x.ev_in.size());
     for (size_t i = 0; i < x.ev_in.size(); ++i) {
@@ -138,18 +147,28 @@ hgx_result* wrap(hgx::EvolutionResult&& r) {
         out->prod_flat[2 * i] = x.ev_prod_first[i];
         out->prod_flat[2 * i + 1] = x.ev_prod_count[i];
     }
-    if (out->r.ev_cons_off.empty()) out->r.ev_cons_off.push_back(0);
-    if (out->r.state_edge_off.empty()) out->r.state_edge_off.push_back(0);
-    if (out->r.state_vert_off.empty()) out->r.state_vert_off.push_back(0);
+    if (x.ev_cons_off.empty()) x.ev_cons_off.push_back(0);
+    if (x.state_edge_off.empty()) x.state_edge_off.push_back(0);
+    if (x.state_vert_off.empty()) x.state_vert_off.push_back(0);
+    for (uint32_t ev : x.state_event) x.n_roots += (ev == 0xFFFFFFFFu) ? 1 : 0;
+    auto set = [&](int i, const auto& v) {
+        out->ptr[i] = v.data();
+        out->count[i] = v.size();
+    };
+    set(HGX_ARR_STATE_HASH, x.state_hash);
+    set(HGX_ARR_STATE_DEPTH, x.state_depth);
+    set(HGX_ARR_EVENTS, out->events_flat);
+    set(HGX_ARR_CAUSAL, x.causal);
+    set(HGX_ARR_BRANCHIAL, x.branchial);
+    set(HGX_ARR_EVENT_CONS_OFF, x.ev_cons_off);
+    set(HGX_ARR_EVENT_CONS, x.ev_cons);
+    set(HGX_ARR_EVENT_PROD, out->prod_flat);
+    set(HGX_ARR_STATE_EDGE_OFF, x.state_edge_off);
+    set(HGX_ARR_STATE_EDGE_IDS, x.state_edge_ids);
+    set(HGX_ARR_STATE_ARITY, x.state_arity);
+    set(HGX_ARR_STATE_VERT_OFF, x.state_vert_off);
+    set(HGX_ARR_STATE_VERTS, x.state_verts);
     return out;
-}
-
-template <class T>
-hgx_status copy_out(const std::vector<T>& v, void* dst, size_t bytes) {
-    const size_t need = v.size() * sizeof(T);
-    if (bytes < need) return fail(HGX_ERR_INVALID, "hgx_result_copy: destination too small");
-    if (need) std::memcpy(dst, v.data(), need);
-    return HGX_OK;
 }
 
 }  // namespace
@@ -303,43 +322,35 @@ uint64_t hgx_result_count(const hgx_result* res, hgx_count what) {
         }
     }
     switch (what) {
-        case HGX_COUNT_STATES: return r.state_hash.size();
-        case HGX_COUNT_EVENTS: return r.ev_in.size();
+        case HGX_COUNT_STATES: return res->count[HGX_ARR_STATE_HASH];
+        case HGX_COUNT_EVENTS: return res->count[HGX_ARR_EVENTS] / 4;
         case HGX_COUNT_CLASSES: return r.num_classes;
-        case HGX_COUNT_CAUSAL: return r.causal.size() / 3;
-        case HGX_COUNT_BRANCHIAL: return r.branchial.size() / 2;
+        case HGX_COUNT_CAUSAL: return res->count[HGX_ARR_CAUSAL] / 3;
+        case HGX_COUNT_BRANCHIAL: return res->count[HGX_ARR_BRANCHIAL] / 2;
         case HGX_COUNT_TRUNCATED: return r.truncated ? 1 : 0;
-        case HGX_COUNT_CONSUMED: return r.ev_cons.size();
-        case HGX_COUNT_STATE_EDGES: return r.state_edge_ids.size();
-        case HGX_COUNT_STATE_VERTS: return r.state_verts.size();
-        case HGX_COUNT_RAW_STATES: {
-            uint64_t roots = 0;
-            for (uint32_t ev : r.state_event) roots += (ev == 0xFFFFFFFFu) ? 1 : 0;
-            return roots + r.ev_in.size();
-        }
+        case HGX_COUNT_CONSUMED: return res->count[HGX_ARR_EVENT_CONS];
+        case HGX_COUNT_STATE_EDGES: return res->count[HGX_ARR_STATE_EDGE_IDS];
+        case HGX_COUNT_STATE_VERTS: return res->count[HGX_ARR_STATE_VERTS];
+        case HGX_COUNT_RAW_STATES: return r.n_roots + res->count[HGX_ARR_EVENTS] / 4;
     }
     return 0;
 }
 
 hgx_status hgx_result_copy(const hgx_result* res, hgx_array what, void* dst, size_t bytes) {
     if (!res || (!dst && bytes)) return fail(HGX_ERR_INVALID, "null argument");
-    const auto& r = res->r;
-    switch (what) {
-        case HGX_ARR_STATE_HASH: return copy_out(r.state_hash, dst, bytes);
-        case HGX_ARR_STATE_DEPTH: return copy_out(r.state_depth, dst, bytes);
-        case HGX_ARR_EVENTS: return copy_out(res->events_flat, dst, bytes);
-        case HGX_ARR_CAUSAL: return copy_out(r.causal, dst, bytes);
-        case HGX_ARR_BRANCHIAL: return copy_out(r.branchial, dst, bytes);
-        case HGX_ARR_EVENT_CONS_OFF: return copy_out(r.ev_cons_off, dst, bytes);
-        case HGX_ARR_EVENT_CONS: return copy_out(r.ev_cons, dst, bytes);
-        case HGX_ARR_EVENT_PROD: return copy_out(res->prod_flat, dst, bytes);
-        case HGX_ARR_STATE_EDGE_OFF: return copy_out(r.state_edge_off, dst, bytes);
-        case HGX_ARR_STATE_EDGE_IDS: return copy_out(r.state_edge_ids, dst, bytes);
-        case HGX_ARR_STATE_ARITY: return copy_out(r.state_arity, dst, bytes);
-        case HGX_ARR_STATE_VERT_OFF: return copy_out(r.state_vert_off, dst, bytes);
-        case HGX_ARR_STATE_VERTS: return copy_out(r.state_verts, dst, bytes);
-    }
-    return fail(HGX_ERR_INVALID, "unknown array");
+    if (static_cast<int>(what) < 0 || static_cast<int>(what) >= 13) return fail(HGX_ERR_INVALID, "unknown array");
+    const size_t need = res->count[what] * (what == HGX_ARR_STATE_HASH ? 8 : 4);
+    if (bytes < need) return fail(HGX_ERR_INVALID, "hgx_result_copy: destination too small");
+    if (need) std::memcpy(dst, res->ptr[what], need);
+    return HGX_OK;
+}
+
+hgx_status hgx_result_view(const hgx_result* res, hgx_array what, const void** ptr, uint64_t* count) {
+    if (!res || !ptr || !count) return fail(HGX_ERR_INVALID, "null argument");
+    if (static_cast<int>(what) < 0 || static_cast<int>(what) >= 13) return fail(HGX_ERR_INVALID, "unknown array");
+    *ptr = res->ptr[what];
+    *count = res->count[what];
+    return HGX_OK;
 }
 
 void hgx_result_free(hgx_result* r) { delete r; }

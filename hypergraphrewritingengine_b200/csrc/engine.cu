@@ -188,6 +188,46 @@ struct LaunchShape {
     uint32_t grid, block, smem;
 };
 
+// Page-locked host blocks for results, recycled when a result is freed. Shared with the results
+// it hands out, so a result may outlive the engine that produced it.
+struct PinnedPool {
+    std::mutex mu;
+    std::vector<std::pair<size_t, void*>> free_blocks;
+    ~PinnedPool() {
+        for (auto& b : free_blocks) cudaFreeHost(b.second);
+    }
+    void* get(size_t bytes, size_t& cap) {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            size_t best = free_blocks.size();
+            for (size_t i = 0; i < free_blocks.size(); ++i)
+                if (free_blocks[i].first >= bytes &&
+                    (best == free_blocks.size() || free_blocks[i].first < free_blocks[best].first))
+                    best = i;
+            if (best != free_blocks.size()) {
+                auto b = free_blocks[best];
+                free_blocks.erase(free_blocks.begin() + best);
+                cap = b.first;
+                return b.second;
+            }
+        }
+        cap = 1 << 20;
+        while (cap < bytes) cap <<= 1;
+        void* p = nullptr;
+        HGX_CUDA_CHECK(cudaHostAlloc(&p, cap, cudaHostAllocDefault));
+        return p;
+    }
+    void put(void* p, size_t cap) {
+        std::lock_guard<std::mutex> lock(mu);
+        free_blocks.emplace_back(cap, p);
+        if (free_blocks.size() > 4) {   // keep a few blocks; return the smallest to the system
+            auto it = std::min_element(free_blocks.begin(), free_blocks.end());
+            cudaFreeHost(it->second);
+            free_blocks.erase(it);
+        }
+    }
+};
+
 }  // namespace
 
 // ==========================================================================================
@@ -221,7 +261,10 @@ struct Engine::Impl {
     DVec<uint32_t> work, flag_new, scan_new, flag_rep, flag_front, new_state_event, level_max;
     DVec<uint32_t> bcount, boff, bpairs, scan_sums, sync_buf, root_ids;
     DVec<unsigned long long> stats, totals;
-    DVec<uint8_t> fmode;
+    DVec<uint8_t> fmode, fin;
+    DVec<uint32_t> fin_cnt;
+    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
+    uint64_t n_roots_admitted = 0;
 
     // host mirrors
     std::vector<DevRule> h_rules;
@@ -283,6 +326,8 @@ struct Engine::Impl {
         stats.release(st);
         totals.release(st);
         fmode.release(st);
+        fin.release(st);
+        fin_cnt.release(st);
         rules.release(st);
         evos.release(st);
         cudaStreamSynchronize(st);
@@ -300,6 +345,7 @@ struct Engine::Impl {
         finished.clear();
         rm = RuleMax{};
         n_states = n_edges = n_events = n_cons = n_bpairs = 0;
+        n_roots_admitted = 0;
         next_vertex = arena_words = tab_slots = 0;
         frontier_size = 0;
         ne_bound = nocc_bound = 1;
@@ -559,6 +605,7 @@ struct Engine::Impl {
         up(state_of_arrival.p + a0, h_sid);
         n_states += nr;
         n_events += nr;
+        n_roots_admitted += nr;
 
         // hash the roots on the device and seed the table
         root_ids.ensure(nr, 0, st);
@@ -635,6 +682,131 @@ struct Engine::Impl {
 
     void read_results(const std::vector<uint32_t>& which, const RunOptions& opt,
                       std::vector<EvolutionResult>& out);
+
+
+    // Single-evolution result, finalised on the device and copied to a pinned block at once.
+    EvolutionResult finalize_single(const RunOptions& opt) {
+        EvolutionResult r;
+        const uint32_t R = static_cast<uint32_t>(n_roots_admitted);
+        uint32_t cut = kNone, stopped = 0;
+        unsigned long long classes = 0;
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&cut, evo_cut.p, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&stopped, evo_stopped.p, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&classes, evo_classes.p, 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        const uint64_t e_end = stopped ? std::min<uint64_t>(n_events, cut) : n_events;
+        const uint32_t E = static_cast<uint32_t>(e_end - R);
+        const uint32_t S = static_cast<uint32_t>(n_states);
+        const uint64_t B = opt.branchial ? n_bpairs : 0;
+        // consumed lists of the kept events are one contiguous range [c0, c0 + C)
+        uint32_t c0 = 0, clast = 0, rlast = 0;
+        if (E) {
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&c0, ev_coff.p + R, 4, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&clast, ev_coff.p + e_end - 1, 4, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&rlast, ev_rule.p + e_end - 1, 4, cudaMemcpyDeviceToHost, st));
+        }
+        // causal counts and state CSR offsets
+        fin_cnt.ensure(uint64_t(E) + 1 + 2ull * (S + 1), 0, st);
+        uint32_t* ccnt = fin_cnt.p;                 // [E+1] counts, then scanned in place
+        uint32_t* eoff = fin_cnt.p + E + 1;         // [S+1]
+        uint32_t* voff = eoff + S + 1;              // [S+1]
+        if (E && opt.causal) {
+            k_fin_causal<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), R, E, ccnt, nullptr, nullptr, 0);
+            check_launch();
+            scan(ccnt, ccnt, E);
+        } else {
+            HGX_CUDA_CHECK(cudaMemsetAsync(ccnt + E, 0, 4, st));
+        }
+        if (opt.keep_state_edges) {
+            scan(st_ne.p, eoff, S);
+            scan(st_nocc.p, voff, S);
+        }
+        uint32_t K = 0, T = 0, V = 0;
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&K, ccnt + E, 4, cudaMemcpyDeviceToHost, st));
+        if (opt.keep_state_edges) {
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&T, eoff + S, 4, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&V, voff + S, 4, cudaMemcpyDeviceToHost, st));
+        }
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        const uint32_t C = E ? clast + h_rules[rlast].n_lhs - c0 : 0;
+        const bool se = opt.keep_state_edges;
+        // host block layout (hgx_array order), 16-byte aligned sections
+        uint64_t count[ResultArrays::kArrays] = {
+            S, S, 4ull * E, 3ull * K, 2 * B, uint64_t(E) + 1, C, 2ull * E,
+            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0};
+        uint64_t off[ResultArrays::kArrays];
+        uint64_t total = 0;
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            off[i] = total;
+            total += (count[i] * (i == 0 ? 8 : 4) + 15) / 16 * 16;
+        }
+        // device staging for the derived arrays (same layout; direct arrays are copied from
+        // their own device buffers)
+        fin.ensure(total, 0, st);
+        uint8_t* d = fin.p;
+        auto dp = [&](int i) { return reinterpret_cast<uint32_t*>(d + off[i]); };
+        if (E) {
+            k_fin_events<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), R, E, h_evos[0].rule_begin, dp(2),
+                                                             dp(5), dp(7), c0);
+            check_launch();
+            HGX_CUDA_CHECK(cudaMemcpyAsync(dp(5) + E, &C, 4, cudaMemcpyHostToDevice, st));
+        } else {
+            HGX_CUDA_CHECK(cudaMemsetAsync(dp(5), 0, 4, st));
+        }
+        if (K) {
+            k_fin_causal<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), R, E, nullptr, ccnt, dp(3), 1);
+            check_launch();
+        }
+        if (B) {
+            k_fin_shift<<<grid_for(2 * B, 256), 256, 0, st>>>(bpairs.p, 2 * B, R, dp(4));
+            check_launch();
+        }
+        if (se) {
+            k_fin_states<<<grid_for(uint64_t(S) * 32, 256), 256, 0, st>>>(ptrs(), S, eoff, voff, dp(9),
+                                                                         dp(10), dp(12));
+            check_launch();
+        } else {
+            HGX_CUDA_CHECK(cudaMemsetAsync(dp(8), 0, 4, st));
+            HGX_CUDA_CHECK(cudaMemsetAsync(dp(11), 0, 4, st));
+        }
+        size_t cap = 0;
+        uint8_t* h = static_cast<uint8_t*>(pinned->get(total, cap));
+        auto pool = pinned;
+        auto flat = std::make_shared<ResultArrays>();
+        flat->owner = std::shared_ptr<void>(h, [pool, cap](void* p) { pool->put(p, cap); });
+        auto d2h_from = [&](int i, const void* src) {
+            const size_t bytes = count[i] * (i == 0 ? 8 : 4);
+            if (bytes) HGX_CUDA_CHECK(cudaMemcpyAsync(h + off[i], src, bytes, cudaMemcpyDeviceToHost, st));
+        };
+        d2h_from(0, st_hash.p);
+        d2h_from(1, st_depth.p);
+        d2h_from(6, ev_cons.p + c0);
+        if (se) {
+            d2h_from(8, eoff);
+            d2h_from(11, voff);
+        }
+        // the derived sections, in one copy from the first through the last derived array
+        for (int i : {2, 3, 4, 5, 7}) d2h_from(i, d + off[i]);
+        if (se) for (int i : {9, 10, 12}) d2h_from(i, d + off[i]);
+        if (!se) {
+            std::memset(h + off[8], 0, 4);
+            std::memset(h + off[11], 0, 4);
+        }
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            flat->ptr[i] = h + off[i];
+            flat->count[i] = count[i];
+        }
+        r.flat = flat;
+        r.n_roots = R;
+        r.num_classes = classes;
+        r.truncated = stopped != 0;
+        if (r.truncated)
+            r.warnings.push_back(
+                "capacity limit reached: the state cap stopped the evolution; the states, events "
+                "and relations returned are valid and incomplete");
+        return r;
+    }
 
     // Counts only (results stay on the device).
     void read_counts(const std::vector<uint32_t>& which, std::vector<EvolutionResult>& out) {
@@ -1116,8 +1288,9 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
     for (const auto& s : specs) ids.push_back(I.admit(s));
     while (I.level(opt)) {}
     std::vector<EvolutionResult> out;
-    if (opt.readback) I.read_results(ids, opt, out);
-    else I.read_counts(ids, out);
+    if (!opt.readback) I.read_counts(ids, out);
+    else if (ids.size() == 1) out.push_back(I.finalize_single(opt));
+    else I.read_results(ids, opt, out);
     I.finish_times();
     return out;
 }

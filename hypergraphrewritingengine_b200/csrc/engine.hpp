@@ -41,7 +41,19 @@ struct EvolutionSpec {
     uint64_t max_states = 0;     // 0 = unlimited; WL classes (quotient) or raw states (full)
 };
 
+// A result's arrays in one host block (page-locked when the block came from the device in a
+// single copy), indexed like the C-ABI's hgx_array codes; `owner` frees the block.
+struct ResultArrays {
+    static constexpr int kArrays = 13;
+    std::shared_ptr<void> owner;
+    const void* ptr[kArrays] = {};
+    uint64_t count[kArrays] = {};   // elements (u64 for the hashes, u32 otherwise)
+};
+
 struct EvolutionResult {
+    // When set, the arrays live in `flat` (and the vectors below are empty).
+    std::shared_ptr<ResultArrays> flat;
+    uint64_t n_roots = 0;
     // States: in full multiway every raw state; in quotient mode one per WL class.
     std::vector<uint64_t> state_hash;
     std::vector<uint32_t> state_depth;

@@ -1202,6 +1202,71 @@ __global__ void k_bemit(DevPtrs P, LevelArgs A) {
 }
 
 // ------------------------------------------------------------------------------------------
+// Result finalisation for a single-evolution run: local ids (roots hold the first `roots`
+// arrival ids, so event e is local e - roots), the event tuples, the causal triples and the
+// state records in state order, written into one staging buffer that is copied to the host once.
+// ------------------------------------------------------------------------------------------
+__global__ void k_fin_events(DevPtrs P, uint32_t roots, uint32_t n, uint32_t rule_begin,
+                             uint32_t* tup, uint32_t* cons_off, uint32_t* prod, uint32_t c0) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t e = roots + i;
+        const uint32_t in = P.ev_in[e];
+        const uint32_t r = P.ev_rule[e];
+        tup[4 * i] = in;
+        tup[4 * i + 1] = P.ev_out[e];
+        tup[4 * i + 2] = r - rule_begin;
+        tup[4 * i + 3] = P.st_depth[in] + 1;
+        cons_off[i] = P.ev_coff[e] - c0;
+        prod[2 * i] = P.ev_prod[e];
+        prod[2 * i + 1] = P.rules[r].n_rhs;
+    }
+}
+
+// Causal triples per event: pass 0 counts (into cnt[i]), pass 1 writes at the scanned offsets.
+__global__ void k_fin_causal(DevPtrs P, uint32_t roots, uint32_t n, uint32_t* cnt,
+                             const uint32_t* off, uint32_t* out, int pass) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t e = roots + i;
+        const uint32_t co = P.ev_coff[e], k = P.rules[P.ev_rule[e]].n_lhs;
+        uint32_t w = pass ? off[i] : 0u;
+        for (uint32_t j = 0; j < k; ++j) {
+            const uint32_t p = P.ev_cprod[co + j];
+            if (p == kNone) continue;
+            if (pass) {
+                out[3 * w] = p - roots;
+                out[3 * w + 1] = i;
+                out[3 * w + 2] = P.ev_cons[co + j];
+            }
+            ++w;
+        }
+        if (!pass) cnt[i] = w;
+    }
+}
+
+__global__ void k_fin_shift(const uint32_t* in, uint64_t n, uint32_t sub, uint32_t* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
+         i += uint64_t(gridDim.x) * blockDim.x)
+        out[i] = in[i] - sub;
+}
+
+// Warp per state: its record's edge ids, arities and vertices at the scanned CSR offsets.
+__global__ void k_fin_states(DevPtrs P, uint32_t n, const uint32_t* eoff, const uint32_t* voff,
+                             uint32_t* ids, uint32_t* ar, uint32_t* verts) {
+    const uint32_t lane = lane_id();
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < n;
+         s += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t ne = P.st_ne[s], nocc = P.st_nocc[s], aw = (ne + 3) >> 2;
+        const uint32_t* rec = P.arena + P.st_off[s];
+        const uint32_t e0 = eoff[s], v0 = voff[s];
+        for (uint32_t i = lane; i < ne; i += 32) {
+            ids[e0 + i] = rec[i];
+            ar[e0 + i] = (rec[ne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
+        }
+        for (uint32_t j = lane; j < nocc; j += 32) verts[v0 + j] = rec[ne + aw + j];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // Exclusive scan of uint32 (in place allowed), writes the total at out[n]. Three phases:
 // per-block sums, one block scans the sums, per-block downsweep.
 // ------------------------------------------------------------------------------------------

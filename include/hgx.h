@@ -162,6 +162,11 @@ HGX_API uint64_t hgx_result_count(const hgx_result* result, hgx_count what);
 HGX_API hgx_status hgx_result_copy(const hgx_result* result, hgx_array what, void* dst, size_t dst_bytes);
 HGX_API void hgx_result_free(hgx_result* result);
 
+/* Zero-copy access: *ptr points at the array inside the result (page-locked host memory for a
+   single-evolution result), *count is its element count; valid until hgx_result_free. */
+HGX_API hgx_status hgx_result_view(const hgx_result* result, hgx_array what, const void** ptr,
+                                   uint64_t* count);
+
 /* Device time per stage of the last evolve call, in milliseconds (HGX_OPT_TIMING must be on):
    out[0..7] = count, scan, expand, select, materialize, branchial, roots, total.
    launches: kernels launched by the call. */
