@@ -262,7 +262,15 @@ struct Engine::Impl {
     DVec<uint32_t> bcount, boff, bpairs, scan_sums, sync_buf, root_ids;
     DVec<unsigned long long> stats, totals;
     DVec<uint8_t> fmode, fin;
-    DVec<uint32_t> fin_cnt;
+    DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e;
+    DVec<uint64_t> fin_rng;
+    // Per evolution: the contiguous id ranges it owns, one entry per level (roots first).
+    struct EvoRanges {
+        std::vector<std::pair<uint32_t, uint32_t>> states, events;
+        std::vector<std::pair<uint64_t, uint64_t>> pairs;
+        uint32_t roots = 0;
+    };
+    std::vector<EvoRanges> evo_ranges;
     std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     uint64_t n_roots_admitted = 0;
 
@@ -328,6 +336,13 @@ struct Engine::Impl {
         fmode.release(st);
         fin.release(st);
         fin_cnt.release(st);
+        evo_frange.release(st);
+        lvl_ranges.release(st);
+        fin_ids.release(st);
+        map_s.release(st);
+        map_e.release(st);
+        fin_rng.release(st);
+        causal_scratch.release(st);
         rules.release(st);
         evos.release(st);
         cudaStreamSynchronize(st);
@@ -340,6 +355,7 @@ struct Engine::Impl {
     void reset() {
         h_rules.clear();
         h_evos.clear();
+        evo_ranges.clear();
         evo_done.clear();
         evo_reported.clear();
         finished.clear();
@@ -603,6 +619,9 @@ struct Engine::Impl {
         up(ev_out.p + a0, h_sid);
         up(ev_kept.p + a0, h_kept);
         up(state_of_arrival.p + a0, h_sid);
+        evo_ranges.emplace_back();
+        evo_ranges.back().states.emplace_back(static_cast<uint32_t>(s0), static_cast<uint32_t>(s0 + nr));
+        evo_ranges.back().roots = nr;
         n_states += nr;
         n_events += nr;
         n_roots_admitted += nr;
@@ -808,6 +827,135 @@ struct Engine::Impl {
         return r;
     }
 
+
+    // One evolution of many, finalised on the device from its recorded id ranges.
+    EvolutionResult finalize_evo(uint32_t evo, const RunOptions& opt) {
+        EvolutionResult r;
+        const EvoRanges& er = evo_ranges.at(evo);
+        std::vector<uint32_t> ids;
+        for (auto& q : er.states) for (uint32_t i = q.first; i < q.second; ++i) ids.push_back(i);
+        const uint32_t S = static_cast<uint32_t>(ids.size());
+        for (auto& q : er.events) for (uint32_t i = q.first; i < q.second; ++i) ids.push_back(i);
+        const uint32_t E = static_cast<uint32_t>(ids.size()) - S;
+        std::vector<uint64_t> rng;   // pair ranges: starts, then cumulative counts
+        uint64_t B = 0;
+        for (auto& q : er.pairs) rng.push_back(q.first);
+        for (auto& q : er.pairs) { rng.push_back(B); B += q.second - q.first; }
+        const uint32_t NR = static_cast<uint32_t>(er.pairs.size());
+        fin_ids.ensure(ids.size() + 1, 0, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(fin_ids.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
+        const uint32_t* sids = fin_ids.p;
+        const uint32_t* eids = fin_ids.p + S;
+        map_s.ensure(n_states, 0, st);
+        map_e.ensure(n_events, 0, st);
+        k_map_ids<<<grid_for(S, 256), 256, 0, st>>>(sids, S, map_s.p);
+        check_launch();
+        if (E) {
+            k_map_ids<<<grid_for(E, 256), 256, 0, st>>>(eids, E, map_e.p);
+            check_launch();
+        }
+        // counts: ne / nocc per state, consumed / causal per event, then their scans
+        fin_cnt.ensure(4ull * (S + 1) + 4ull * (E + 1), 0, st);
+        uint32_t* sne = fin_cnt.p;               // [S+1] -> eoff
+        uint32_t* sno = sne + S + 1;             // [S+1] -> voff
+        uint32_t* ecc = sno + S + 1;             // [E+1] -> coff
+        uint32_t* ekc = ecc + E + 1;             // [E+1] -> koff
+        const bool se = opt.keep_state_edges;
+        uint64_t hbytes = 8ull * S + 4ull * S;
+        fin.ensure(std::max<uint64_t>(hbytes, 16), 0, st);
+        k_gather_states<<<grid_for(S, 256), 256, 0, st>>>(ptrs(), sids, S, reinterpret_cast<uint64_t*>(fin.p),
+                                                          reinterpret_cast<uint32_t*>(fin.p + 8ull * S), sne, sno);
+        check_launch();
+        scan(sne, sne, S);
+        scan(sno, sno, S);
+        if (E) {
+            k_gather_events<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), eids, E, h_evos[evo].rule_begin,
+                                                              map_s.p, map_e.p, ecc, ekc, nullptr, nullptr,
+                                                              nullptr, nullptr, nullptr, nullptr, 0);
+            check_launch();
+        }
+        scan(ecc, ecc, E);
+        scan(ekc, ekc, E);
+        uint32_t T = 0, V = 0, C = 0, K = 0, stopped = 0;
+        unsigned long long classes = 0;
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&T, sne + S, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&V, sno + S, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&C, ecc + E, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&K, ekc + E, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&stopped, evo_stopped.p + evo, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&classes, evo_classes.p + evo, 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (!opt.causal) K = 0;
+        uint64_t count[ResultArrays::kArrays] = {
+            S, S, 4ull * E, 3ull * K, 2 * B, uint64_t(E) + 1, C, 2ull * E,
+            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0};
+        uint64_t off[ResultArrays::kArrays];
+        uint64_t total = 0;
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            off[i] = total;
+            total += (count[i] * (i == 0 ? 8 : 4) + 15) / 16 * 16;
+        }
+        // staging: hashes/depths were gathered at the front of `fin`; move them into place
+        fin.ensure(total + hbytes, hbytes, st);
+        uint8_t* d = fin.p + hbytes;
+        auto dp = [&](int i) { return reinterpret_cast<uint32_t*>(d + off[i]); };
+        HGX_CUDA_CHECK(cudaMemcpyAsync(d + off[0], fin.p, 8ull * S, cudaMemcpyDeviceToDevice, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(d + off[1], fin.p + 8ull * S, 4ull * S, cudaMemcpyDeviceToDevice, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(dp(5), ecc, 4ull * (E + 1), cudaMemcpyDeviceToDevice, st));
+        if (E) {
+            k_gather_events<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), eids, E, h_evos[evo].rule_begin,
+                                                              map_s.p, map_e.p, nullptr, nullptr, ecc, ekc,
+                                                              dp(2), dp(6), dp(7),
+                                                              opt.causal ? dp(3) : fin_scratch_causal(K), 1);
+            check_launch();
+        }
+        if (B) {
+            fin_rng.ensure(rng.size(), 0, st);
+            HGX_CUDA_CHECK(cudaMemcpyAsync(fin_rng.p, rng.data(), rng.size() * 8, cudaMemcpyHostToDevice, st));
+            k_gather_pairs<<<grid_for(B, 256), 256, 0, st>>>(bpairs.p, fin_rng.p, fin_rng.p + NR, NR, B,
+                                                             map_e.p, dp(4));
+            check_launch();
+        }
+        if (se) {
+            HGX_CUDA_CHECK(cudaMemcpyAsync(dp(8), sne, 4ull * (S + 1), cudaMemcpyDeviceToDevice, st));
+            HGX_CUDA_CHECK(cudaMemcpyAsync(dp(11), sno, 4ull * (S + 1), cudaMemcpyDeviceToDevice, st));
+            k_gather_records<<<grid_for(uint64_t(S) * 32, 256), 256, 0, st>>>(ptrs(), sids, S, sne, sno,
+                                                                              dp(9), dp(10), dp(12));
+            check_launch();
+        } else {
+            HGX_CUDA_CHECK(cudaMemsetAsync(dp(8), 0, 4, st));
+            HGX_CUDA_CHECK(cudaMemsetAsync(dp(11), 0, 4, st));
+        }
+        size_t cap = 0;
+        uint8_t* h = static_cast<uint8_t*>(pinned->get(total, cap));
+        auto pool = pinned;
+        auto flat = std::make_shared<ResultArrays>();
+        flat->owner = std::shared_ptr<void>(h, [pool, cap](void* p) { pool->put(p, cap); });
+        HGX_CUDA_CHECK(cudaMemcpyAsync(h, d, total, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            flat->ptr[i] = h + off[i];
+            flat->count[i] = count[i];
+        }
+        r.flat = flat;
+        r.n_roots = er.roots;
+        r.num_classes = classes;
+        r.truncated = stopped != 0;
+        if (r.truncated)
+            r.warnings.push_back(
+                "capacity limit reached: the state cap stopped the evolution; the states, events "
+                "and relations returned are valid and incomplete");
+        return r;
+    }
+
+    // Causal triples are written even when the caller did not ask for them; they then land in
+    // this scratch instead of the result.
+    DVec<uint32_t> causal_scratch;
+    uint32_t* fin_scratch_causal(uint32_t K) {
+        causal_scratch.ensure(3ull * K + 3, 0, st);
+        return causal_scratch.p;
+    }
+
     // Counts only (results stay on the device).
     void read_counts(const std::vector<uint32_t>& which, std::vector<EvolutionResult>& out) {
         const size_t nevo = h_evos.size();
@@ -912,7 +1060,8 @@ struct Engine::Impl {
         scan(item_prod.p, item_prod.p, NI);
         scan(item_fresh.p, item_fresh.p, NI);
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_first_ev.p, 0xFF, h_evos.size() * 4, st));
-        k_evo_first<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p);
+        evo_frange.ensure(2 * h_evos.size(), 0, st);
+        k_evo_first<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, evo_frange.p);
         check_launch();
         toc(times.scan);
 
@@ -1064,8 +1213,23 @@ struct Engine::Impl {
             scan(bcount.p, boff.p, F_eff);
             toc(times.branchial);
         } else {
-            HGX_CUDA_CHECK(cudaMemsetAsync(boff.p + F_eff, 0, 4, st));
+            // no pairs this level: every offset is 0 (the per-evolution pair ranges read them)
+            HGX_CUDA_CHECK(cudaMemsetAsync(boff.p, 0, (uint64_t(F_eff) + 1) * 4, st));
         }
+
+        // per-evolution ranges of this level (events kept, new states, branchial pairs)
+        A.state_base = static_cast<uint32_t>(n_states);
+        A.bbase = static_cast<uint32_t>(n_bpairs);
+        lvl_ranges.ensure(6 * nevo, 0, st);
+        if (ne2 || F_eff) {
+            A.n_frontier = F;   // boundaries over the whole frontier; pair ranges clamp to F_eff
+            k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, evo_frange.p,
+                                                          F_eff, lvl_ranges.p);
+            check_launch();
+            A.n_frontier = F_eff;
+        }
+        std::vector<uint32_t> h_rng(6 * nevo);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(h_rng.data(), lvl_ranges.p, 6 * nevo * 4, cudaMemcpyDeviceToHost, st));
 
         // ---- sync 2: new states, next frontier, branchial pairs, errors
         uint32_t s2[4];
@@ -1076,6 +1240,17 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         if (s2[3]) throw std::runtime_error("hgx: device error flags 0x" + std::to_string(s2[3]));
         const uint32_t n_new = s2[0], n_front = s2[1], n_b = s2[2];
+        for (size_t e = 0; e < nevo; ++e) {
+            if (evo_done[e] || h_first[e] == kNone) continue;
+            const uint32_t* q = &h_rng[6 * e];
+            // ranges must lie inside what this level produced
+            if (q[0] > q[1] || q[1] > n_events + ne2 || q[2] > q[3] || q[3] > n_states + n_new ||
+                q[4] > q[5] || q[5] > n_bpairs + n_b)
+                throw std::runtime_error("hgx: inconsistent per-evolution ranges at a level");
+            if (q[1] > q[0]) evo_ranges[e].events.emplace_back(q[0], q[1]);
+            if (q[3] > q[2]) evo_ranges[e].states.emplace_back(q[2], q[3]);
+            if (opt.branchial && q[5] > q[4]) evo_ranges[e].pairs.emplace_back(q[4], q[5]);
+        }
 
         grow_states(n_states + n_new);
         new_state_event.ensure(n_new, 0, st);
@@ -1304,9 +1479,10 @@ std::vector<uint32_t> Engine::take_finished() {
     return f;
 }
 EvolutionResult Engine::collect(uint32_t evo, const RunOptions& opt) {
+    if (evo >= impl_->h_evos.size()) throw std::invalid_argument("collect: unknown evolution id");
+    if (opt.readback) return impl_->finalize_evo(evo, opt);
     std::vector<EvolutionResult> out;
-    if (opt.readback) impl_->read_results({evo}, opt, out);
-    else impl_->read_counts({evo}, out);
+    impl_->read_counts({evo}, out);
     return std::move(out[0]);
 }
 uint32_t Engine::active() const {

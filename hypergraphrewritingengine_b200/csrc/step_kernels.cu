@@ -855,16 +855,129 @@ __global__ void k_evo_totals(DevPtrs P, uint32_t n_events, const uint32_t* bpair
 
 // First / one-past-last event of every evolution in this level (the frontier is grouped by
 // evolution, so each evolution's items are contiguous); resets the evolution's cap cut.
-__global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last) {
+__global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t* evo_frange) {
     for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
          f += gridDim.x * blockDim.x) {
         const uint32_t evo = P.st_evo[A.frontier[f]];
         if (f == 0 || P.st_evo[A.frontier[f - 1]] != evo) {
             P.evo_first_ev[evo] = A.ev_base + A.item_ev[f * A.rules_stride];
             P.evo_cut[evo] = kNone;
+            evo_frange[2 * evo] = f;
         }
-        if (f + 1 == A.n_frontier || P.st_evo[A.frontier[f + 1]] != evo)
+        if (f + 1 == A.n_frontier || P.st_evo[A.frontier[f + 1]] != evo) {
             evo_last[evo] = A.ev_base + A.item_ev[(f + 1) * A.rules_stride];
+            evo_frange[2 * evo + 1] = f + 1;
+        }
+    }
+}
+
+// Per evolution of the level: its kept events, its new states and its branchial pairs are each
+// one contiguous range (the frontier is grouped by evolution and everything is numbered in
+// frontier order). out[evo * 6 + {0..5}] = event first/end, state first/end, pair first/end.
+__global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last,
+                             const uint32_t* evo_frange, uint32_t n_built_front, uint32_t* out) {
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
+         f += gridDim.x * blockDim.x) {
+        const uint32_t evo = P.st_evo[A.frontier[f]];
+        if (f != 0 && P.st_evo[A.frontier[f - 1]] == evo) continue;
+        const uint32_t e0 = P.evo_first_ev[evo];
+        uint32_t e1 = min(evo_last[evo], A.ev_base + A.n_events);
+        e1 = max(e0, min(e1, P.evo_cut[evo]));
+        const uint32_t f0 = min(evo_frange[2 * evo], n_built_front);
+        const uint32_t f1 = min(evo_frange[2 * evo + 1], n_built_front);
+        uint32_t* o = out + 6ull * evo;
+        o[0] = e0;
+        o[1] = e1;
+        o[2] = A.state_base + A.flag_rep[e0 - A.ev_base];
+        o[3] = A.state_base + A.flag_rep[e1 - A.ev_base];
+        o[4] = A.bbase + A.boff[f0];
+        o[5] = A.bbase + A.boff[f1];
+    }
+}
+
+// Result finalisation of one evolution of many: ids -> local ids through maps filled here.
+__global__ void k_map_ids(const uint32_t* ids, uint32_t n, uint32_t* map) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        map[ids[i]] = i;
+}
+
+__global__ void k_gather_states(DevPtrs P, const uint32_t* ids, uint32_t n, uint64_t* hash,
+                                uint32_t* depth, uint32_t* ne, uint32_t* nocc) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = ids[i];
+        hash[i] = P.st_hash[s];
+        depth[i] = P.st_depth[s];
+        ne[i] = P.st_ne[s];
+        nocc[i] = P.st_nocc[s];
+    }
+}
+
+__global__ void k_gather_records(DevPtrs P, const uint32_t* sids, uint32_t n, const uint32_t* eoff,
+                                 const uint32_t* voff, uint32_t* oids, uint32_t* oar, uint32_t* overts) {
+    const uint32_t lane = lane_id();
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+         i += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t s = sids[i];
+        const uint32_t ne = P.st_ne[s], nocc = P.st_nocc[s], aw = (ne + 3) >> 2;
+        const uint32_t* rec = P.arena + P.st_off[s];
+        for (uint32_t k = lane; k < ne; k += 32) {
+            oids[eoff[i] + k] = rec[k];
+            oar[eoff[i] + k] = (rec[ne + (k >> 2)] >> ((k & 3u) * 8u)) & 0xFFu;
+        }
+        for (uint32_t j = lane; j < nocc; j += 32) overts[voff[i] + j] = rec[ne + aw + j];
+    }
+}
+
+// Events of one evolution (ids: global event ids in canonical order). pass 0: consumed and
+// causal counts; pass 1: tuples, consumed lists, produced ranges and causal triples.
+__global__ void k_gather_events(DevPtrs P, const uint32_t* ids, uint32_t n, uint32_t rule_begin,
+                                const uint32_t* smap, const uint32_t* emap, uint32_t* ccount,
+                                uint32_t* kcount, const uint32_t* coff, const uint32_t* koff,
+                                uint32_t* tup, uint32_t* cons, uint32_t* prod, uint32_t* causal,
+                                int pass) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t e = ids[i];
+        const uint32_t r = P.ev_rule[e];
+        const DevRule& R = P.rules[r];
+        const uint32_t co = P.ev_coff[e];
+        if (!pass) {
+            uint32_t k = 0;
+            for (uint32_t j = 0; j < R.n_lhs; ++j) k += P.ev_cprod[co + j] != kNone ? 1u : 0u;
+            ccount[i] = R.n_lhs;
+            kcount[i] = k;
+            continue;
+        }
+        const uint32_t in = P.ev_in[e];
+        tup[4 * i] = smap[in];
+        tup[4 * i + 1] = smap[P.ev_out[e]];
+        tup[4 * i + 2] = r - rule_begin;
+        tup[4 * i + 3] = P.st_depth[in] + 1;
+        prod[2 * i] = P.ev_prod[e];
+        prod[2 * i + 1] = R.n_rhs;
+        uint32_t w = koff[i];
+        for (uint32_t j = 0; j < R.n_lhs; ++j) {
+            const uint32_t c = P.ev_cons[co + j];
+            cons[coff[i] + j] = c;
+            const uint32_t p = P.ev_cprod[co + j];
+            if (p == kNone) continue;
+            causal[3 * w] = emap[p];
+            causal[3 * w + 1] = i;
+            causal[3 * w + 2] = c;
+            ++w;
+        }
+    }
+}
+
+// Branchial pairs of one evolution: the concatenation of `nr` ranges of the pair array.
+__global__ void k_gather_pairs(const uint32_t* pairs, const uint64_t* rstart, const uint64_t* rcum,
+                               uint32_t nr, uint64_t n, const uint32_t* emap, uint32_t* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t k = 0;
+        while (k + 1 < nr && rcum[k + 1] <= i) ++k;
+        const uint64_t g = rstart[k] + (i - rcum[k]);
+        out[2 * i] = emap[pairs[2 * g]];
+        out[2 * i + 1] = emap[pairs[2 * g + 1]];
     }
 }
 
