@@ -174,9 +174,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the batched comparison")
     ap.add_argument("--levels", type=int, default=8)
+    ap.add_argument("--profile-run", action="store_true",
+                    help="run the workload once, device-resident, and exit (for profilers)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile_run:
+        from hypergraphrewritingengine_b200 import Engine
+        from hypergraphrewritingengine_b200 import workloads as W
+        ev = W.config2(args.levels)
+        c = Engine(0).counts(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+        print(json.dumps(c))
+        return
 
     import numpy as np
     import torch
@@ -308,6 +317,7 @@ def main():
         line["cpu_baseline"] = cpu_baseline_reference()
         if not args.no_extras:
             line["batched"] = batched_vs_plain(eng)
+            line["served"] = served_vs_plain(eng)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -355,6 +365,37 @@ def batched_vs_plain(eng, n=1024):
             "batched_ms": t_batch * 1e3, "plain_ms": t_plain * 1e3,
             "speedup_vs_plain": t_plain / t_batch,
             "identical_outputs": batch_counts == plain_counts}
+
+
+def served_vs_plain(eng, n=400, rates=(100.0, 1000.0, float("inf"))):
+    """Poisson stream of random evolve requests (initial edges lognormal, median 16, max 256;
+    2-8 steps; WL quotient, cap 4096 states), served with continuous batching vs. one request per
+    call in arrival order, at arrival rates up to saturation (inf = all requests at t=0)."""
+    from hypergraphrewritingengine_b200 import workloads as W
+    from hypergraphrewritingengine_b200.serve import Server, serve_plain, summarize
+    out = {"workload": f"c5: {n} requests per rate, seed 0xC0FFEE, lognormal initial edges "
+                       "(median 16, max 256), 2-8 steps, WL quotient, cap 4096 states; "
+                       "admission by estimated device bytes <= 140 GB",
+           "rates": []}
+    warm = W.config5_stream(32, rate_per_s=1e9, seed=1, max_states=4096)
+    Server(eng).run(warm, realtime=False, admit_per_step=32)
+    serve_plain(eng, warm, realtime=False)
+    for rate in rates:
+        stream = W.config5_stream(n, rate_per_s=rate if rate != float("inf") else 1e12,
+                                  seed=0xC0FFEE, max_states=4096)
+        if rate == float("inf"):
+            stream = [(0.0, ev) for _, ev in stream]
+        served = Server(eng).run(stream, realtime=True)
+        plain = serve_plain(eng, stream, realtime=True)
+        same = all(a.result.num_events == b.result.num_events and
+                   a.result.num_states == b.result.num_states and
+                   a.result.num_classes == b.result.num_classes for a, b in zip(served, plain))
+        ss, sp = summarize(served), summarize(plain)
+        out["rates"].append({"arrivals_per_s": rate if rate != float("inf") else "all at t=0",
+                             "served": ss, "plain": sp,
+                             "throughput_speedup": ss["events_per_s"] / sp["events_per_s"],
+                             "identical_outputs": same})
+    return out
 
 
 if __name__ == "__main__":
