@@ -112,6 +112,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(mhz)}
 
 
+def max_over_ranks(dist, value: float, device: str = "cuda") -> float:
+    """Max of a per-rank time over all ranks (a collective every rank must call)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def profile_traffic():
     """dram bytes per k_expand launch from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", "k_expand.c2-8step.txt")
@@ -246,11 +256,7 @@ def main():
             launches += nl
         barrier()
     eng.set_option(api.OPT_TIMING, 0)
-    t_ms = sum(step_ms) / len(step_ms)
-    if dist is not None:
-        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
+    t_ms = max_over_ranks(dist, sum(step_ms) / len(step_ms))
     events = counts["events"]
     states = counts["states"]
     value = world * events / (t_ms / 1e3)
@@ -271,13 +277,7 @@ def main():
             e2e_s.append(dt)
         d2h = res.bytes()
         assert res.num_events == events and res.num_states == states
-    e2e_t = max(e2e_s) if dist is None else e2e_s[-1]
-    if dist is not None:
-        t = torch.tensor([statistics.mean(e2e_s)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
-    else:
-        e2e_t = statistics.mean(e2e_s)
+    e2e_t = max_over_ranks(dist, statistics.mean(e2e_s))
 
     if rank != 0:
         if dist is not None:

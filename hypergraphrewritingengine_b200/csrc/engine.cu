@@ -956,17 +956,21 @@ struct Engine::Impl {
         return causal_scratch.p;
     }
 
-    // Counts only (results stay on the device).
+    // Counts only (results stay on the device): events and branchial pairs from the recorded
+    // per-evolution ranges, states and classes from the device counters, causal triples by one
+    // pass over the events.
     void read_counts(const std::vector<uint32_t>& which, std::vector<EvolutionResult>& out) {
         const size_t nevo = h_evos.size();
-        totals.ensure(3 * nevo, 0, st);
-        HGX_CUDA_CHECK(cudaMemsetAsync(totals.p, 0, 3 * nevo * sizeof(unsigned long long), st));
-        k_evo_totals<<<grid_for(std::max<uint64_t>(n_events, n_bpairs), 256), 256, 0, st>>>(
-            ptrs(), static_cast<uint32_t>(n_events), bpairs.p, n_bpairs, totals.p);
-        check_launch();
-        std::vector<unsigned long long> tot(3 * nevo), cls(nevo), sts(nevo);
+        totals.ensure(nevo, 0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(totals.p, 0, nevo * sizeof(unsigned long long), st));
+        if (n_events) {
+            k_evo_causal<<<grid_for(n_events, 256), 256, 0, st>>>(ptrs(), static_cast<uint32_t>(n_events),
+                                                                  totals.p);
+            check_launch();
+        }
+        std::vector<unsigned long long> causal(nevo), cls(nevo), sts(nevo);
         std::vector<uint32_t> stop(nevo);
-        HGX_CUDA_CHECK(cudaMemcpyAsync(tot.data(), totals.p, tot.size() * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(causal.data(), totals.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(cls.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(sts.data(), evo_states.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(stop.data(), evo_stopped.p, nevo * 4, cudaMemcpyDeviceToHost, st));
@@ -978,9 +982,9 @@ struct Engine::Impl {
             r.counts_only = true;
             r.num_classes = cls[e];
             r.n_states = sts[e];
-            r.n_events = tot[3 * e];
-            r.n_causal = tot[3 * e + 1];
-            r.n_branchial = tot[3 * e + 2];
+            for (auto& q : evo_ranges[e].events) r.n_events += q.second - q.first;
+            for (auto& q : evo_ranges[e].pairs) r.n_branchial += q.second - q.first;
+            r.n_causal = causal[e];
             r.truncated = stop[e] != 0;
         }
     }

@@ -826,32 +826,34 @@ __global__ void k_cprod(DevPtrs P, uint32_t ev_base, uint32_t n) {
     }
 }
 
-// Per-evolution totals without reading the result back: kept events, causal triples,
-// branchial pairs. out[evo * 3 + {0,1,2}].
-__global__ void k_evo_totals(DevPtrs P, uint32_t n_events, const uint32_t* bpairs, uint64_t n_bpairs,
-                             unsigned long long* out) {
+// Causal triples per evolution without reading the result back: kept events whose consumed
+// edges have a producer. out[evo] += count (warp-aggregated per evolution).
+__global__ void k_evo_causal(DevPtrs P, uint32_t n_events, unsigned long long* out) {
     const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < n_events; t0 += stride) {
         const uint64_t e = t0 + threadIdx.x;
-        bool live = false;
         uint32_t evo = 0, nc = 0;
         if (e < n_events && P.ev_in[e] != kNone && P.ev_kept[e]) {
-            live = true;
             evo = P.st_evo[P.ev_in[e]];
             const DevRule& R = P.rules[P.ev_rule[e]];
             const uint32_t co = P.ev_coff[e];
             for (uint32_t k = 0; k < R.n_lhs; ++k) nc += P.ev_cprod[co + k] != kNone ? 1u : 0u;
         }
-        warp_count(out, live ? evo * 3 : 0, live);
-        if (live && nc) atomicAdd(&out[evo * 3 + 1], static_cast<unsigned long long>(nc));
-    }
-    for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < n_bpairs; t0 += stride) {
-        const uint64_t i = t0 + threadIdx.x;
-        const bool live = i < n_bpairs;
-        const uint32_t evo = live ? P.st_evo[P.ev_in[bpairs[2 * i]]] : 0;
-        warp_count(out, evo * 3 + 2, live);
+        const bool live = nc != 0;
+        const uint32_t act = __ballot_sync(0xFFFFFFFFu, live);
+        if (live) {
+            const uint32_t peers = __match_any_sync(act, evo);
+            uint32_t sum = nc;
+            // sum nc over the peers (same evolution) -- lanes of one warp, tiny loop
+            for (uint32_t m = peers & ~(1u << lane_id()); m; m &= m - 1)
+                sum += __shfl_sync(peers, nc, __ffs(m) - 1);
+            if (lane_id() == static_cast<uint32_t>(__ffs(peers) - 1))
+                atomicAdd(&out[evo], static_cast<unsigned long long>(sum));
+        }
     }
 }
+
+
 
 // First / one-past-last event of every evolution in this level (the frontier is grouped by
 // evolution, so each evolution's items are contiguous); resets the evolution's cap cut.

@@ -1,0 +1,40 @@
+// The header-only C++ drop-ins (include/hgx/compat.hpp) driven with the reference's call
+// sequence; exit 0 when the counts are the reference engine's (config 1 at 5 steps) and the
+// oracle's (config 2 quotient at 5 steps). Needs a GPU.
+#include <cstdio>
+
+#include "hgx/compat.hpp"
+
+int main() {
+    using namespace hgx::compat::engine;
+    Hypergraph hg;
+    ParallelEvolutionEngine engine(&hg, 8);
+    engine.add_rule(make_rule(0).lhs({0, 1}).lhs({1, 2}).rhs({0, 1}).rhs({1, 2}).rhs({2, 0}).build());
+    engine.set_transitive_reduction(false);
+    engine.evolve({{1, 2}, {2, 3}, {3, 1}}, 5);
+    const auto cg = hg.causal_graph();
+    std::printf("c1: states %u events %u classes %zu causal %zu branchial %zu\n", hg.num_states(),
+                hg.num_events(), hg.num_canonical_states(), cg.get_causal_edges().size(),
+                cg.get_branchial_edges().size());
+    bool ok = hg.num_states() == 22204 && hg.num_events() == 22203 && hg.num_canonical_states() == 20 &&
+              cg.get_causal_edges().size() == 42816 && cg.get_branchial_edges().size() == 78045;
+
+    hgx::compat::gpu::EvolveInput in;
+    in.rules.push_back({{{0, 1}, {0, 2}}, {{0, 2}, {0, 3}, {1, 3}, {2, 3}}, 3, 4});
+    in.initial_state = {{1, 1}, {1, 1}};
+    in.num_steps = 5;
+    in.explore_from_canonical_states_only = true;
+    const auto r = hgx::compat::gpu::evolve(in);
+    std::printf("c2: states %zu events %zu classes %llu\n", r.states.size(), r.events.size(),
+                (unsigned long long)r.num_classes);
+    ok = ok && r.states.size() == 1952 && r.events.size() == 5056 && r.num_classes == 1952;
+    bool threw = false;
+    try {
+        make_rule(0).lhs({0, 40});
+    } catch (const std::length_error&) {
+        threw = true;
+    }
+    ok = ok && threw;
+    std::printf(ok ? "compat ok\n" : "compat MISMATCH\n");
+    return ok ? 0 : 1;
+}

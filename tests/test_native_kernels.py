@@ -22,3 +22,27 @@ def test_lane_wl_matches_oracle(tmp_path):
     out = subprocess.run([str(exe), "20000"], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "0 / 20000 mismatches" in out.stdout
+
+
+def _build_compat(tmp_path):
+    from hypergraphrewritingengine_b200 import build
+    build.build()
+    exe = tmp_path / "compat_test"
+    subprocess.check_call(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "native", "compat_test.cpp"),
+                           "-L", os.path.dirname(build.LIB), "-lhgx",
+                           "-Wl,-rpath," + os.path.dirname(build.LIB), "-o", str(exe)])
+    return exe
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_compat_header_compiles_and_links(tmp_path):
+    assert _build_compat(tmp_path).exists()
+
+
+@pytest.mark.gpu
+def test_compat_drop_ins_on_gpu(tmp_path):
+    exe = _build_compat(tmp_path)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "compat ok" in out.stdout
