@@ -34,6 +34,14 @@ constexpr int kLaneVMax = 32;
 constexpr int kLaneEMax = 64;
 constexpr int kLaneNMax = 64;    // neighbour entries a lane sorts for one vertex
 
+// Match forwarding: at most this many delta matches per state (else the state is re-joined), and
+// rules of at most 4 LHS edges (a match's canonical key packs 4 positions of 16 bits).
+constexpr uint32_t kFwdCap = 256;
+constexpr uint32_t kFwdMaxLhs = 4;
+
+// States with more vertex occurrences than this number their vertices through a hash table.
+constexpr uint32_t kHashOccMin = 96;
+
 HGX_HD uint64_t fnv(uint64_t h, uint64_t x) { return (h ^ x) * kFnvPrime; }
 
 HGX_HD uint64_t smix(uint64_t z) {

@@ -123,7 +123,7 @@ enum class LayoutKind { Count, Lane, Warp };
 
 // Shared-memory carve-up per warp. Count: the parent and the join. Lane: plus the parent's
 // per-vertex occurrence lists and a 32-match batch. Warp: plus the warp-per-child WL arrays.
-Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kind) {
+Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kind, bool fwd = false) {
     const bool wl = kind == LayoutKind::Warp;
     const bool lane = kind == LayoutKind::Lane;
     Layout L;
@@ -172,6 +172,27 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
     L.o_pear = take(NE, 1);
     if (wl) L.o_car = take(L.CNE, 1);
     L.o_rule = take(sizeof(DevRule), 4);
+    if (fwd) {
+        L.o_fkc = take(4 * kMaxPatternEdges, 4);
+        L.o_dkey = take(8 * kFwdCap, 8);
+        L.o_dkey2 = take(8 * kFwdCap, 8);
+        L.o_fkey = take(8 * 32, 8);
+        L.o_dpos = take(2 * kFwdMaxLhs * kFwdCap, 2);
+        L.o_dpos2 = take(2 * kFwdMaxLhs * kFwdCap, 2);
+        L.o_fpos = take(2 * kFwdMaxLhs * 32, 2);
+        L.o_sched2 = take(kMaxPatternEdges, 1);
+    }
+    if (NOCC > kHashOccMin) {
+        L.VT = 1;
+        while (L.VT < 2 * NOCC) L.VT <<= 1;
+        L.o_vtab = take(4 * L.VT, 4);
+        L.o_vtid = take(2 * L.VT, 2);
+    }
+    if (wl) {
+        uint32_t n2 = 64;
+        while (n2 < L.V) n2 <<= 1;
+        L.o_srt = take(8 * n2, 8);
+    }
     if (lane) {
         L.SB = rm.lhs + rm.rhs_total;
         L.o_poff = take(2 * (kLaneVMax + 1), 2);
@@ -243,7 +264,7 @@ struct Engine::Impl {
     DVec<DevRule> rules;
     DVec<DevEvo> evos;
     DVec<uint64_t> st_off, st_hash;
-    DVec<uint32_t> st_ne, st_nocc, st_evo, st_depth, st_event;
+    DVec<uint32_t> st_ne, st_nocc, st_evo, st_depth, st_event, st_ev0, st_evn;
     DVec<uint32_t> arena;
     DVec<unsigned long long> arena_top;
     DVec<uint32_t> edge_creator;
@@ -315,7 +336,8 @@ struct Engine::Impl {
         cudaSetDevice(device);
         cudaStreamSynchronize(st);
         for (auto* v : std::initializer_list<DVec<uint32_t>*>{
-                 &st_ne, &st_nocc, &st_evo, &st_depth, &st_event, &arena, &edge_creator, &ev_in,
+                 &st_ne, &st_nocc, &st_evo, &st_depth, &st_event, &st_ev0, &st_evn, &arena,
+                 &edge_creator, &ev_in,
                  &ev_rule, &ev_coff, &ev_prod, &ev_fresh, &ev_out, &ev_cons, &ev_cprod,
                  &state_of_arrival, &tab_vals, &evo_cut, &evo_first_ev, &evo_last_ev,
                  &evo_stopped, &evo_front, &err, &frontier, &next_frontier, &counts, &item_ev,
@@ -384,6 +406,8 @@ struct Engine::Impl {
         P.st_evo = st_evo.p;
         P.st_depth = st_depth.p;
         P.st_event = st_event.p;
+        P.st_ev0 = st_ev0.p;
+        P.st_evn = st_evn.p;
         P.st_hash = st_hash.p;
         P.arena = arena.p;
         P.arena_top = arena_top.p;
@@ -530,7 +554,10 @@ struct Engine::Impl {
                     throw std::invalid_argument("evolve: initial edge arity must be 1..16");
                 nocc += static_cast<uint32_t>(e.size());
                 rm.arity = std::max<uint32_t>(rm.arity, static_cast<uint32_t>(e.size()));
-                for (uint32_t v : e) max_label = std::max<uint64_t>(max_label, v);
+                for (uint32_t v : e) {
+                    if (v == kNone) throw std::invalid_argument("evolve: vertex label 4294967295 is reserved");
+                    max_label = std::max<uint64_t>(max_label, v);
+                }
             }
             if (ne == 0) throw std::invalid_argument("evolve: an initial state has no edges");
             offs.push_back(arena_words + words.size());
@@ -663,6 +690,8 @@ struct Engine::Impl {
         st_evo.ensure(n, k, st);
         st_depth.ensure(n, k, st);
         st_event.ensure(n, k, st);
+        st_ev0.ensure(n, k, st);
+        st_evn.ensure(n, k, st);
     }
 
     void grow_events(uint64_t n) {
@@ -1044,7 +1073,9 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemsetAsync(level_max.p, 0, 4 * sizeof(uint32_t), st));
 
         // ---- count
-        const Layout Lc = make_layout(ne_bound, nocc_bound, rm, LayoutKind::Count);
+        const bool fwd = opt.forwarding != 0;
+        A.fwd_mode = opt.forwarding;
+        const Layout Lc = make_layout(ne_bound, nocc_bound, rm, LayoutKind::Count, fwd);
         fmode.ensure(F, 0, st);
         A.fmode = fmode.p;
         LaunchShape sc = warp_shape(k_count, Lc, F);
@@ -1063,6 +1094,8 @@ struct Engine::Impl {
         scan(item_cons.p, item_cons.p, NI);
         scan(item_prod.p, item_prod.p, NI);
         scan(item_fresh.p, item_fresh.p, NI);
+        k_fwd_record<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A);
+        check_launch();
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_first_ev.p, 0xFF, h_evos.size() * 4, st));
         evo_frange.ensure(2 * h_evos.size(), 0, st);
         k_evo_first<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, evo_frange.p);
@@ -1125,8 +1158,8 @@ struct Engine::Impl {
         uint32_t F_eff = F;
         if (n_ev) {
             const uint32_t mne = std::max<uint32_t>(fmax_ne, 1), mno = std::max<uint32_t>(fmax_nocc, 1);
-            const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane);
-            const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp);
+            const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane, fwd);
+            const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp, fwd);
             LaunchShape sl = warp_shape(k_expand<true>, Ll, F);
             LaunchShape sw = warp_shape(k_expand<false>, Lw, F);
             // chunking applies to a level holding one evolution whose cap this level can reach

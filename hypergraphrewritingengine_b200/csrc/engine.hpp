@@ -85,6 +85,9 @@ struct RunOptions {
     bool readback = true;            // false: leave results on the device, return counts
     bool causal = true;
     bool branchial = true;
+    // Match forwarding: 0 = re-join every state, 1 = forward wherever it applies, 2 = forward
+    // for states of 48 edges or more (results are identical in every mode).
+    uint32_t forwarding = 0;
 };
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.

@@ -166,6 +166,40 @@ __device__ Parent load_parent(const DevPtrs& P, const Layout& L, char* sm, uint3
         if (i < pa.ne) pevo[i] = static_cast<uint16_t>(run + inc - a);
         run += __shfl_sync(0xFFFFFFFFu, inc, 31);
     }
+    if (pa.nocc > kHashOccMin && L.VT) {
+        // Large state: vertex -> local id through a shared-memory hash table, O(occurrences).
+        // Ids follow slot order; any consistent numbering works (WL is label-invariant and the
+        // join only compares vertices for equality).
+        uint32_t* tab = smp<uint32_t>(sm, L.o_vtab);
+        uint16_t* tid = smp<uint16_t>(sm, L.o_vtid);
+        const uint32_t TS = L.VT;
+        for (uint32_t t = lane; t < TS; t += 32) tab[t] = kNone;
+        __syncwarp();
+        for (uint32_t j = lane; j < pa.nocc; j += 32) {
+            const uint32_t v = glob[j];
+            uint32_t h = (v * 2654435761u) & (TS - 1);
+            for (uint32_t probe = 0; probe < TS; ++probe) {
+                const uint32_t prev = atomicCAS(&tab[h], kNone, v);
+                if (prev == kNone || prev == v) break;
+                h = (h + 1) & (TS - 1);
+            }
+            first[j] = h;
+        }
+        __syncwarp();
+        uint32_t ids = 0;
+        for (uint32_t b = 0; b < TS; b += 32) {
+            const uint32_t t = b + lane;
+            const bool used = tab[t] != kNone;
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, used);
+            if (used) tid[t] = static_cast<uint16_t>(ids + __popc(bal & ((1u << lane) - 1u)));
+            ids += __popc(bal);
+        }
+        __syncwarp();
+        for (uint32_t j = lane; j < pa.nocc; j += 32) vloc[j] = tid[first[j]];
+        __syncwarp();
+        pa.nvp = ids;
+        return pa;
+    }
     run = 0;
     for (uint32_t b = 0; b < pa.nocc; b += 32) {
         const uint32_t j = b + lane;
@@ -238,9 +272,11 @@ __device__ void compute_cands(const Layout& L, char* sm, const DevRule& R, uint3
     __syncwarp();
 }
 
+// sched: the binding order of the LHS positions; seed >= 0 pins the first scheduled position to
+// that state position (a seeded join: every emitted match uses it there).
 template <class F>
 __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Parent& pa,
-                          F&& on_match) {
+                          const uint8_t* sched, int seed, F&& on_match) {
     const uint32_t lane = lane_id();
     const uint32_t n = R.n_lhs;
     const uint32_t nw = (pa.ne + 31) >> 5;
@@ -259,7 +295,13 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
     __syncwarp();
     uint32_t mask = 0;
     uint32_t d = 0;
-    compute_cands(L, sm, R, R.sched[0], pa, mask, cand);
+    compute_cands(L, sm, R, sched[0], pa, mask, cand);
+    if (seed >= 0) {
+        // keep only the seed among the first position's candidates
+        for (uint32_t w = lane; w < nw; w += 32)
+            cand[w] &= (static_cast<uint32_t>(seed) >> 5) == w ? (1u << (seed & 31)) : 0u;
+        __syncwarp();
+    }
     while (true) {
         int pick = -1;
         for (uint32_t w = 0; w < nw; ++w) {
@@ -277,7 +319,7 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
             __syncwarp();
             continue;
         }
-        const uint32_t p = R.sched[d];
+        const uint32_t p = sched[d];
         if (lane == 0) {
             cand[d * L.W + (pick >> 5)] &= ~(1u << (pick & 31));
             taken[pick >> 5] |= 1u << (pick & 31);
@@ -305,7 +347,7 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
         } else {
             mask = nm;
             ++d;
-            compute_cands(L, sm, R, R.sched[d], pa, mask, cand + d * L.W);
+            compute_cands(L, sm, R, sched[d], pa, mask, cand + d * L.W);
         }
     }
     __syncwarp();
@@ -359,17 +401,41 @@ __device__ uint32_t build_child(const Layout& L, char* sm, const DevRule& R, con
 // sorted neighbour folds until the distinct-colour count stops changing (<= 100), then the
 // component fold and the final FNV over (n_v, n_e, sums).
 // ------------------------------------------------------------------------------------------
-__device__ uint32_t wl_distinct(const uint64_t* cur, const uint32_t* deg, uint32_t V) {
-    uint32_t cnt = 0;
-    for (uint32_t v = lane_id(); v < V; v += 32) {
-        if (!deg[v]) continue;
-        const uint64_t c = cur[v];
-        bool first = true;
-        for (uint32_t u = 0; u < v; ++u)
-            if (deg[u] && cur[u] == c) { first = false; break; }
-        cnt += first ? 1u : 0u;
+__device__ uint32_t wl_distinct(const uint64_t* cur, const uint32_t* deg, uint32_t V, uint32_t nv,
+                                uint64_t* srt) {
+    const uint32_t lane = lane_id();
+    if (V <= 32) {
+        // one vertex per lane: equal colours found by match_any among the present lanes
+        const bool present = lane < V && deg[lane] != 0;
+        const uint32_t pm = __ballot_sync(0xFFFFFFFFu, present);
+        bool lead = false;
+        if (present) {
+            const uint32_t grp = __match_any_sync(pm, static_cast<unsigned long long>(cur[lane]));
+            lead = lane == static_cast<uint32_t>(__ffs(grp) - 1);
+        }
+        return __popc(__ballot_sync(0xFFFFFFFFu, lead));
     }
-    return warp_sum32(cnt);
+    // bitonic sort of the present colours (absent ones padded with the maximum), then count
+    // the distinct values among the first nv
+    uint32_t n2 = 64;
+    while (n2 < V) n2 <<= 1;
+    for (uint32_t i = lane; i < n2; i += 32) srt[i] = (i < V && deg[i]) ? cur[i] : ~0ull;
+    __syncwarp();
+    for (uint32_t k = 2; k <= n2; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = lane; i < n2; i += 32) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const uint64_t a = srt[i], b = srt[l];
+                    if ((a > b) == ((i & k) == 0)) { srt[i] = b; srt[l] = a; }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    uint32_t d = 0;
+    for (uint32_t i = lane; i < nv; i += 32) d += (i == 0 || srt[i] != srt[i - 1]) ? 1u : 0u;
+    return warp_sum32(d);
 }
 
 __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, WlInfo& info) {
@@ -460,7 +526,8 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, 
         cur[v] = h;
     }
     __syncwarp();
-    uint32_t prev = wl_distinct(cur, deg, V);
+    uint64_t* srt = smp<uint64_t>(sm, L.o_srt);
+    uint32_t prev = wl_distinct(cur, deg, V, nv, srt);
     for (uint32_t it = 0; it < kWlMaxRounds; ++it) {
         for (uint32_t v = lane; v < V; v += 32) {
             const uint32_t dv = deg[v];
@@ -483,7 +550,7 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, 
         __syncwarp();
         for (uint32_t v = lane; v < V; v += 32) cur[v] = nxt[v];
         __syncwarp();
-        const uint32_t dd = wl_distinct(cur, deg, V);
+        const uint32_t dd = wl_distinct(cur, deg, V, nv, srt);
         ++info.rounds;
         if (dd == prev) break;
         prev = dd;
@@ -492,16 +559,21 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, 
     // components (union-find on one lane; the partition is what enters the hash)
     for (uint32_t v = lane; v < V; v += 32) { comp[v] = v; csum[v] = 0; ccnt[v] = 0; }
     __syncwarp();
-    if (lane == 0) {
-        for (uint32_t e = 0; e < ne; ++e) {
+    // lock-free union-find: a root is only ever hooked under a smaller root (atomicCAS), so the
+    // forest stays acyclic and every failed hook means another lane made progress
+    {
+        volatile uint32_t* vc = comp;
+        for (uint32_t e = lane; e < ne; e += 32) {
             const uint32_t a = car[e], vo = cvo[e];
-            if (!a) continue;
-            uint32_t r = vloc[vo];
-            while (comp[r] != r) { comp[r] = comp[comp[r]]; r = comp[r]; }
             for (uint32_t q = 1; q < a; ++q) {
-                uint32_t x = vloc[vo + q];
-                while (comp[x] != x) { comp[x] = comp[comp[x]]; x = comp[x]; }
-                if (x != r) comp[x] = r;
+                uint32_t x = vloc[vo], y = vloc[vo + q];
+                for (uint32_t tries = 0; tries < 2 * V + 8; ++tries) {
+                    while (vc[x] != x) x = vc[x];
+                    while (vc[y] != y) y = vc[y];
+                    if (x == y) break;
+                    if (x < y) { const uint32_t t = x; x = y; y = t; }
+                    if (atomicCAS(&comp[x], x, y) == x) break;
+                }
             }
         }
     }
@@ -543,6 +615,221 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, 
     return h;
 }
 
+
+
+// ------------------------------------------------------------------------------------------
+// Incremental match forwarding (reference: hypergraph/src/parallel_evolution.cpp:630-755,
+// forward_existing_parent_matches; hypergraph/include/hypergraph/pattern_matcher.hpp:469-537,
+// find_delta_matches). A state created by event c from parent p has as matches exactly
+//   F = the parent's matches (= p's events, already in canonical order) avoiding c's consumed
+//       edges, plus
+//   D = matches using at least one edge c produced, found by joins seeded at each produced edge
+//       in each LHS position and kept only when the seed position is the first position that
+//       holds a produced edge (so each is found once);
+// F and D are disjoint, and merging them by the canonical key (state positions in schedule
+// order) gives the same sequence the full join enumerates. Edge ids are stable and positions are
+// monotone in ids, so F stays sorted.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t fwd_key(const DevRule& R, const uint16_t* pos) {
+    uint64_t k = 0;
+    for (uint32_t i = 0; i < R.n_lhs; ++i) k = (k << 16) | pos[R.sched[i]];
+    return k;
+}
+
+// Delta matches of state `pa` into dkey2/dpos2, sorted by key. Returns their number, or kNone
+// if more than kFwdCap (the state is then re-joined instead).
+__device__ uint32_t fwd_collect_delta(const Layout& L, char* sm, const DevRule& R, const Parent& pa,
+                                      uint32_t prod0) {
+    const uint32_t lane = lane_id();
+    const uint32_t n = R.n_lhs;
+    uint8_t* sched2 = smp<uint8_t>(sm, L.o_sched2);
+    uint64_t* dkey = smp<uint64_t>(sm, L.o_dkey);
+    uint16_t* dpos = smp<uint16_t>(sm, L.o_dpos);
+    uint64_t* dkey2 = smp<uint64_t>(sm, L.o_dkey2);
+    uint16_t* dpos2 = smp<uint16_t>(sm, L.o_dpos2);
+    const uint16_t* match = smp<uint16_t>(sm, L.o_match);
+    uint32_t nd = 0;
+    bool over = false;
+    for (uint32_t x = prod0; x < pa.ne && !over; ++x) {
+        for (uint32_t q = 0; q < n && !over; ++q) {
+            if (lane == 0) {
+                sched2[0] = static_cast<uint8_t>(q);
+                uint32_t k = 1;
+                for (uint32_t i = 0; i < n; ++i)
+                    if (R.sched[i] != q) sched2[k++] = R.sched[i];
+            }
+            __syncwarp();
+            warp_join(L, sm, R, pa, sched2, static_cast<int>(x), [&](uint32_t) {
+                uint32_t first = n;
+                for (uint32_t k = 0; k < n; ++k)
+                    if (match[k] >= prod0) { first = k; break; }
+                if (first != q || over) return;
+                if (nd >= kFwdCap) { over = true; return; }
+                if (lane < n) dpos[nd * kFwdMaxLhs + lane] = match[lane];
+                if (lane == 0) dkey[nd] = fwd_key(R, match);
+                ++nd;
+                __syncwarp();
+            });
+        }
+    }
+    if (over) return kNone;
+    __syncwarp();
+    for (uint32_t i = lane; i < nd; i += 32) {
+        const uint64_t k = dkey[i];
+        uint32_t r = 0;
+        for (uint32_t j = 0; j < nd; ++j) r += dkey[j] < k ? 1u : 0u;
+        dkey2[r] = k;
+        for (uint32_t t = 0; t < kFwdMaxLhs; ++t) dpos2[r * kFwdMaxLhs + t] = dpos[i * kFwdMaxLhs + t];
+    }
+    __syncwarp();
+    return nd;
+}
+
+// State position of edge id `id` in the staged state (ids ascending).
+__device__ __forceinline__ uint32_t fwd_find(const uint32_t* peid, uint32_t ne, uint32_t id) {
+    uint32_t lo = 0, hi = ne;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (peid[mid] < id) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+struct Fwd {
+    bool on;
+    uint32_t e0, en;     // the parent's events
+    uint32_t nk;         // consumed edges of the creating event (ids in smem o_fkc)
+    uint32_t prod0;      // state position of the first produced edge
+    uint32_t nd;         // delta matches (sorted in dkey2 / dpos2)
+};
+
+// Decide forwarding for a staged state and collect its delta matches.
+__device__ Fwd fwd_prepare(const DevPtrs& P, const LevelArgs& A, const Layout& L, char* sm,
+                           const DevRule& R, const DevEvo& ev, const Parent& pa, uint32_t sid,
+                           bool want) {
+    Fwd f;
+    f.on = false;
+    f.e0 = f.en = f.nk = f.prod0 = f.nd = 0;
+    if (!want || A.fwd_mode == 0 || ev.rule_count != 1 || R.n_lhs > kFwdMaxLhs || R.n_rhs > pa.ne)
+        return f;
+    if (A.fwd_mode == 2 && pa.ne < 48) return f;
+    const uint32_t c = P.st_event[sid];
+    const uint32_t parent = c == kNone ? kNone : P.ev_in[c];
+    if (parent == kNone) return f;   // a root
+    uint32_t* kc = smp<uint32_t>(sm, L.o_fkc);
+    const uint32_t lane = lane_id();
+    const uint32_t co = P.ev_coff[c];
+    if (lane < R.n_lhs) kc[lane] = P.ev_cons[co + lane];
+    f.nk = R.n_lhs;
+    f.e0 = P.st_ev0[parent];
+    f.en = P.st_evn[parent];
+    f.prod0 = pa.ne - R.n_rhs;
+    __syncwarp();
+    const uint32_t nd = fwd_collect_delta(L, sm, R, pa, f.prod0);
+    if (nd == kNone) return f;
+    f.nd = nd;
+    f.on = true;
+    return f;
+}
+
+// Forwarded parent matches, 32 at a time: for each one avoiding the consumed edges, its state
+// positions (pattern order) and key into fkey/fpos[slot]. Returns how many of the 32 survived.
+__device__ uint32_t fwd_chunk(const DevPtrs& P, const Layout& L, char* sm, const DevRule& R,
+                              const Parent& pa, const Fwd& f, uint32_t base) {
+    const uint32_t lane = lane_id();
+    const uint32_t* kc = smp<uint32_t>(sm, L.o_fkc);
+    const uint32_t* peid = smp<uint32_t>(sm, L.o_peid);
+    uint64_t* fkey = smp<uint64_t>(sm, L.o_fkey);
+    uint16_t* fpos = smp<uint16_t>(sm, L.o_fpos);
+    bool valid = base + lane < f.en;
+    uint16_t pos[kFwdMaxLhs] = {0, 0, 0, 0};
+    if (valid) {
+        const uint32_t e = f.e0 + base + lane;
+        const uint32_t co = P.ev_coff[e];
+        for (uint32_t k = 0; k < R.n_lhs && valid; ++k) {
+            const uint32_t id = P.ev_cons[co + k];
+            for (uint32_t m = 0; m < f.nk; ++m) valid &= kc[m] != id;
+            pos[k] = static_cast<uint16_t>(fwd_find(peid, pa.ne, id));
+        }
+    }
+    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, valid);
+    if (valid) {
+        const uint32_t slot = __popc(bal & ((1u << lane) - 1u));
+        fkey[slot] = fwd_key(R, pos);
+        for (uint32_t k = 0; k < kFwdMaxLhs; ++k) fpos[slot * kFwdMaxLhs + k] = pos[k];
+    }
+    __syncwarp();
+    return __popc(bal);
+}
+
+// Emit one match given by its state positions (pattern order): sets match / taken / binding
+// exactly as the join does, then calls on_match.
+template <class F>
+__device__ void fwd_emit(const Layout& L, char* sm, const DevRule& R, const uint16_t* pos,
+                         F&& on_match) {
+    const uint32_t lane = lane_id();
+    uint16_t* match = smp<uint16_t>(sm, L.o_match);
+    uint32_t* taken = smp<uint32_t>(sm, L.o_taken);
+    uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
+    const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    uint32_t nm = 0;
+    for (uint32_t k = 0; k < R.n_lhs; ++k) {
+        const uint32_t e = pos[k];
+        const uint32_t a = R.lhs_ar[k], vo = pevo[e];
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t var = R.lhs_vars[R.lhs_off[k] + q];
+            if (lane == 0) bind[var] = vloc[vo + q];
+            nm |= 1u << var;
+        }
+        if (lane == 0) {
+            match[k] = static_cast<uint16_t>(e);
+            taken[e >> 5] |= 1u << (e & 31u);
+        }
+    }
+    __syncwarp();
+    on_match(nm);
+    __syncwarp();
+    if (lane == 0)
+        for (uint32_t k = 0; k < R.n_lhs; ++k) taken[pos[k] >> 5] &= ~(1u << (pos[k] & 31u));
+    __syncwarp();
+}
+
+// Every match of the staged state in canonical order: the full join, or forwarding.
+template <class F>
+__device__ void enumerate_matches(const DevPtrs& P, const Layout& L, char* sm, const DevRule& R,
+                                  const Parent& pa, const Fwd& f, F&& on_match) {
+    if (!f.on) {
+        warp_join(L, sm, R, pa, R.sched, -1, on_match);
+        return;
+    }
+    const uint32_t lane = lane_id();
+    uint32_t* taken = smp<uint32_t>(sm, L.o_taken);
+    for (uint32_t w = lane; w < L.W; w += 32) taken[w] = 0;
+    __syncwarp();
+    const uint64_t* dkey2 = smp<uint64_t>(sm, L.o_dkey2);
+    const uint16_t* dpos2 = smp<uint16_t>(sm, L.o_dpos2);
+    const uint64_t* fkey = smp<uint64_t>(sm, L.o_fkey);
+    const uint16_t* fpos = smp<uint16_t>(sm, L.o_fpos);
+    uint32_t j = 0;
+    for (uint32_t base = 0; base < f.en; base += 32) {
+        const uint32_t m = fwd_chunk(P, L, sm, R, pa, f, base);
+        for (uint32_t t = 0; t < m; ++t) {
+            while (j < f.nd && dkey2[j] < fkey[t]) fwd_emit(L, sm, R, dpos2 + j++ * kFwdMaxLhs, on_match);
+            fwd_emit(L, sm, R, fpos + t * kFwdMaxLhs, on_match);
+        }
+        __syncwarp();
+    }
+    while (j < f.nd) fwd_emit(L, sm, R, dpos2 + j++ * kFwdMaxLhs, on_match);
+}
+
+// Number of matches under forwarding (F survivors + D).
+__device__ uint32_t fwd_count(const DevPtrs& P, const Layout& L, char* sm, const DevRule& R,
+                              const Parent& pa, const Fwd& f) {
+    uint32_t c = f.nd;
+    for (uint32_t base = 0; base < f.en; base += 32) c += fwd_chunk(P, L, sm, R, pa, f, base);
+    return c;
+}
 
 // ------------------------------------------------------------------------------------------
 // Lane-per-child WL. For the small states that dominate deep evolutions (a handful of
@@ -661,6 +948,7 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
                         if (vloc[pevo[e] + q] == lane) nn += pear[e] - 1u;
             pnn_max = warp_max32(nn);
         }
+        bool fwd_on = false;
         for (uint32_t r = 0; r < A.rules_stride; ++r) {
             uint32_t cnt = 0;
             if (r < ev.rule_count) {
@@ -668,12 +956,15 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
                 uint32_t gain = 0;
                 for (uint32_t k = 0; k < R.n_rhs; ++k) gain += uint32_t(R.rhs_ar[k]) * (R.rhs_ar[k] - 1u);
                 lane_ok = lane_ok && pa.nvp + R.n_fresh <= kLaneVMax && pnn_max + gain <= kLaneNMax;
-                warp_join(L, sm, R, pa, [&](uint32_t) { ++cnt; });
+                const Fwd fw = fwd_prepare(P, A, L, sm, R, ev, pa, sid, true);
+                fwd_on = fw.on;
+                if (fw.on) cnt = fwd_count(P, L, sm, R, pa, fw);
+                else warp_join(L, sm, R, pa, R.sched, -1, [&](uint32_t) { ++cnt; });
             }
             if (lane == 0) A.counts[f * A.rules_stride + r] = cnt;
             __syncwarp();
         }
-        if (lane == 0) A.fmode[f] = lane_ok ? 1 : 0;
+        if (lane == 0) A.fmode[f] = (lane_ok ? 1 : 0) | (fwd_on ? 2 : 0);
     }
 }
 
@@ -720,7 +1011,8 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
         if (lane == 0) f = A.f_begin + atomicAdd(work, 1u);
         f = __shfl_sync(0xFFFFFFFFu, f, 0);
         if (f >= A.f_end) break;
-        if ((A.fmode[f] != 0) != kLane) continue;
+        const uint8_t fm = A.fmode[f];
+        if (((fm & 1u) != 0) != kLane) continue;
         const uint32_t sid = A.frontier[f];
         const Parent pa = load_parent(P, L, sm, sid);
         const uint32_t evo = P.st_evo[sid];
@@ -737,6 +1029,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
             const uint32_t prod0 = A.prod_base + A.item_prod[item];
             const uint32_t fresh0 = A.fresh_base + A.item_fresh[item];
             const uint32_t rule_g = ev.rule_begin + r;
+            const Fwd fwd = fwd_prepare(P, A, L, sm, R, ev, pa, sid, (fm & 2u) != 0);
             // per-child work shared by both paths: the event record and the table insert
             auto finish = [&](uint32_t idx, uint64_t h, const WlInfo& info, const uint8_t* rpos) {
                 const uint32_t e = ev0 + idx;
@@ -776,7 +1069,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                     done += nb;
                     nb = 0;
                 };
-                warp_join(L, sm, R, pa, [&](uint32_t nm) {
+                enumerate_matches(P, L, sm, R, pa, fwd, [&](uint32_t nm) {
                     uint8_t* slot = batch + nb * L.SB;
                     if (lane < R.n_lhs) slot[lane] = static_cast<uint8_t>(match[lane]);
                     for (uint32_t t = lane; t < R.rhs_total; t += 32) {
@@ -791,7 +1084,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
             } else {
                 uint32_t idx = 0;
                 uint8_t rpos[kMaxPatternEdges];
-                warp_join(L, sm, R, pa, [&](uint32_t nm) {
+                enumerate_matches(P, L, sm, R, pa, fwd, [&](uint32_t nm) {
                     for (uint32_t k = 0; k < R.n_lhs; ++k) rpos[k] = static_cast<uint8_t>(match[k]);
                     const uint32_t nec = build_child(L, sm, R, pa, nm);
                     WlInfo info;
@@ -980,6 +1273,18 @@ __global__ void k_gather_pairs(const uint32_t* pairs, const uint64_t* rstart, co
         const uint64_t g = rstart[k] + (i - rcum[k]);
         out[2 * i] = emap[pairs[2 * g]];
         out[2 * i + 1] = emap[pairs[2 * g + 1]];
+    }
+}
+
+// Each frontier state's event range (its matches, in canonical order), for its children's
+// match forwarding. Single-rule evolutions only (item f * R of the state).
+__global__ void k_fwd_record(DevPtrs P, LevelArgs A) {
+    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
+         f += gridDim.x * blockDim.x) {
+        const uint32_t sid = A.frontier[f];
+        const uint32_t t = f * A.rules_stride;
+        P.st_ev0[sid] = A.ev_base + A.item_ev[t];
+        P.st_evn[sid] = A.item_ev[t + 1] - A.item_ev[t];
     }
 }
 

@@ -31,6 +31,8 @@ struct DevPtrs {
     uint32_t* st_evo;
     uint32_t* st_depth;
     uint32_t* st_event;     // arrival (event or root pseudo-event) that created it
+    uint32_t* st_ev0;       // first event of the state's expansion (single-rule evolutions)
+    uint32_t* st_evn;       // events of the state's expansion
     uint64_t* st_hash;
     uint32_t* arena;        // per-state records: ids[ne] | arity bytes[ceil(ne/4) words] | verts[nocc]
     unsigned long long* arena_top;
@@ -79,7 +81,8 @@ struct LevelArgs {
     uint32_t ev_base, cons_base, prod_base, fresh_base;   // level bases
     uint32_t n_events;          // events minted this level
     uint32_t f_begin, f_end;    // frontier range the expand kernel works on
-    uint8_t* fmode;             // [F] 1 = the state's children are hashed lane-per-child
+    uint8_t* fmode;             // [F] bit 0: children hashed lane-per-child; bit 1: forwarding
+    uint32_t fwd_mode;          // 0 off, 1 every eligible state, 2 states with >= 48 edges
     uint32_t* work;             // work-queue counters
     // select / assign
     uint32_t* flag_new;         // [n_events]
@@ -109,7 +112,12 @@ struct Layout {
     // lane-per-child path: parent occurrence lists by vertex, per-vertex degree / neighbour
     // counts, and a batch of up to 32 matches (removed positions + produced local vertices)
     uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_batch;
+    // match forwarding: seeded schedule, creating event's consumed edges, delta matches (and a
+    // sorted copy), a 32-match chunk of forwarded matches
+    uint32_t o_sched2, o_fkc, o_dkey, o_dpos, o_dkey2, o_dpos2, o_fkey, o_fpos;
     uint32_t SB;                                                    // bytes per batch slot
+    uint32_t VT, o_vtab, o_vtid;   // vertex hash table for large states (VT slots, 0 = unused)
+    uint32_t o_srt;                // warp WL: sort buffer of the distinct-colour count
     uint32_t bytes;
 };
 

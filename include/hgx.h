@@ -67,7 +67,13 @@ typedef enum hgx_option {
     HGX_OPT_TIMING = 6,
     /* 1 (default) = copy the result to host memory; 0 = keep it on the device and report the
        counts only (hgx_result_count works, hgx_result_copy returns empty arrays). */
-    HGX_OPT_READBACK = 7
+    HGX_OPT_READBACK = 7,
+    /* Incremental match forwarding (reference: ParallelEvolutionEngine::set_match_forwarding,
+       parallel_evolution.hpp:775): a child's matches are its parent's matches that avoid the
+       consumed edges plus the matches through the produced edges, instead of a full re-join.
+       0 (default) = off, 1 = wherever it applies, 2 = states of 48 edges or more. Results are
+       identical in every mode. */
+    HGX_OPT_FORWARDING = 8
 } hgx_option;
 
 /* One evolution of a batch or a served request. */

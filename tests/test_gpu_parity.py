@@ -126,3 +126,33 @@ def test_full_size_workloads_match_oracle(engine, ev):
     assert res.truncated == ref["truncated"]
     assert res.num_classes == ref["classes"]
     assert_same(norm_gpu(res), norm_oracle(ref), ev.name)
+
+
+def _forwarding_cases():
+    out = [(W.config2(6), None), (W.config3(5), None),
+           (W.Evolution(rules=[cases.C1_RULE], roots=[cases.C1_INIT], steps=4, quotient=False), None),
+           # a hub of 100 edges: delta matches overflow the forwarding buffer (fallback path)
+           (W.Evolution(rules=[cases.C2_RULE], roots=[[[1, k] for k in range(2, 102)]], steps=2,
+                        max_states=3000), None)]
+    for name, rules, init, depth in cases.CORPUS:
+        out.append((W.Evolution(rules=rules, roots=[init], steps=depth + 1, quotient=True), name))
+    return out
+
+
+@pytest.mark.parametrize("mode", [1, 0, 2])
+def test_forwarding_modes_match_oracle(engine, mode):
+    from hypergraphrewritingengine_b200 import api
+    engine.set_option(api.OPT_FORWARDING, mode)
+    try:
+        for ev, name in _forwarding_cases():
+            res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient,
+                                max_states=ev.max_states)
+            ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient,
+                                  max_states=ev.max_states)
+            assert_same(norm_gpu(res), norm_oracle(ref), f"{name or ev.name} forwarding={mode}")
+        evs = W.config4(n=32, max_states=1024)   # initial states up to 64 edges
+        for ev, res in zip(evs, engine.evolve_batch(evs)):
+            ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} forwarding={mode}")
+    finally:
+        engine.set_option(api.OPT_FORWARDING, 2)
