@@ -32,7 +32,7 @@ LIB_PATH = os.path.join(HERE, "libhgx.so")
 
 HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_ERR_INTERNAL = range(6)
 (OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
- OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING) = range(9)
+ OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING, OPT_CHUNK_MIN) = range(10)
 (COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
  COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES) = range(10)
 (ARR_STATE_HASH, ARR_STATE_DEPTH, ARR_EVENTS, ARR_CAUSAL, ARR_BRANCHIAL, ARR_EVENT_CONS_OFF,
@@ -43,7 +43,7 @@ HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_
 EXPORTS = (
     "hgx_last_error", "hgx_version", "hgx_engine_create", "hgx_engine_destroy",
     "hgx_engine_add_rule", "hgx_engine_clear_rules", "hgx_engine_set_option", "hgx_evolve",
-    "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_step",
+    "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_admit_batch", "hgx_serve_step",
     "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_device_bytes", "hgx_result_count",
     "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
     "hgx_engine_stream", "hgx_hash_states_noalloc", "hgx_result_view",
@@ -88,6 +88,7 @@ def load_library(path: str = LIB_PATH):
         "hgx_evolve_batch": ([vp, ctypes.POINTER(Job), ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
         "hgx_serve_reset": ([vp], ctypes.c_int),
         "hgx_serve_admit": ([vp, ctypes.POINTER(Job), u32p], ctypes.c_int),
+        "hgx_serve_admit_batch": ([vp, ctypes.POINTER(Job), ctypes.c_uint32, u32p], ctypes.c_int),
         "hgx_serve_step": ([vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "hgx_serve_take_finished": ([vp, u32p, ctypes.c_uint32, u32p], ctypes.c_int),
         "hgx_serve_collect": ([vp, ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
@@ -321,6 +322,13 @@ class Engine:
         i = ctypes.c_uint32()
         _check(self._L.hgx_serve_admit(self._h, ctypes.byref(job), ctypes.byref(i)))
         return int(i.value)
+
+    def serve_admit_batch(self, jobs, n: int | None = None) -> list:
+        """Admit the first n jobs of a Job array in one call; returns their evolution ids."""
+        n = len(jobs) if n is None else n
+        ids = (ctypes.c_uint32 * max(n, 1))()
+        _check(self._L.hgx_serve_admit_batch(self._h, jobs, n, ids))
+        return list(ids[:n])
 
     def serve_step(self) -> bool:
         a = ctypes.c_int()

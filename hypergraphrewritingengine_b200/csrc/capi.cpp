@@ -228,6 +228,7 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
             if (value > 2) return fail(HGX_ERR_INVALID, "forwarding mode must be 0, 1 or 2");
             e->opt.forwarding = static_cast<uint32_t>(value);
             return HGX_OK;
+        case HGX_OPT_CHUNK_MIN: e->opt.chunk_min = value; return HGX_OK;
     }
     return fail(HGX_ERR_INVALID, "unknown option");
 }
@@ -273,6 +274,18 @@ hgx_status hgx_serve_admit(hgx_engine* e, const hgx_job* job, uint32_t* id) {
     if (!e || !job || !id) return fail(HGX_ERR_INVALID, "null argument");
     return guarded([&] {
         *id = e->engine.admit(spec_of(*job));
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_serve_admit_batch(hgx_engine* e, const hgx_job* jobs, uint32_t n, uint32_t* ids) {
+    if (!e || (n && (!jobs || !ids))) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        std::vector<hgx::EvolutionSpec> specs;
+        specs.reserve(n);
+        for (uint32_t i = 0; i < n; ++i) specs.push_back(spec_of(jobs[i]));
+        const std::vector<uint32_t> got = e->engine.admit(specs);
+        for (uint32_t i = 0; i < n; ++i) ids[i] = got[i];
         return HGX_OK;
     });
 }

@@ -283,7 +283,8 @@ struct Engine::Impl {
     DVec<uint32_t> bcount, boff, bpairs, scan_sums, sync_buf, root_ids;
     DVec<unsigned long long> stats, totals;
     DVec<uint8_t> fmode, fin;
-    DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e;
+    DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e, frng, slice_off;
+    DVec<unsigned long long> evo_new;
     DVec<uint64_t> fin_rng;
     // Per evolution: the contiguous id ranges it owns, one entry per level (roots first).
     struct EvoRanges {
@@ -359,6 +360,9 @@ struct Engine::Impl {
         fin.release(st);
         fin_cnt.release(st);
         evo_frange.release(st);
+        frng.release(st);
+        slice_off.release(st);
+        evo_new.release(st);
         lvl_ranges.release(st);
         fin_ids.release(st);
         map_s.release(st);
@@ -517,125 +521,175 @@ struct Engine::Impl {
     }
 
     // ---- admission ------------------------------------------------------------------------
-    uint32_t admit(const EvolutionSpec& spec) {
-        if (spec.rules.empty()) throw std::invalid_argument("evolve: no rules");
-        if (spec.roots.empty()) throw std::invalid_argument("evolve: no initial state");
-        const uint32_t evo = static_cast<uint32_t>(h_evos.size());
-        DevEvo d;
-        std::memset(&d, 0, sizeof(d));
-        d.rule_begin = static_cast<uint32_t>(h_rules.size());
-        d.rule_count = static_cast<uint32_t>(spec.rules.size());
-        d.steps = spec.steps;
-        d.quotient = spec.quotient ? 1u : 0u;
-        d.max_states = spec.max_states;
-        for (const auto& r : spec.rules) {
-            DevRule pr = pack_rule(r);
-            h_rules.push_back(pr);
-            rm.rhs = std::max<uint32_t>(rm.rhs, pr.n_rhs);
-            rm.rhs_total = std::max<uint32_t>(rm.rhs_total, pr.rhs_total);
-            rm.fresh = std::max<uint32_t>(rm.fresh, pr.n_fresh);
-            rm.lhs = std::max<uint32_t>(rm.lhs, pr.n_lhs);
-            for (uint32_t i = 0; i < pr.n_rhs; ++i) rm.arity = std::max<uint32_t>(rm.arity, pr.rhs_ar[i]);
-            rm.grow_e = std::max<int>(rm.grow_e, int(pr.n_rhs) - int(pr.n_lhs));
-            rm.grow_o = std::max<int>(rm.grow_o, int(pr.rhs_total) - int(pr.lhs_total));
-        }
-        rm.stride = std::max<uint32_t>(rm.stride, d.rule_count);
+    //
+    // A batch is validated and packed on the host first (nothing changes if a spec is invalid),
+    // then uploaded with one copy per array and its roots hashed in one launch.
+    uint32_t admit(const EvolutionSpec& spec) { return admit_many({&spec}).front(); }
 
-        // roots: edge records, uploaded to the arena
+    std::vector<uint32_t> admit_many(const std::vector<const EvolutionSpec*>& specs) {
+        // phase 1: validate and pack (no engine state is touched)
+        struct Packed {
+            std::vector<DevRule> rules;
+            std::vector<uint32_t> words;     // root records with edge ids relative to the batch
+            std::vector<uint32_t> nes, noccs;
+            std::vector<uint64_t> rel_off;   // record offsets relative to the batch's words
+            uint32_t arity = 0;
+            uint64_t max_label = 0;
+        };
+        std::vector<Packed> pk(specs.size());
+        uint64_t batch_words = 0, batch_edges = 0;
+        for (size_t i = 0; i < specs.size(); ++i) {
+            const EvolutionSpec& spec = *specs[i];
+            Packed& q = pk[i];
+            if (spec.rules.empty()) throw std::invalid_argument("evolve: no rules");
+            if (spec.roots.empty()) throw std::invalid_argument("evolve: no initial state");
+            for (const auto& r : spec.rules) q.rules.push_back(pack_rule(r));
+            for (const auto& root : spec.roots) {
+                const uint32_t ne = static_cast<uint32_t>(root.size());
+                if (ne == 0) throw std::invalid_argument("evolve: an initial state has no edges");
+                uint32_t nocc = 0;
+                for (const auto& e : root) {
+                    if (e.empty() || e.size() > kMaxArity)
+                        throw std::invalid_argument("evolve: initial edge arity must be 1..16");
+                    nocc += static_cast<uint32_t>(e.size());
+                    q.arity = std::max<uint32_t>(q.arity, static_cast<uint32_t>(e.size()));
+                    for (uint32_t v : e) {
+                        if (v == kNone) throw std::invalid_argument("evolve: vertex label 4294967295 is reserved");
+                        q.max_label = std::max<uint64_t>(q.max_label, v);
+                    }
+                }
+                q.rel_off.push_back(batch_words + q.words.size());
+                q.nes.push_back(ne);
+                q.noccs.push_back(nocc);
+                const uint32_t aw = (ne + 3) / 4;
+                const size_t base = q.words.size();
+                q.words.resize(base + ne + aw + nocc, 0);
+                uint32_t vo = 0;
+                for (uint32_t k = 0; k < ne; ++k) {
+                    q.words[base + k] = static_cast<uint32_t>(batch_edges + k);   // + n_edges below
+                    q.words[base + ne + k / 4] |= static_cast<uint32_t>(root[k].size()) << ((k % 4) * 8);
+                    for (uint32_t v : root[k]) q.words[base + ne + aw + vo++] = v;
+                }
+                batch_edges += ne;
+            }
+            batch_words += q.words.size();
+        }
+        if (specs.empty()) return {};
+
+        // phase 2: host mirrors and per-root host arrays
+        const uint32_t evo0 = static_cast<uint32_t>(h_evos.size());
+        const size_t rules0 = h_rules.size();
+        const uint64_t s0 = n_states, a0 = n_events, edges0 = n_edges, arena0 = arena_words, tab0 = tab_slots;
         std::vector<uint32_t> words;
+        words.reserve(batch_words);
         std::vector<uint64_t> offs;
-        std::vector<uint32_t> nes, noccs;
+        std::vector<uint32_t> nes, noccs, h_evo, h_ev, h_sid, h_front;
+        std::vector<uint32_t> ids;
         uint64_t max_label = 0;
-        for (const auto& root : spec.roots) {
-            const uint32_t ne = static_cast<uint32_t>(root.size());
-            uint32_t nocc = 0;
-            for (const auto& e : root) {
-                if (e.empty() || e.size() > kMaxArity)
-                    throw std::invalid_argument("evolve: initial edge arity must be 1..16");
-                nocc += static_cast<uint32_t>(e.size());
-                rm.arity = std::max<uint32_t>(rm.arity, static_cast<uint32_t>(e.size()));
-                for (uint32_t v : e) {
-                    if (v == kNone) throw std::invalid_argument("evolve: vertex label 4294967295 is reserved");
-                    max_label = std::max<uint64_t>(max_label, v);
+        for (size_t i = 0; i < specs.size(); ++i) {
+            const EvolutionSpec& spec = *specs[i];
+            Packed& q = pk[i];
+            const uint32_t evo = evo0 + static_cast<uint32_t>(i);
+            DevEvo d;
+            std::memset(&d, 0, sizeof(d));
+            d.rule_begin = static_cast<uint32_t>(h_rules.size());
+            d.rule_count = static_cast<uint32_t>(q.rules.size());
+            d.steps = spec.steps;
+            d.quotient = spec.quotient ? 1u : 0u;
+            d.max_states = spec.max_states;
+            for (const DevRule& pr : q.rules) {
+                h_rules.push_back(pr);
+                rm.rhs = std::max<uint32_t>(rm.rhs, pr.n_rhs);
+                rm.rhs_total = std::max<uint32_t>(rm.rhs_total, pr.rhs_total);
+                rm.fresh = std::max<uint32_t>(rm.fresh, pr.n_fresh);
+                rm.lhs = std::max<uint32_t>(rm.lhs, pr.n_lhs);
+                for (uint32_t k = 0; k < pr.n_rhs; ++k) rm.arity = std::max<uint32_t>(rm.arity, pr.rhs_ar[k]);
+                rm.grow_e = std::max<int>(rm.grow_e, int(pr.n_rhs) - int(pr.n_lhs));
+                rm.grow_o = std::max<int>(rm.grow_o, int(pr.rhs_total) - int(pr.lhs_total));
+            }
+            rm.stride = std::max<uint32_t>(rm.stride, d.rule_count);
+            rm.arity = std::max<uint32_t>(rm.arity, q.arity);
+            max_label = std::max(max_label, q.max_label);
+            const uint32_t nr = static_cast<uint32_t>(q.nes.size());
+            for (uint32_t k = 0; k < nr; ++k) {
+                const uint32_t ne = q.nes[k];
+                ne_bound = std::max(ne_bound, ne);
+                nocc_bound = std::max(nocc_bound, q.noccs[k]);
+                offs.push_back(arena0 + q.rel_off[k]);
+                nes.push_back(ne);
+                noccs.push_back(q.noccs[k]);
+                const uint32_t sid = static_cast<uint32_t>(s0 + h_sid.size());
+                h_ev.push_back(static_cast<uint32_t>(a0 + h_sid.size()));
+                h_sid.push_back(sid);
+                h_evo.push_back(evo);
+                if (spec.steps > 0) h_front.push_back(sid);
+            }
+            // edge ids in the records are relative to the batch: shift by the edge counter
+            {
+                size_t base = 0;
+                for (uint32_t k = 0; k < nr; ++k) {
+                    const uint32_t ne = q.nes[k], aw = (ne + 3) / 4;
+                    for (uint32_t j = 0; j < ne; ++j) q.words[base + j] += static_cast<uint32_t>(edges0);
+                    base += ne + aw + q.noccs[k];
                 }
             }
-            if (ne == 0) throw std::invalid_argument("evolve: an initial state has no edges");
-            offs.push_back(arena_words + words.size());
-            nes.push_back(ne);
-            noccs.push_back(nocc);
-            const uint32_t aw = (ne + 3) / 4;
-            const size_t base = words.size();
-            words.resize(base + ne + aw + nocc, 0);
-            uint32_t vo = 0;
-            for (uint32_t i = 0; i < ne; ++i) {
-                words[base + i] = static_cast<uint32_t>(n_edges + i);
-                words[base + ne + i / 4] |= static_cast<uint32_t>(root[i].size()) << ((i % 4) * 8);
-                for (uint32_t v : root[i]) words[base + ne + aw + vo++] = v;
-            }
-            n_edges += ne;
-            ne_bound = std::max(ne_bound, ne);
-            nocc_bound = std::max(nocc_bound, nocc);
+            words.insert(words.end(), q.words.begin(), q.words.end());
+            // dedup table region
+            const uint64_t cap = next_pow2(std::max<uint64_t>(256, 4ull * nr));
+            d.table_off = tab_slots;
+            d.table_mask = cap - 1;
+            tab_slots += cap + 1;
+            evo_ranges.emplace_back();
+            evo_ranges.back().states.emplace_back(static_cast<uint32_t>(s0 + h_sid.size() - nr),
+                                                  static_cast<uint32_t>(s0 + h_sid.size()));
+            evo_ranges.back().roots = nr;
+            h_evos.push_back(d);
+            evo_done.push_back(spec.steps > 0 ? 0 : 1);
+            evo_reported.push_back(0);
+            if (spec.steps == 0) finished.push_back(evo);
+            ids.push_back(evo);
         }
+        const uint32_t nr = static_cast<uint32_t>(h_sid.size());
+        const size_t nevo = h_evos.size(), nnew = nevo - evo0;
+        n_edges += batch_edges;
         next_vertex = std::max<uint64_t>(next_vertex, max_label + 1);
-        const uint32_t nr = static_cast<uint32_t>(spec.roots.size());
 
-        // dedup table region
-        const uint64_t cap = next_pow2(std::max<uint64_t>(256, 4ull * nr));
-        d.table_off = tab_slots;
-        d.table_mask = cap - 1;
-        const uint64_t new_slots = tab_slots + cap + 1;
-        tab_keys.ensure(new_slots, tab_slots, st);
-        tab_vals.ensure(new_slots, tab_slots, st);
-        HGX_CUDA_CHECK(cudaMemsetAsync(tab_keys.p + tab_slots, 0, (cap + 1) * sizeof(unsigned long long), st));
-        HGX_CUDA_CHECK(cudaMemsetAsync(tab_vals.p + tab_slots, 0xFF, (cap + 1) * sizeof(uint32_t), st));
-        tab_slots = new_slots;
-
-        h_evos.push_back(d);
-        evo_done.push_back(0);
-        evo_reported.push_back(0);
-        const size_t nevo = h_evos.size();
-        // per-evolution device arrays
-        rules.ensure(h_rules.size(), h_rules.size() - spec.rules.size(), st);
-        HGX_CUDA_CHECK(cudaMemcpyAsync(rules.p + d.rule_begin, h_rules.data() + d.rule_begin,
-                                       spec.rules.size() * sizeof(DevRule), cudaMemcpyHostToDevice, st));
-        evos.ensure(nevo, nevo - 1, st);
-        HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + evo, &h_evos[evo], sizeof(DevEvo), cudaMemcpyHostToDevice, st));
-        evo_classes.ensure(nevo, nevo - 1, st);
-        evo_states.ensure(nevo, nevo - 1, st);
-        evo_cut.ensure(nevo, nevo - 1, st);
-        evo_first_ev.ensure(nevo, nevo - 1, st);
-        evo_last_ev.ensure(nevo, nevo - 1, st);
-        evo_stopped.ensure(nevo, nevo - 1, st);
-        evo_front.ensure(nevo, nevo - 1, st);
-        HGX_CUDA_CHECK(cudaMemsetAsync(evo_classes.p + evo, 0, sizeof(unsigned long long), st));
-        HGX_CUDA_CHECK(cudaMemsetAsync(evo_states.p + evo, 0, sizeof(unsigned long long), st));
-        HGX_CUDA_CHECK(cudaMemsetAsync(evo_cut.p + evo, 0xFF, sizeof(uint32_t), st));
-        HGX_CUDA_CHECK(cudaMemsetAsync(evo_stopped.p + evo, 0, sizeof(uint32_t), st));
-
-        // arena
-        arena.ensure(arena_words + words.size(), arena_words, st);
-        HGX_CUDA_CHECK(cudaMemcpyAsync(arena.p + arena_words, words.data(), words.size() * 4,
-                                       cudaMemcpyHostToDevice, st));
+        // phase 3: device arrays, one copy or fill per array
+        auto up = [&](auto* dst, const auto& src) {
+            if (!src.empty())
+                HGX_CUDA_CHECK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(src[0]), cudaMemcpyHostToDevice, st));
+        };
+        tab_keys.ensure(tab_slots, tab0, st);
+        tab_vals.ensure(tab_slots, tab0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_keys.p + tab0, 0, (tab_slots - tab0) * sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_vals.p + tab0, 0xFF, (tab_slots - tab0) * sizeof(uint32_t), st));
+        rules.ensure(h_rules.size(), rules0, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(rules.p + rules0, h_rules.data() + rules0,
+                                       (h_rules.size() - rules0) * sizeof(DevRule), cudaMemcpyHostToDevice, st));
+        evos.ensure(nevo, evo0, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + evo0, &h_evos[evo0], nnew * sizeof(DevEvo), cudaMemcpyHostToDevice, st));
+        evo_classes.ensure(nevo, evo0, st);
+        evo_states.ensure(nevo, evo0, st);
+        evo_cut.ensure(nevo, evo0, st);
+        evo_first_ev.ensure(nevo, evo0, st);
+        evo_last_ev.ensure(nevo, evo0, st);
+        evo_stopped.ensure(nevo, evo0, st);
+        evo_front.ensure(nevo, evo0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_classes.p + evo0, 0, nnew * sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_states.p + evo0, 0, nnew * sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_cut.p + evo0, 0xFF, nnew * sizeof(uint32_t), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_stopped.p + evo0, 0, nnew * sizeof(uint32_t), st));
+        arena.ensure(arena0 + words.size(), arena0, st);
+        up(arena.p + arena0, words);
         arena_words += words.size();
         const unsigned long long top = arena_words;
         HGX_CUDA_CHECK(cudaMemcpyAsync(arena_top.p, &top, sizeof(top), cudaMemcpyHostToDevice, st));
-        // initial edges have no producer
-        uint64_t total_root_edges = 0;
-        for (uint32_t ne : nes) total_root_edges += ne;
-        const uint64_t e0 = n_edges - total_root_edges;
-        edge_creator.ensure(n_edges, e0, st);
-        HGX_CUDA_CHECK(cudaMemsetAsync(edge_creator.p + e0, 0xFF, total_root_edges * sizeof(uint32_t), st));
-
-        // states and root pseudo-events
-        const uint64_t s0 = n_states, a0 = n_events;
-        grow_states(n_states + nr);
-        grow_events(n_events + nr);
-        std::vector<uint32_t> h_evo(nr, evo), h_zero(nr, 0), h_ev(nr), h_sid(nr), h_none(nr, kNone);
+        edge_creator.ensure(n_edges, edges0, st);   // initial edges have no producer
+        HGX_CUDA_CHECK(cudaMemsetAsync(edge_creator.p + edges0, 0xFF, batch_edges * sizeof(uint32_t), st));
+        grow_states(s0 + nr);
+        grow_events(a0 + nr);
+        std::vector<uint32_t> h_zero(nr, 0), h_none(nr, kNone);
         std::vector<uint8_t> h_kept(nr, 0);
-        for (uint32_t i = 0; i < nr; ++i) { h_ev[i] = static_cast<uint32_t>(a0 + i); h_sid[i] = static_cast<uint32_t>(s0 + i); }
-        auto up = [&](auto* dst, const auto& src) {
-            HGX_CUDA_CHECK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(src[0]), cudaMemcpyHostToDevice, st));
-        };
         up(st_off.p + s0, offs);
         up(st_ne.p + s0, nes);
         up(st_nocc.p + s0, noccs);
@@ -646,39 +700,33 @@ struct Engine::Impl {
         up(ev_out.p + a0, h_sid);
         up(ev_kept.p + a0, h_kept);
         up(state_of_arrival.p + a0, h_sid);
-        evo_ranges.emplace_back();
-        evo_ranges.back().states.emplace_back(static_cast<uint32_t>(s0), static_cast<uint32_t>(s0 + nr));
-        evo_ranges.back().roots = nr;
         n_states += nr;
         n_events += nr;
         n_roots_admitted += nr;
 
-        // hash the roots on the device and seed the table
+        // hash the roots on the device and seed the tables
         root_ids.ensure(nr, 0, st);
         up(root_ids.p, h_sid);
         RuleMax none;
         none.arity = rm.arity;
-        uint32_t mne = *std::max_element(nes.begin(), nes.end());
-        uint32_t mno = *std::max_element(noccs.begin(), noccs.end());
+        const uint32_t mne = *std::max_element(nes.begin(), nes.end());
+        const uint32_t mno = *std::max_element(noccs.begin(), noccs.end());
         Layout L = make_layout(mne, mno, none, LayoutKind::Warp);
         HGX_CUDA_CHECK(cudaMemsetAsync(work.p, 0, 8 * sizeof(uint32_t), st));
-        LaunchShape s = warp_shape(k_roots, L, nr);
+        LaunchShape sh = warp_shape(k_roots, L, nr);
         tic();
-        k_roots<<<s.grid, s.block, s.smem, st>>>(ptrs(), root_ids.p, nr, work.p, L);
+        k_roots<<<sh.grid, sh.block, sh.smem, st>>>(ptrs(), root_ids.p, nr, work.p, L);
         check_launch();
         k_root_counts<<<grid_for(nr, 256), 256, 0, st>>>(ptrs(), root_ids.p, nr);
         check_launch();
         toc(times.roots);
 
-        if (spec.steps > 0) {
-            frontier.ensure(frontier_size + nr, frontier_size, st);
-            up(frontier.p + frontier_size, h_sid);
-            frontier_size += nr;
-        } else {
-            evo_done[evo] = 1;
-            finished.push_back(evo);
+        if (!h_front.empty()) {
+            frontier.ensure(frontier_size + h_front.size(), frontier_size, st);
+            up(frontier.p + frontier_size, h_front);
+            frontier_size += static_cast<uint32_t>(h_front.size());
         }
-        return evo;
+        return ids;
     }
 
     void grow_states(uint64_t n) {
@@ -724,8 +772,14 @@ struct Engine::Impl {
         const uint64_t old_n = d.table_mask + 2;
         k_rehash<<<grid_for(old_n, 256), 256, 0, st>>>(tab_keys.p, tab_vals.p, d.table_off, d.table_mask, nd.table_off, nd.table_mask, err.p);
         check_launch();
-        d = nd;
-        HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + evo, &d, sizeof(DevEvo), cudaMemcpyHostToDevice, st));
+        d = nd;   // the caller uploads the changed h_evos entries
+    }
+
+    // Upload h_evos[lo, hi) (one copy for all the tables a level regrew).
+    void upload_evos(size_t lo, size_t hi) {
+        if (hi > lo)
+            HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + lo, &h_evos[lo], (hi - lo) * sizeof(DevEvo),
+                                           cudaMemcpyHostToDevice, st));
     }
 
     void read_results(const std::vector<uint32_t>& which, const RunOptions& opt,
@@ -1140,52 +1194,40 @@ struct Engine::Impl {
         A.flag_front = flag_front.p;
         // tables: room for every event of the level plus every class seen
         bool any_cap = false;
+        size_t grown_lo = nevo, grown_hi = 0;
         for (size_t e = 0; e < nevo; ++e) {
             if (evo_done[e] || h_first[e] == kNone) continue;
             if (h_evos[e].max_states) any_cap = true;
             const uint64_t lv = (h_last[e] >= h_first[e]) ? h_last[e] - h_first[e] : 0;
             const uint64_t need = h_classes[e] + lv + 1;
-            if (2 * need > h_evos[e].table_mask + 1) regrow_table(static_cast<uint32_t>(e), need);
+            if (2 * need > h_evos[e].table_mask + 1) {
+                regrow_table(static_cast<uint32_t>(e), need);
+                grown_lo = std::min(grown_lo, e);
+                grown_hi = e + 1;
+            }
         }
+        upload_evos(grown_lo, grown_hi);
 
         // ---- expand: events, produced edges, children's WL hashes, table inserts
         //
-        // A level that a state cap may cut is expanded in chunks of the frontier, in frontier
-        // (= canonical event) order, stopping after the chunk that holds the cut: every event
-        // after the cut is dropped anyway, so the result is identical and the dropped tail is
-        // never built. Dedup stays exact because a chunk's events are selected only after every
-        // earlier event has been inserted.
+        // An evolution whose state cap this level can reach is expanded in rounds over its
+        // frontier range, in frontier (= canonical event) order, until the built events hold its
+        // cut: every later event is dropped anyway, so the result is identical and the dropped
+        // tail is never built. The other evolutions of the level are expanded whole in the first
+        // round. Dedup stays exact because a round's events are selected only after every earlier
+        // event of the evolution has been inserted. Unbuilt events of the last evolution in
+        // frontier order are cut from the level; those of the others are voided (in-range ids,
+        // never kept).
         uint32_t F_eff = F;
         if (n_ev) {
             const uint32_t mne = std::max<uint32_t>(fmax_ne, 1), mno = std::max<uint32_t>(fmax_nocc, 1);
             const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane, fwd);
             const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp, fwd);
             LaunchShape sl = warp_shape(k_expand<true>, Ll, F);
-            LaunchShape sw = warp_shape(k_expand<false>, Lw, F);
-            // chunking applies to a level holding one evolution whose cap this level can reach
-            uint32_t only = kNone, n_in_level = 0;
-            for (size_t e = 0; e < nevo; ++e)
-                if (!evo_done[e] && h_first[e] != kNone) { only = static_cast<uint32_t>(e); ++n_in_level; }
-            uint64_t remaining = 0;
-            bool chunked = false;
-            if (n_in_level == 1 && h_evos[only].max_states) {
-                const uint64_t have = h_evos[only].quotient ? h_classes[only] : h_states_now(only);
-                remaining = h_evos[only].max_states > have ? h_evos[only].max_states - have : 0;
-                chunked = uint64_t(n_ev) > remaining && F >= 4096;
-            }
-            std::vector<uint32_t> h_item;
-            if (chunked) {
-                h_item.resize(NI + 1);
-                HGX_CUDA_CHECK(cudaMemcpyAsync(h_item.data(), item_ev.p, (NI + 1) * 4, cudaMemcpyDeviceToHost, st));
-                HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-            }
-            const uint32_t chunk = chunked ? std::max<uint32_t>(1024, (F + 31) / 32) : F;
-            uint64_t cum = 0;
-            uint32_t f0 = 0;
-            while (f0 < F) {
-                const uint32_t f1 = std::min<uint64_t>(F, uint64_t(f0) + chunk);
-                A.f_begin = f0;
-                A.f_end = f1;
+            LaunchShape sw = warp_shape(k_expand<false>, Lw, n_ev);   // work units: slices
+            auto expand = [&](uint32_t n_work) {
+                A.f_begin = 0;
+                A.f_end = n_work;
                 HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, 2 * sizeof(uint32_t), st));
                 tic();
                 k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
@@ -1193,30 +1235,147 @@ struct Engine::Impl {
                 toc(times.expand);
                 ++times.expand_launches;
                 tic();
+                slice_off.ensure(uint64_t(n_work) + 1, 0, st);
+                k_slice_counts<<<grid_for(n_work, 256), 256, 0, st>>>(A, n_work, slice_off.p);
+                check_launch();
+                scan(slice_off.p, slice_off.p, n_work);
+                A.soff = slice_off.p;
+                A.n_sw = n_work;
                 k_expand<false><<<sw.grid, sw.block, sw.smem, st>>>(ptrs(), A, Lw);
                 check_launch();
+                A.soff = nullptr;
                 toc(times.expand_warp);
-                const uint32_t t0 = chunked ? h_item[uint64_t(f0) * R] : 0u;
-                const uint32_t t1 = chunked ? h_item[uint64_t(f1) * R] : n_ev;
+            };
+            struct Capped {
+                uint32_t evo, lo, hi, built;
+                uint64_t remaining, got, ev_built;
+                bool open;
+            };
+            std::vector<Capped> capped;
+            uint64_t avoidable = 0;
+            for (size_t e = 0; e < nevo && any_cap; ++e) {
+                if (evo_done[e] || h_first[e] == kNone || !h_evos[e].max_states) continue;
+                const uint64_t have = h_evos[e].quotient ? h_classes[e] : h_states_now(e);
+                const uint64_t remaining = h_evos[e].max_states > have ? h_evos[e].max_states - have : 0;
+                const uint64_t lv = (h_last[e] >= h_first[e]) ? h_last[e] - h_first[e] : 0;
+                if (lv <= remaining) continue;
+                capped.push_back({static_cast<uint32_t>(e), 0, 0, 0, remaining, 0, 0, true});
+                avoidable += lv - remaining;
+            }
+            if (capped.empty() || avoidable < opt.chunk_min) {
+                A.frng = nullptr;
+                expand(F);
                 tic();
-                k_select<<<grid_for(t1 - t0, 256), 256, 0, st>>>(ptrs(), A, t0, t1);
+                k_select<<<grid_for(n_ev, 256), 256, 0, st>>>(ptrs(), A, 0, n_ev);
                 check_launch();
                 toc(times.select);
-                f0 = f1;
-                if (!chunked) break;
-                uint32_t cnt = t1 - t0;
-                if (h_evos[only].quotient) {
-                    HGX_CUDA_CHECK(cudaMemsetAsync(sync_buf.p, 0, 4, st));
-                    k_sum_flags<<<grid_for(t1 - t0, 256), 256, 0, st>>>(flag_new.p + t0, t1 - t0, sync_buf.p);
-                    check_launch();
-                    HGX_CUDA_CHECK(cudaMemcpyAsync(&cnt, sync_buf.p, 4, cudaMemcpyDeviceToHost, st));
-                    HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            } else {
+                std::vector<uint32_t> h_item(NI + 1), h_fr(2 * nevo);
+                HGX_CUDA_CHECK(cudaMemcpyAsync(h_item.data(), item_ev.p, (NI + 1) * 4, cudaMemcpyDeviceToHost, st));
+                HGX_CUDA_CHECK(cudaMemcpyAsync(h_fr.data(), evo_frange.p, 2 * nevo * 4, cudaMemcpyDeviceToHost, st));
+                HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+                auto fev = [&](uint32_t f) -> uint64_t { return h_item[uint64_t(f) * R]; };
+                std::vector<uint8_t> is_capped(nevo, 0);
+                for (Capped& c : capped) {
+                    c.lo = c.built = h_fr[2 * c.evo];
+                    c.hi = h_fr[2 * c.evo + 1];
+                    is_capped[c.evo] = 1;
                 }
-                cum += cnt;
-                if (cum > remaining) break;   // the cut event lies in the chunk just processed
+                // the frontier ranges of a round, merged where adjacent, uploaded as A.frng
+                std::vector<std::pair<uint32_t, uint32_t>> rng;
+                auto run_ranges = [&](bool select) -> uint32_t {
+                    std::sort(rng.begin(), rng.end());
+                    std::vector<uint32_t> lo, off(1, 0);
+                    for (const auto& r : rng) {
+                        if (r.first >= r.second) continue;
+                        if (!lo.empty() && lo.back() + (off.back() - off[off.size() - 2]) == r.first) {
+                            off.back() += r.second - r.first;
+                        } else {
+                            lo.push_back(r.first);
+                            off.push_back(off.back() + (r.second - r.first));
+                        }
+                    }
+                    rng.clear();
+                    const uint32_t n = static_cast<uint32_t>(lo.size()), total = off.back();
+                    if (!total) return 0;
+                    std::vector<uint32_t> buf(lo);
+                    buf.insert(buf.end(), off.begin(), off.end());
+                    frng.ensure(buf.size(), 0, st);
+                    HGX_CUDA_CHECK(cudaMemcpyAsync(frng.p, buf.data(), buf.size() * 4, cudaMemcpyHostToDevice, st));
+                    A.frng = frng.p;
+                    A.n_frng = n;
+                    if (select) {
+                        expand(total);
+                        tic();
+                        k_select_list<<<grid_for(uint64_t(total) * 32, 256), 256, 0, st>>>(ptrs(), A, total, evo_new.p);
+                        check_launch();
+                        toc(times.select);
+                    }
+                    return total;
+                };
+                evo_new.ensure(nevo, 0, st);
+                std::vector<unsigned long long> h_new(nevo);
+                for (size_t e = 0; e < nevo; ++e)
+                    if (!evo_done[e] && h_first[e] != kNone && !is_capped[e])
+                        rng.emplace_back(h_fr[2 * e], h_fr[2 * e + 1]);
+                for (int round = 0;; ++round) {
+                    std::vector<uint32_t> target(capped.size());
+                    for (size_t i = 0; i < capped.size(); ++i) {
+                        Capped& c = capped[i];
+                        if (!c.open) continue;
+                        // events to add: the new states still needed for the cut, scaled by the
+                        // fraction of new classes seen so far (quotient mode), plus a margin
+                        const uint64_t need = c.remaining + 1 - c.got;
+                        uint64_t want = need;
+                        if (h_evos[c.evo].quotient && c.ev_built) {
+                            want = c.got ? need * c.ev_built / c.got : c.ev_built;
+                            want += want / 4 + 32;
+                        }
+                        if (round >= 12) want = UINT64_MAX;
+                        const uint64_t goal = fev(c.built) + std::min<uint64_t>(want, UINT64_MAX / 2);
+                        uint32_t a = c.built + 1, b = c.hi;   // first p in [a, b] with fev(p) >= goal
+                        while (a < b) {
+                            const uint32_t m = a + (b - a) / 2;
+                            if (fev(m) >= goal) b = m; else a = m + 1;
+                        }
+                        target[i] = a;
+                        rng.emplace_back(c.built, a);
+                    }
+                    HGX_CUDA_CHECK(cudaMemsetAsync(evo_new.p, 0, nevo * 8, st));
+                    run_ranges(true);
+                    HGX_CUDA_CHECK(cudaMemcpyAsync(h_new.data(), evo_new.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+                    HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+                    bool any_open = false;
+                    for (size_t i = 0; i < capped.size(); ++i) {
+                        Capped& c = capped[i];
+                        if (!c.open) continue;
+                        const uint64_t built = fev(target[i]) - fev(c.built);
+                        c.got += h_evos[c.evo].quotient ? h_new[c.evo] : built;
+                        c.ev_built += built;
+                        c.built = target[i];
+                        c.open = c.got <= c.remaining && c.built < c.hi;
+                        any_open |= c.open;
+                    }
+                    if (!any_open) break;
+                }
+                for (const Capped& c : capped) {
+                    if (c.built == c.hi) continue;
+                    if (c.hi == F) F_eff = c.built;   // the level ends at the last built state
+                    else rng.emplace_back(c.built, c.hi);
+                }
+                if (const uint32_t n_void = run_ranges(false)) {
+                    k_void<<<grid_for(uint64_t(n_void) * 32, 256), 256, 0, st>>>(ptrs(), A, n_void);
+                    check_launch();
+                }
+                A.frng = nullptr;
+                A.n_frng = 0;
             }
-            F_eff = f0;
-            const uint32_t n_ev_eff = chunked ? h_item[uint64_t(F_eff) * R] : n_ev;
+            const uint32_t n_ev_eff = F_eff == F ? n_ev : [&] {
+                uint32_t v = 0;
+                HGX_CUDA_CHECK(cudaMemcpyAsync(&v, item_ev.p + uint64_t(F_eff) * R, 4, cudaMemcpyDeviceToHost, st));
+                HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+                return v;
+            }();
             A.n_events = n_ev_eff;
             if (n_ev_eff) {
                 k_cprod<<<grid_for(n_ev_eff, 256), 256, 0, st>>>(ptrs(), A.ev_base, n_ev_eff);
@@ -1496,8 +1655,9 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
     Impl& I = *impl_;
     HGX_CUDA_CHECK(cudaSetDevice(I.device));
     I.reset();
-    std::vector<uint32_t> ids;
-    for (const auto& s : specs) ids.push_back(I.admit(s));
+    std::vector<const EvolutionSpec*> ptrs;
+    for (const auto& s : specs) ptrs.push_back(&s);
+    const std::vector<uint32_t> ids = I.admit_many(ptrs);
     while (I.level(opt)) {}
     std::vector<EvolutionResult> out;
     if (!opt.readback) I.read_counts(ids, out);
@@ -1509,6 +1669,11 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
 
 void Engine::reset() { impl_->reset(); }
 uint32_t Engine::admit(const EvolutionSpec& spec) { return impl_->admit(spec); }
+std::vector<uint32_t> Engine::admit(const std::vector<EvolutionSpec>& specs) {
+    std::vector<const EvolutionSpec*> ptrs;
+    for (const auto& s : specs) ptrs.push_back(&s);
+    return impl_->admit_many(ptrs);
+}
 bool Engine::step(const RunOptions& opt) { return impl_->level(opt); }
 std::vector<uint32_t> Engine::take_finished() {
     std::vector<uint32_t> f;

@@ -88,6 +88,9 @@ struct RunOptions {
     // Match forwarding: 0 = re-join every state, 1 = forward wherever it applies, 2 = forward
     // for states of 48 edges or more (results are identical in every mode).
     uint32_t forwarding = 0;
+    // A level whose state caps leave at least this many events unneeded is expanded in rounds
+    // that stop at each evolution's cut (results are identical either way).
+    uint64_t chunk_min = 8192;
 };
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.
@@ -122,6 +125,7 @@ public:
     // Continuous-batching interface.
     void reset();                                   // drop everything, keep allocations
     uint32_t admit(const EvolutionSpec& spec);      // returns the evolution id (engine-wide)
+    std::vector<uint32_t> admit(const std::vector<EvolutionSpec>& specs);   // all or none
     bool step(const RunOptions& opt = {});          // one level for every active evolution
     std::vector<uint32_t> take_finished();          // evolutions that completed since last call
     EvolutionResult collect(uint32_t evo, const RunOptions& opt = {});

@@ -276,7 +276,8 @@ __device__ void compute_cands(const Layout& L, char* sm, const DevRule& R, uint3
 // that state position (a seeded join: every emitted match uses it there).
 template <class F>
 __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Parent& pa,
-                          const uint8_t* sched, int seed, F&& on_match) {
+                          const uint8_t* sched, int seed, F&& on_match,
+                          uint32_t limit = 0xFFFFFFFFu) {
     const uint32_t lane = lane_id();
     const uint32_t n = R.n_lhs;
     const uint32_t nw = (pa.ne + 31) >> 5;
@@ -344,6 +345,7 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
             __syncwarp();
             if (lane == 0) taken[pick >> 5] &= ~(1u << (pick & 31));
             __syncwarp();
+            if (--limit == 0) break;   // the caller needs no later match
         } else {
             mask = nm;
             ++d;
@@ -798,9 +800,10 @@ __device__ void fwd_emit(const Layout& L, char* sm, const DevRule& R, const uint
 // Every match of the staged state in canonical order: the full join, or forwarding.
 template <class F>
 __device__ void enumerate_matches(const DevPtrs& P, const Layout& L, char* sm, const DevRule& R,
-                                  const Parent& pa, const Fwd& f, F&& on_match) {
+                                  const Parent& pa, const Fwd& f, F&& on_match,
+                                  uint32_t limit = 0xFFFFFFFFu) {
     if (!f.on) {
-        warp_join(L, sm, R, pa, R.sched, -1, on_match);
+        warp_join(L, sm, R, pa, R.sched, -1, on_match, limit);
         return;
     }
     const uint32_t lane = lane_id();
@@ -990,6 +993,40 @@ __global__ void k_item_sizes(DevPtrs P, LevelArgs A) {
     }
 }
 
+// Frontier position of work index w (identity unless the level runs over a list of ranges).
+__device__ __forceinline__ uint32_t frontier_at(const LevelArgs& A, uint32_t w) {
+    if (!A.frng) return w;
+    const uint32_t* off = A.frng + A.n_frng;
+    uint32_t a = 0, b = A.n_frng;   // off[a] <= w < off[b]
+    while (b - a > 1) {
+        const uint32_t m = (a + b) >> 1;
+        if (off[m] <= w) a = m; else b = m;
+    }
+    return A.frng[a] + (w - off[a]);
+}
+
+// Children per slice of a parent hashed warp-per-child: the smallest power of two >= 4 and
+// >= sqrt(children), so a parent with many children is spread over about sqrt(children) warps
+// while each warp re-enumerates at most its slice's end of the parent's matches.
+__device__ __forceinline__ uint32_t slice_size(uint32_t children) {
+    uint32_t s = 4;
+    while (uint64_t(s) * s < children) s <<= 1;
+    return s;
+}
+
+__device__ __forceinline__ uint32_t children_of(const LevelArgs& A, uint32_t f) {
+    return A.item_ev[(f + 1) * A.rules_stride] - A.item_ev[f * A.rules_stride];
+}
+
+// Slice counts of the work indices [f_begin, f_begin + n) for the warp-per-child kernel.
+__global__ void k_slice_counts(LevelArgs A, uint32_t n, uint32_t* cnt) {
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < n; w += gridDim.x * blockDim.x) {
+        const uint32_t f = frontier_at(A, A.f_begin + w);
+        const uint32_t c = children_of(A, f);
+        cnt[w] = ((A.fmode[f] & 1u) || !c) ? 0u : (c + slice_size(c) - 1) / slice_size(c);
+    }
+}
+
 // Enumerate again; mint events, produced edges and fresh vertices at the scanned offsets;
 // hash every child; insert the hash into the dedup table. Two instantiations over the same
 // frontier range: kLane hashes the children of the states flagged by k_count one per lane,
@@ -1007,22 +1044,40 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
     uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
     uint32_t* work = &A.work[kLane ? 1 : 2];
     while (true) {
-        uint32_t f = 0;
-        if (lane == 0) f = A.f_begin + atomicAdd(work, 1u);
-        f = __shfl_sync(0xFFFFFFFFu, f, 0);
-        if (f >= A.f_end) break;
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(work, 1u);
+        u = __shfl_sync(0xFFFFFFFFu, u, 0);
+        // the parent's children [c_lo, c_hi) (in its child order over all rules) built by this unit
+        uint32_t f, c_lo = 0, c_hi = 0xFFFFFFFFu;
+        if (kLane || !A.soff) {
+            if (u >= A.f_end - A.f_begin) break;
+            f = frontier_at(A, A.f_begin + u);
+        } else {
+            if (u >= A.soff[A.n_sw]) break;
+            uint32_t a = 0, b = A.n_sw;   // the work index whose slices hold u
+            while (b - a > 1) {
+                const uint32_t m = (a + b) >> 1;
+                if (A.soff[m] <= u) a = m; else b = m;
+            }
+            f = frontier_at(A, A.f_begin + a);
+            const uint32_t S = slice_size(children_of(A, f));
+            c_lo = (u - A.soff[a]) * S;
+            c_hi = c_lo + S;
+        }
         const uint8_t fm = A.fmode[f];
         if (((fm & 1u) != 0) != kLane) continue;
         const uint32_t sid = A.frontier[f];
         const Parent pa = load_parent(P, L, sm, sid);
         const uint32_t evo = P.st_evo[sid];
         const DevEvo ev = P.evos[evo];
-        if (lane == 0) b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
+        if (lane == 0 && c_lo == 0) b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
         if (kLane) build_parent_csr(L, sm, pa);
         for (uint32_t r = 0; r < A.rules_stride && r < ev.rule_count; ++r) {
             const uint32_t item = f * A.rules_stride + r;
-            if (lane == 0) b_stage += 4ull * pa.ne + 4ull * pa.nocc;   // join: ids and vertices
-            if (A.counts[item] == 0) continue;
+            if (lane == 0 && c_lo == 0) b_stage += 4ull * pa.ne + 4ull * pa.nocc;   // join: ids and vertices
+            const uint32_t rn = A.counts[item];
+            const uint32_t rb = A.item_ev[item] - A.item_ev[f * A.rules_stride];
+            if (rn == 0 || rb + rn <= c_lo || rb >= c_hi) continue;
             load_rule(sm, L, &P.rules[ev.rule_begin + r]);
             const uint32_t ev0 = A.ev_base + A.item_ev[item];
             const uint32_t cons0 = A.cons_base + A.item_cons[item];
@@ -1082,17 +1137,22 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                 });
                 if (nb) flush();
             } else {
+                // this rule's children inside the unit's slice: [lo, hi) of its match order
+                const uint32_t lo = c_lo > rb ? c_lo - rb : 0u;
+                const uint32_t hi = min(rn, c_hi - rb);
                 uint32_t idx = 0;
                 uint8_t rpos[kMaxPatternEdges];
                 enumerate_matches(P, L, sm, R, pa, fwd, [&](uint32_t nm) {
-                    for (uint32_t k = 0; k < R.n_lhs; ++k) rpos[k] = static_cast<uint8_t>(match[k]);
-                    const uint32_t nec = build_child(L, sm, R, pa, nm);
-                    WlInfo info;
-                    const uint64_t h = warp_wl(L, sm, nec, pa.nvp + R.n_fresh, info);
-                    if (lane == 0) finish(idx, h, info, rpos);
-                    __syncwarp();
+                    if (idx >= lo && idx < hi) {
+                        for (uint32_t k = 0; k < R.n_lhs; ++k) rpos[k] = static_cast<uint8_t>(match[k]);
+                        const uint32_t nec = build_child(L, sm, R, pa, nm);
+                        WlInfo info;
+                        const uint64_t h = warp_wl(L, sm, nec, pa.nvp + R.n_fresh, info);
+                        if (lane == 0) finish(idx, h, info, rpos);
+                        __syncwarp();
+                    }
                     ++idx;
-                });
+                }, hi);
             }
         }
     }
@@ -1361,13 +1421,63 @@ __global__ void k_select(DevPtrs P, LevelArgs A, uint32_t t_begin, uint32_t t_en
     }
 }
 
-// Sum of flags[0, n) into *out.
-__global__ void k_sum_flags(const uint32_t* flags, uint32_t n, uint32_t* out) {
-    uint32_t c = 0;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        c += flags[t];
-    c = warp_sum32(c);
-    if (lane_id() == 0 && c) atomicAdd(out, c);
+// k_select over the events of the frontier ranges in A.frng (a warp per state); the new classes
+// found are added to evo_new[evolution].
+__global__ void k_select_list(DevPtrs P, LevelArgs A, uint32_t n, unsigned long long* evo_new) {
+    const uint32_t lane = lane_id();
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+         i += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t f = frontier_at(A, i);
+        const uint32_t lo = A.item_ev[f * A.rules_stride], hi = A.item_ev[(f + 1) * A.rules_stride];
+        const uint32_t evo = P.st_evo[A.frontier[f]];
+        const DevEvo ev = P.evos[evo];
+        uint32_t c = 0;
+        for (uint32_t t = lo + lane; t < hi; t += 32) {
+            const uint32_t e = A.ev_base + t;
+            const uint32_t w = table_lookup(P, ev, P.ev_hash[e]);
+            P.ev_out[e] = w;
+            A.flag_new[t] = (w == e) ? 1u : 0u;
+            c += (w == e) ? 1u : 0u;
+        }
+        c = warp_sum32(c);
+        if (lane == 0 && c) atomicAdd(&evo_new[evo], static_cast<unsigned long long>(c));
+    }
+}
+
+// Events of frontier states that a capped level never built (they all come after the
+// evolution's cut): give them in-range ids so the per-event kernels see ordinary events that the
+// cap dropped (k_rep marks them not kept).
+__global__ void k_void(DevPtrs P, LevelArgs A, uint32_t n) {
+    const uint32_t lane = lane_id();
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
+         i += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t f = frontier_at(A, i);
+        const uint32_t sid = A.frontier[f];
+        const DevEvo ev = P.evos[P.st_evo[sid]];
+        for (uint32_t r = 0; r < A.rules_stride && r < ev.rule_count; ++r) {
+            const uint32_t item = f * A.rules_stride + r;
+            const uint32_t lo = A.item_ev[item], cnt = A.item_ev[item + 1] - lo;
+            if (!cnt) continue;
+            const DevRule& R = P.rules[ev.rule_begin + r];
+            const uint32_t cons0 = A.cons_base + A.item_cons[item];
+            const uint32_t prod0 = A.prod_base + A.item_prod[item];
+            const uint32_t fresh0 = A.fresh_base + A.item_fresh[item];
+            for (uint32_t idx = lane; idx < cnt; idx += 32) {
+                const uint32_t e = A.ev_base + lo + idx;
+                const uint32_t coff = cons0 + idx * R.n_lhs, pid = prod0 + idx * R.n_rhs;
+                P.ev_in[e] = sid;
+                P.ev_rule[e] = ev.rule_begin + r;
+                P.ev_coff[e] = coff;
+                P.ev_prod[e] = pid;
+                P.ev_fresh[e] = fresh0 + idx * R.n_fresh;
+                P.ev_hash[e] = 0;
+                P.ev_out[e] = kNone;
+                for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = 0;   // edge 0 exists
+                for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
+                A.flag_new[lo + idx] = 0;
+            }
+        }
+    }
 }
 
 // State cap: the first event of an evolution that would take it past max_states cuts the level

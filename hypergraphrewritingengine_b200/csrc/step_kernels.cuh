@@ -81,6 +81,14 @@ struct LevelArgs {
     uint32_t ev_base, cons_base, prod_base, fresh_base;   // level bases
     uint32_t n_events;          // events minted this level
     uint32_t f_begin, f_end;    // frontier range the expand kernel works on
+    // if set: work index w in [f_begin, f_end) is a position inside n_frng frontier ranges,
+    // frng[0, n) = first positions, frng[n, 2n+1) = exclusive prefix of the range lengths
+    const uint32_t* frng;
+    uint32_t n_frng;
+    // warp-per-child kernel: exclusive scan over the n_sw work indices of their parents' slice
+    // counts (soff[n_sw] = total); a slice is a run of slice_size(children) consecutive children
+    const uint32_t* soff;
+    uint32_t n_sw;
     uint8_t* fmode;             // [F] bit 0: children hashed lane-per-child; bit 1: forwarding
     uint32_t fwd_mode;          // 0 off, 1 every eligible state, 2 states with >= 48 edges
     uint32_t* work;             // work-queue counters

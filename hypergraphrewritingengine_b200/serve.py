@@ -65,7 +65,7 @@ class Server:
         pending = collections.deque(range(len(arrivals)))
         active = {}            # engine evolution id -> request index
         reserved = 0           # estimated bytes of the admitted requests
-        keep = {}              # job blobs must outlive admission
+        keep = {}              # job arrays of the admitted requests
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
 
@@ -79,27 +79,30 @@ class Server:
                 keep.pop(i, None)
 
         while pending or active:
-            # admission: arrived requests that fit the memory budget
-            admitted = 0
-            while pending and len(active) < self.max_active:
+            # admission: arrived requests that fit the memory budget, admitted in one call
+            take = []
+            while pending and len(active) + len(take) < self.max_active:
                 i = pending[0]
                 t_arr, ev = arrivals[i]
                 if realtime and t_arr > now():
                     break
-                if not realtime and admit_per_step is not None and admitted >= admit_per_step:
+                if not realtime and admit_per_step is not None and len(take) >= admit_per_step:
                     break
                 est = estimate_bytes(ev)
-                if active and reserved + est > self.budget:
+                if (active or take) and reserved + est > self.budget:
                     break
                 pending.popleft()
-                jobs, blobs = api.Engine.make_jobs([ev])
-                keep[i] = (jobs, blobs)
-                evo = eng.serve_admit(jobs[0])
-                active[evo] = i
-                recs[i].admitted = now()
+                take.append(i)
                 recs[i].meta["est"] = est
                 reserved += est
-                admitted += 1
+            if take:
+                jobs, blobs = api.Engine.make_jobs([arrivals[i][1] for i in take])
+                ids = eng.serve_admit_batch(jobs, len(take))
+                t_adm = now()
+                for i, evo in zip(take, ids):
+                    active[evo] = i
+                    recs[i].admitted = t_adm
+                    keep[i] = (jobs, blobs)
             collect_finished()                 # zero-step requests finish at admission
             if not active:
                 if not pending:

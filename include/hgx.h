@@ -73,7 +73,12 @@ typedef enum hgx_option {
        consumed edges plus the matches through the produced edges, instead of a full re-join.
        0 (default) = off, 1 = wherever it applies, 2 = states of 48 edges or more. Results are
        identical in every mode. */
-    HGX_OPT_FORWARDING = 8
+    HGX_OPT_FORWARDING = 8,
+    /* A level whose state caps (HGX_OPT_MAX_STATES / hgx_job.max_states) leave at least this many
+       of its events past every cut is built in rounds that stop at each evolution's cut, so the
+       dropped events are never built (default 8192; 0 = whenever a cap can cut). No reference
+       counterpart; results are identical for every value. */
+    HGX_OPT_CHUNK_MIN = 9
 } hgx_option;
 
 /* One evolution of a batch or a served request. */
@@ -155,6 +160,10 @@ HGX_API hgx_status hgx_evolve_batch(hgx_engine* engine, const hgx_job* jobs, uin
    advance together, each at its own depth. */
 HGX_API hgx_status hgx_serve_reset(hgx_engine* engine);
 HGX_API hgx_status hgx_serve_admit(hgx_engine* engine, const hgx_job* job, uint32_t* evolution_id);
+/* Admit n jobs at once (one upload per array and one root-hashing launch for all of them);
+   ids[i] receives job i's evolution id. Either every job is admitted or none is. */
+HGX_API hgx_status hgx_serve_admit_batch(hgx_engine* engine, const hgx_job* jobs, uint32_t n,
+                                         uint32_t* evolution_ids);
 HGX_API hgx_status hgx_serve_step(hgx_engine* engine, int* still_active);
 HGX_API hgx_status hgx_serve_take_finished(hgx_engine* engine, uint32_t* ids, uint32_t cap, uint32_t* n);
 HGX_API hgx_status hgx_serve_collect(hgx_engine* engine, uint32_t evolution_id, hgx_result** out);

@@ -155,4 +155,31 @@ def test_forwarding_modes_match_oracle(engine, mode):
             ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
             assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} forwarding={mode}")
     finally:
-        engine.set_option(api.OPT_FORWARDING, 2)
+        engine.set_option(api.OPT_FORWARDING, 0)
+
+
+@pytest.mark.parametrize("chunk_min", [0, 100])
+def test_capped_rounds_match_oracle(engine, chunk_min):
+    """Capped levels built in rounds that stop at each evolution's cut (forced on small cases):
+    batches whose evolutions hit their caps in the same level, and single evolutions."""
+    from hypergraphrewritingengine_b200 import api
+    engine.set_option(api.OPT_CHUNK_MIN, chunk_min)
+    try:
+        evs = W.config4(n=48, max_states=256)
+        evs += [W.Evolution(rules=[cases.C1_RULE], roots=[cases.C1_INIT], steps=5, quotient=False,
+                            max_states=cap) for cap in (40, 333)]
+        evs += [W.Evolution(rules=[cases.C2_RULE], roots=[cases.C2_INIT], steps=6, quotient=True,
+                            max_states=cap) for cap in (1, 7, 100, 1000)]
+        for ev, res in zip(evs, engine.evolve_batch(evs)):
+            ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient,
+                                  max_states=ev.max_states)
+            assert res.truncated == ref["truncated"], ev.name
+            assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} chunk_min={chunk_min}")
+        for ev in evs[-6:]:
+            res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient,
+                                max_states=ev.max_states)
+            ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient,
+                                  max_states=ev.max_states)
+            assert_same(norm_gpu(res), norm_oracle(ref), f"single {ev.name}")
+    finally:
+        engine.set_option(api.OPT_CHUNK_MIN, 8192)
