@@ -527,8 +527,7 @@ class ParallelEvolutionEngine:
         self._quotient = bool(enable)
 
     def set_transitive_reduction(self, enable: bool):
-        if enable:
-            raise NotImplementedError("transitive reduction is not implemented on this path")
+        self._engine.set_option(OPT_TRANSITIVE_REDUCTION, bool(enable))
 
     def set_max_states(self, n: int):
         self._max_states = int(n)

@@ -216,9 +216,7 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
     switch (opt) {
         case HGX_OPT_QUOTIENT: e->quotient = value != 0; return HGX_OK;
         case HGX_OPT_MAX_STATES: e->max_states = value; return HGX_OK;
-        case HGX_OPT_TRANSITIVE_REDUCTION:
-            if (value) return fail(HGX_ERR_INVALID, "transitive reduction is not implemented on this path");
-            return HGX_OK;
+        case HGX_OPT_TRANSITIVE_REDUCTION: e->opt.transitive_reduction = value != 0; return HGX_OK;
         case HGX_OPT_RECORD_CAUSAL: e->opt.causal = value != 0; return HGX_OK;
         case HGX_OPT_RECORD_BRANCHIAL: e->opt.branchial = value != 0; return HGX_OK;
         case HGX_OPT_KEEP_STATE_EDGES: e->opt.keep_state_edges = value != 0; return HGX_OK;

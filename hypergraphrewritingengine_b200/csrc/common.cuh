@@ -84,6 +84,7 @@ enum ErrorBits : uint32_t {
     kErrStateTooLarge = 1u << 1,
     kErrArenaFull = 1u << 2,
     kErrBadRule = 1u << 3,
+    kErrTrDepth = 1u << 4,       // transitive reduction past 64 levels
 };
 
 }  // namespace hgx

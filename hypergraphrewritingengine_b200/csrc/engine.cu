@@ -284,7 +284,7 @@ struct Engine::Impl {
     DVec<unsigned long long> stats, totals;
     DVec<uint8_t> fmode, fin;
     DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e, frng, slice_off;
-    DVec<unsigned long long> evo_new;
+    DVec<unsigned long long> evo_new, ev_anc;
     DVec<uint64_t> fin_rng;
     // Per evolution: the contiguous id ranges it owns, one entry per level (roots first).
     struct EvoRanges {
@@ -363,6 +363,7 @@ struct Engine::Impl {
         frng.release(st);
         slice_off.release(st);
         evo_new.release(st);
+        ev_anc.release(st);
         lvl_ranges.release(st);
         fin_ids.release(st);
         map_s.release(st);
@@ -427,6 +428,7 @@ struct Engine::Impl {
         P.ev_hash = ev_hash.p;
         P.ev_cons = ev_cons.p;
         P.ev_cprod = ev_cprod.p;
+        P.ev_anc = ev_anc.p;
         P.state_of_arrival = state_of_arrival.p;
         P.tab_keys = tab_keys.p;
         P.tab_vals = tab_vals.p;
@@ -1380,6 +1382,11 @@ struct Engine::Impl {
             if (n_ev_eff) {
                 k_cprod<<<grid_for(n_ev_eff, 256), 256, 0, st>>>(ptrs(), A.ev_base, n_ev_eff);
                 check_launch();
+                if (opt.transitive_reduction) {
+                    ev_anc.ensure(uint64_t(n_events) + n_ev_eff, n_events, st);
+                    k_tr<<<grid_for(n_ev_eff, 256), 256, 0, st>>>(ptrs(), A.ev_base, n_ev_eff);
+                    check_launch();
+                }
             }
 
             // ---- cap / representatives over the events actually built
@@ -1434,6 +1441,8 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + F_eff, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[3], err.p, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (s2[3] & kErrTrDepth)
+            throw std::invalid_argument("transitive reduction supports evolutions of at most 64 levels");
         if (s2[3]) throw std::runtime_error("hgx: device error flags 0x" + std::to_string(s2[3]));
         const uint32_t n_new = s2[0], n_front = s2[1], n_b = s2[2];
         for (size_t e = 0; e < nevo; ++e) {

@@ -91,6 +91,8 @@ struct RunOptions {
     // A level whose state caps leave at least this many events unneeded is expanded in rounds
     // that stop at each evolution's cut (results are identical either way).
     uint64_t chunk_min = 8192;
+    // Transitive reduction of the causal graph (evolutions of at most 64 levels).
+    bool transitive_reduction = false;
 };
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.

@@ -1179,6 +1179,50 @@ __global__ void k_cprod(DevPtrs P, uint32_t ev_base, uint32_t n) {
     }
 }
 
+// Transitive reduction of the causal relation, one level at a time (after k_cprod).
+//
+// Every producer of an edge consumed by event c created an edge of c's input state, so it lies on
+// that state's history chain (root -> ... -> input state, one creating event per level), and so
+// do all of its own causal ancestors. An event's causal ancestors are therefore identified by
+// their levels: anc(c) = OR over c's producers q of (bit level(q) | anc(q)). A pair (p, c) is
+// implied by a longer path exactly when another producer q of c has p among its ancestors
+// (bit level(p) in anc(q)); such consumed positions get producer kNone, which removes their
+// triples from every causal output. Reachability over the reduced pairs equals reachability over
+// all pairs, so anc stays exact for later levels. The result is the unique transitive reduction
+// of the stored (producer, consumer) relation that the reference computes
+// (common/include/hgcommon/transitive_reduction.hpp:36-94; kept triples: those whose pair
+// survives, hypergraph/include/hypergraph/causal_graph.hpp:295-305).
+__global__ void k_tr(DevPtrs P, uint32_t ev_base, uint32_t n) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t e = ev_base + t;
+        const uint32_t co = P.ev_coff[e], k = P.rules[P.ev_rule[e]].n_lhs;
+        uint32_t q[kMaxPatternEdges];
+        uint32_t lv[kMaxPatternEdges];
+        unsigned long long qa[kMaxPatternEdges];
+        unsigned long long anc = 0;
+        bool deep = false;
+        for (uint32_t i = 0; i < k; ++i) {
+            q[i] = P.ev_cprod[co + i];
+            lv[i] = 0;
+            qa[i] = 0;
+            if (q[i] == kNone) continue;
+            lv[i] = P.st_depth[P.ev_in[q[i]]];
+            deep |= lv[i] >= 64;
+            qa[i] = P.ev_anc[q[i]];
+            anc |= qa[i] | (1ull << (lv[i] & 63u));
+        }
+        P.ev_anc[e] = anc;
+        if (deep) { atomicOr(P.err, kErrTrDepth); continue; }
+        for (uint32_t i = 0; i < k; ++i) {
+            if (q[i] == kNone) continue;
+            bool implied = false;
+            for (uint32_t j = 0; j < k && !implied; ++j)
+                implied = q[j] != kNone && q[j] != q[i] && ((qa[j] >> lv[i]) & 1ull);
+            if (implied) P.ev_cprod[co + i] = kNone;
+        }
+    }
+}
+
 // Causal triples per evolution without reading the result back: kept events whose consumed
 // edges have a producer. out[evo] += count (warp-aggregated per evolution).
 __global__ void k_evo_causal(DevPtrs P, uint32_t n_events, unsigned long long* out) {

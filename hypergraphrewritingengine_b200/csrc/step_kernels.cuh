@@ -60,6 +60,9 @@ struct DevPtrs {
     uint32_t* evo_cut;                 // first event cut off by the cap this level (kNone = none)
     uint32_t* evo_first_ev;            // first event of the evolution in this level
     uint32_t* evo_stopped;
+    // transitive reduction: per event, bit d set = an event at level d is a proper causal
+    // ancestor (levels < 64; an event's ancestors lie on its input state's history chain)
+    unsigned long long* ev_anc;
     // errors
     uint32_t* err;
     // expand-kernel counters, [0..3] lane-per-child kernel, [4..7] warp-per-child kernel:

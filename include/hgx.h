@@ -55,7 +55,9 @@ typedef enum hgx_option {
     HGX_OPT_QUOTIENT = 0,
     /* set_max_states (parallel_evolution.hpp:764): 0 = unlimited. */
     HGX_OPT_MAX_STATES = 1,
-    /* set_transitive_reduction (parallel_evolution.hpp:781). Only 0 is accepted. */
+    /* set_transitive_reduction (parallel_evolution.hpp:781): 1 = the causal graph is reduced
+       transitively (a (producer, consumer) pair implied by a longer path is dropped with all its
+       triples), as hgcommon::tr_reduce. Evolutions of at most 64 levels; default 0. */
     HGX_OPT_TRANSITIVE_REDUCTION = 2,
     /* RecordSet::causal / ::branchial (common/include/hgcommon/core.hpp:128-155). */
     HGX_OPT_RECORD_CAUSAL = 3,

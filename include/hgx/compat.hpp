@@ -254,7 +254,7 @@ struct EvolveInput {
     std::vector<std::vector<VertexId>> initial_state;
     std::vector<std::vector<std::vector<VertexId>>> initial_states;   // takes precedence
     uint32_t num_steps = 0;
-    bool transitive_reduction = false;          // the reference defaults to true; not provided here
+    bool transitive_reduction = true;           // as the reference's default
     bool explore_from_canonical_states_only = true;
     bool edge_identity = true;                  // keep the state edge records
     uint64_t max_states = 0;

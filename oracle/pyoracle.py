@@ -146,6 +146,8 @@ def lib():
         L.oracle_copy.restype = None
         L.oracle_free.argtypes = [ctypes.c_void_p]
         L.oracle_free.restype = None
+        L.oracle_reduce_causal.argtypes = [ctypes.c_void_p]
+        L.oracle_reduce_causal.restype = None
         _lib = L
     return _lib
 
@@ -163,9 +165,9 @@ def wl_hash(edges) -> int:
     return int(lib().oracle_wl_hash(_ptr(b), len(b)))
 
 
-def evolve(rules, roots, steps, quotient=False, max_states=0):
+def evolve(rules, roots, steps, quotient=False, max_states=0, tr=False):
     """Run the restatement. Returns raw arrays (state_hash, state_depth, events, causal,
-    branchial) plus counts."""
+    branchial) plus counts. tr=True reduces the causal triples transitively."""
     L = lib()
     rb = encode_rules(rules)
     sb = encode_roots(roots)
@@ -174,6 +176,8 @@ def evolve(rules, roots, steps, quotient=False, max_states=0):
     if not h:
         raise ValueError("oracle rejected the rule or root encoding")
     try:
+        if tr:
+            L.oracle_reduce_causal(h)
         ns, ne, nc, nb = (int(L.oracle_count(h, i)) for i in range(4))
         classes = int(L.oracle_count(h, 4))
         truncated = bool(L.oracle_count(h, 5))
@@ -195,9 +199,10 @@ def evolve(rules, roots, steps, quotient=False, max_states=0):
 # The reference engine itself (oracle/_ref/hgref, built from the reference's own sources)
 # --------------------------------------------------------------------------------------------
 
-def spec_text(rules, roots, steps, quotient=False, threads=0, arrays=False):
+def spec_text(rules, roots, steps, quotient=False, threads=0, arrays=False, tr=False, evkeys=0):
     lines = [f"steps {int(steps)}", f"mode {'quotient' if quotient else 'full'}",
-             f"threads {int(threads)}", f"arrays {1 if arrays else 0}"]
+             f"threads {int(threads)}", f"arrays {1 if arrays else 0}", f"tr {1 if tr else 0}",
+             f"evkeys {int(evkeys)}"]
     for lhs, rhs in rules:
         parts = ["rule", str(len(lhs))]
         for e in lhs:
@@ -214,7 +219,8 @@ def spec_text(rules, roots, steps, quotient=False, threads=0, arrays=False):
     return "\n".join(lines) + "\n"
 
 
-def run_reference(rules, roots, steps, quotient=False, threads=0, arrays=False, timeout=None):
+def run_reference(rules, roots, steps, quotient=False, threads=0, arrays=False, timeout=None,
+                  tr=False, evkeys=0):
     """Run the compiled reference engine harness; returns its parsed JSON line."""
     import json
     import tempfile
@@ -222,7 +228,7 @@ def run_reference(rules, roots, steps, quotient=False, threads=0, arrays=False, 
     if not os.path.exists(REF_BIN):
         raise FileNotFoundError(REF_BIN)
     with tempfile.NamedTemporaryFile("w", suffix=".spec", delete=False) as f:
-        f.write(spec_text(rules, roots, steps, quotient, threads, arrays))
+        f.write(spec_text(rules, roots, steps, quotient, threads, arrays, tr, evkeys))
         path = f.name
     try:
         out = subprocess.run([REF_BIN, path], capture_output=True, text=True, check=True,

@@ -20,6 +20,10 @@
 //   rule <nl> (<a> v..)*nl <nr> (<a> v..)*nr      (repeatable)
 //   root <ne> (<a> v..)*ne                        (repeatable: several roots)
 //   arrays 0|1             1 = also print the full sorted key arrays
+//   tr 0|1                 transitive reduction of the causal graph (default 0)
+//   evkeys <bits>          event signature keys (hgcommon EventSignatureKeys; default 0 = none):
+//                          then "events" is the canonical event count and "signature_digest" the
+//                          digest of the sorted distinct signatures of the canonical events
 #include <hypergraph/hypergraph.hpp>
 #include <hypergraph/parallel_evolution.hpp>
 #include <hypergraph/pattern.hpp>
@@ -62,6 +66,8 @@ struct Spec {
     bool quotient = false;
     int threads = 0;
     bool arrays = false;
+    bool tr = false;
+    int evkeys = 0;
     std::vector<std::pair<std::vector<std::vector<uint8_t>>, std::vector<std::vector<uint8_t>>>> rules;
     std::vector<std::vector<std::vector<VertexId>>> roots;
 };
@@ -84,6 +90,8 @@ bool read_spec(const char* path, Spec& s) {
         else if (tok == "mode") { std::string m; in >> m; s.quotient = (m == "quotient"); }
         else if (tok == "threads") in >> s.threads;
         else if (tok == "arrays") { int a; in >> a; s.arrays = a != 0; }
+        else if (tok == "tr") { int a; in >> a; s.tr = a != 0; }
+        else if (tok == "evkeys") in >> s.evkeys;
         else if (tok == "rule") {
             std::vector<std::vector<uint8_t>> l, r;
             read_edges_u8(l);
@@ -129,7 +137,8 @@ int main(int argc, char** argv) {
     const auto mode = spec.threads == 0 ? ParallelEvolutionEngine::ExecutionMode::Serial
                                         : ParallelEvolutionEngine::ExecutionMode::Parallel;
     ParallelEvolutionEngine engine(&hg, static_cast<size_t>(spec.threads), mode);
-    engine.set_transitive_reduction(false);
+    hg.set_event_signature_keys(static_cast<hgcommon::EventSignatureKeys>(spec.evkeys));
+    engine.set_transitive_reduction(spec.tr);
     engine.set_explore_from_canonical_states_only(spec.quotient);
     for (size_t i = 0; i < spec.rules.size(); ++i) {
         RuleBuilder b(static_cast<uint16_t>(i));
@@ -158,9 +167,11 @@ int main(int argc, char** argv) {
         }
         std::unordered_map<uint32_t, uint64_t> key_of;
         std::vector<uint64_t> ekeys;
+        std::set<uint64_t> sigs;
         for (uint32_t e = 0; e < hg.num_published_events(); ++e) {
             const auto& ev = hg.get_event(e);
             if (ev.id == INVALID_ID) continue;
+            if (spec.evkeys && hg.get_canonical_event(e) == e) sigs.insert(ev.signature);
             const uint32_t step = hg.get_state(ev.output_state).step;
             const uint64_t k = event_key(hash_of[ev.input_state], hash_of[ev.output_state],
                                          ev.rule_index, step);
@@ -187,6 +198,11 @@ int main(int argc, char** argv) {
         std::printf(",\"event_digest\":%llu,\"causal_digest\":%llu,\"branchial_digest\":%llu",
                     (unsigned long long)digest(ekeys), (unsigned long long)digest(ckeys),
                     (unsigned long long)digest(bkeys));
+        if (spec.evkeys) {
+            std::vector<uint64_t> sv(sigs.begin(), sigs.end());
+            std::printf(",\"raw_events\":%u,\"signatures\":%zu,\"signature_digest\":%llu",
+                        hg.num_raw_events(), sv.size(), (unsigned long long)digest(sv));
+        }
         print_array("state_hashes", hs);
         if (spec.arrays) {
             print_array("event_keys", ekeys);

@@ -16,6 +16,8 @@
 #include "restate.hpp"
 
 #include <algorithm>
+#include <map>
+#include <set>
 #include <cstring>
 #include <functional>
 #include <numeric>
@@ -372,6 +374,40 @@ Result evolve(const std::vector<Rule>& rules,
     return res;
 }
 
+// Reachability restated directly: a pair (p, c) is implied when some other successor w of p
+// reaches c. For each producer p the set of nodes reachable from p's successors is gathered by a
+// depth-first walk over the unique-pair adjacency; a pair survives if c is not in that set.
+std::vector<uint32_t> reduce_causal(const std::vector<uint32_t>& triples) {
+    std::map<uint32_t, std::set<uint32_t>> succ;
+    for (size_t i = 0; i + 2 < triples.size(); i += 3) succ[triples[i]].insert(triples[i + 1]);
+    std::set<std::pair<uint32_t, uint32_t>> implied;
+    for (const auto& [p, targets] : succ) {
+        std::set<uint32_t> reach;          // reachable from p by a path of length >= 2
+        std::vector<uint32_t> todo;
+        for (uint32_t w : targets) {
+            auto it = succ.find(w);
+            if (it == succ.end()) continue;
+            for (uint32_t x : it->second)
+                if (reach.insert(x).second) todo.push_back(x);
+        }
+        while (!todo.empty()) {
+            const uint32_t x = todo.back();
+            todo.pop_back();
+            auto it = succ.find(x);
+            if (it == succ.end()) continue;
+            for (uint32_t y : it->second)
+                if (reach.insert(y).second) todo.push_back(y);
+        }
+        for (uint32_t c : targets)
+            if (reach.count(c)) implied.insert({p, c});
+    }
+    std::vector<uint32_t> out;
+    for (size_t i = 0; i + 2 < triples.size(); i += 3)
+        if (!implied.count({triples[i], triples[i + 1]}))
+            out.insert(out.end(), {triples[i], triples[i + 1], triples[i + 2]});
+    return out;
+}
+
 }  // namespace hgx_oracle
 
 // ---------------------------------------------------------------------------------------------
@@ -459,6 +495,12 @@ void* oracle_evolve(const uint32_t* rules, size_t rules_len, const uint32_t* roo
         h->event_out_hash.push_back(e.out_hash);
     }
     return h;
+}
+
+// Replace the handle's causal triples by their transitive reduction.
+void oracle_reduce_causal(void* hp) {
+    auto* h = static_cast<Handle*>(hp);
+    h->r.causal = hgx_oracle::reduce_causal(h->r.causal);
 }
 
 // what: 0 states, 1 events, 2 causal triples, 3 branchial pairs, 4 classes, 5 truncated

@@ -52,6 +52,13 @@ uint64_t wl_hash(const std::vector<std::vector<uint32_t>>& edges);
 Rule make_rule(const std::vector<std::vector<uint8_t>>& lhs,
                const std::vector<std::vector<uint8_t>>& rhs);
 
+// Transitive reduction of a causal triple list (producer, consumer, edge), flattened: keeps the
+// triples whose (producer, consumer) pair is not implied by a path of two or more pairs.
+// Restates the unique reduction of the stored relation, hgcommon::tr_reduce
+// (common/include/hgcommon/transitive_reduction.hpp:36-94), as read by
+// CausalGraph::for_each_causal_edge (hypergraph/include/hypergraph/causal_graph.hpp:295-305).
+std::vector<uint32_t> reduce_causal(const std::vector<uint32_t>& triples);
+
 Result evolve(const std::vector<Rule>& rules,
               const std::vector<std::vector<std::vector<uint32_t>>>& roots, uint32_t steps,
               bool quotient, uint64_t max_states);

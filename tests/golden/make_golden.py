@@ -15,6 +15,10 @@ where the reference's serial quotient exploration is complete (<= 5 on the named
 
 Also records the reference's own golden-matrix rows for the None/None/full-multiway mode
 (reference/golden_matrix.txt), read as text.
+
+The "tr" section re-runs the full-multiway cases with the causal graph's transitive reduction on
+(serial execution) and stores the reduced causal count and key digest. `python make_golden.py tr`
+recomputes only that section in the existing golden.json.
 """
 import json
 import os
@@ -30,7 +34,28 @@ import cases  # noqa: E402
 REF_MATRIX = "/root/reference/reference/golden_matrix.txt"
 
 
+def tr_section():
+    out = {}
+    for name, rules, roots, steps in cases.all_full_cases():
+        r = pyoracle.run_reference(rules, roots, steps, quotient=False, threads=0, arrays=True,
+                                   tr=True)
+        entry = {"steps": steps, "causal": r["causal"], "causal_digest": r["causal_digest"]}
+        if r["causal"] <= 1500:
+            entry["causal_keys"] = r["causal_keys"]
+        out[name] = entry
+        print("tr", name, r["causal"], f"{r['ms']:.0f}ms", flush=True)
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["tr"]:
+        path = os.path.join(HERE, "golden.json")
+        with open(path) as fh:
+            out = json.load(fh)
+        out["tr"] = tr_section()
+        with open(path, "w") as fh:
+            json.dump(out, fh, indent=0, sort_keys=True)
+        return
     out = {"full": {}, "quotient": {}, "matrix": {}}
     for name, rules, roots, steps in cases.all_full_cases():
         r = pyoracle.run_reference(rules, roots, steps, quotient=False, threads=8, arrays=True)
@@ -58,6 +83,7 @@ def main():
             if len(f) >= 11 and not line.startswith("#") and f[1:4] == ["None", "None", "0"]:
                 out["matrix"][f[0]] = {"steps": int(f[4]), "states": int(f[5]), "events": int(f[6]),
                                        "causal": int(f[7]), "pairs": int(f[8]), "branchial": int(f[9])}
+    out["tr"] = tr_section()
     with open(os.path.join(HERE, "golden.json"), "w") as fh:
         json.dump(out, fh, indent=0, sort_keys=True)
 

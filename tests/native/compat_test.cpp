@@ -19,6 +19,15 @@ int main() {
     bool ok = hg.num_states() == 22204 && hg.num_events() == 22203 && hg.num_canonical_states() == 20 &&
               cg.get_causal_edges().size() == 42816 && cg.get_branchial_edges().size() == 78045;
 
+    // the same evolution with the causal graph reduced transitively (reference: 31,188 triples)
+    Hypergraph hg2;
+    ParallelEvolutionEngine engine2(&hg2, 8);
+    engine2.add_rule(make_rule(0).lhs({0, 1}).lhs({1, 2}).rhs({0, 1}).rhs({1, 2}).rhs({2, 0}).build());
+    engine2.set_transitive_reduction(true);
+    engine2.evolve({{1, 2}, {2, 3}, {3, 1}}, 5);
+    std::printf("c1 reduced: causal %zu\n", hg2.causal_graph().get_causal_edges().size());
+    ok = ok && hg2.causal_graph().get_causal_edges().size() == 31188;
+
     hgx::compat::gpu::EvolveInput in;
     in.rules.push_back({{{0, 1}, {0, 2}}, {{0, 2}, {0, 3}, {1, 3}, {2, 3}}, 3, 4});
     in.initial_state = {{1, 1}, {1, 1}};

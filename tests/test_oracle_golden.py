@@ -29,6 +29,19 @@ def test_full_multiway_matches_reference(name, golden):
     assert_matches_golden(norm_oracle(r), golden["full"][name], name)
 
 
+@pytest.mark.parametrize("name", sorted(FULL))
+def test_transitive_reduction_matches_reference(name, golden):
+    """Causal graph with transitive reduction on (the reference's product default)."""
+    rules, roots, steps = FULL[name]
+    r = pyoracle.evolve(rules, roots, steps, quotient=False, tr=True)
+    n = norm_oracle(r)
+    g = golden["tr"][name]
+    assert n["causal"] == g["causal"], name
+    assert pyoracle.digest(n["causal_keys"]) == g["causal_digest"], name
+    if "causal_keys" in g:
+        assert np.array_equal(n["causal_keys"], np.array(g["causal_keys"], np.uint64)), name
+
+
 # WL classes the reference's IR-keyed quotient separates but the WL hash merges (a WL collision
 # at the deepest level). Events are unaffected: they come from the levels above.
 WL_COLLISIONS = {"c2-quot-5": 3, "c3-quot-5": 1}
