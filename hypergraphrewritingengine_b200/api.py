@@ -32,12 +32,17 @@ LIB_PATH = os.path.join(HERE, "libhgx.so")
 
 HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_ERR_INTERNAL = range(6)
 (OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
- OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING, OPT_CHUNK_MIN) = range(10)
+ OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING, OPT_CHUNK_MIN,
+ OPT_EVENT_SIGNATURE_KEYS) = range(11)
 (COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
- COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES) = range(10)
+ COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES,
+ COUNT_CANONICAL_EVENTS) = range(11)
 (ARR_STATE_HASH, ARR_STATE_DEPTH, ARR_EVENTS, ARR_CAUSAL, ARR_BRANCHIAL, ARR_EVENT_CONS_OFF,
  ARR_EVENT_CONS, ARR_EVENT_PROD, ARR_STATE_EDGE_OFF, ARR_STATE_EDGE_IDS, ARR_STATE_ARITY,
- ARR_STATE_VERT_OFF, ARR_STATE_VERTS) = range(13)
+ ARR_STATE_VERT_OFF, ARR_STATE_VERTS, ARR_EVENT_SIG) = range(14)
+# hgcommon EventSignatureKeys bits provided on this path; FULL is the reference's Full preset
+EVENT_KEY_INPUT, EVENT_KEY_OUTPUT, EVENT_KEY_STEP, EVENT_KEY_RULE = 1, 2, 4, 8
+EVENT_SIG_NONE, EVENT_SIG_FULL = 0, 3
 
 # Every symbol include/hgx.h declares (the library must export all of them).
 EXPORTS = (
@@ -178,6 +183,17 @@ class EvolveResult:
     state_verts: np.ndarray
     num_classes: int
     truncated: bool
+    event_signature: np.ndarray = None   # u64 per event (event canonicalisation on), else empty
+    num_canonical_events: int = 0        # distinct event signatures (= events when off)
+
+    def canonical_event(self) -> np.ndarray:
+        """Per event, the local id of the first event with its signature (itself when event
+        canonicalisation is off)."""
+        n = len(self.events)
+        if self.event_signature is None or len(self.event_signature) != n:
+            return np.arange(n, dtype=np.uint32)
+        _, first, inv = np.unique(self.event_signature, return_index=True, return_inverse=True)
+        return first[inv].astype(np.uint32)
 
     @property
     def num_states(self) -> int:
@@ -217,7 +233,7 @@ class _ResultOwner:
             pass
 
 
-_ARR_TYPES = {ARR_STATE_HASH: np.uint64}
+_ARR_TYPES = {ARR_STATE_HASH: np.uint64, ARR_EVENT_SIG: np.uint64}
 _ARR_SHAPES = {ARR_EVENTS: 4, ARR_CAUSAL: 3, ARR_BRANCHIAL: 2, ARR_EVENT_PROD: 2}
 
 
@@ -228,7 +244,7 @@ def _read_result(handle) -> EvolveResult:
     owner = _ResultOwner(handle)
     cnt = lambda w: int(L.hgx_result_count(handle, w))  # noqa: E731
     arrays = {}
-    for what in range(13):
+    for what in range(14):
         ptr = ctypes.c_void_p()
         n = ctypes.c_uint64()
         _check(L.hgx_result_view(handle, what, ctypes.byref(ptr), ctypes.byref(n)))
@@ -249,7 +265,8 @@ def _read_result(handle) -> EvolveResult:
         event_prod=arrays[ARR_EVENT_PROD], state_edge_off=arrays[ARR_STATE_EDGE_OFF],
         state_edge_ids=arrays[ARR_STATE_EDGE_IDS], state_arity=arrays[ARR_STATE_ARITY],
         state_vert_off=arrays[ARR_STATE_VERT_OFF], state_verts=arrays[ARR_STATE_VERTS],
-        num_classes=cnt(COUNT_CLASSES), truncated=bool(cnt(COUNT_TRUNCATED)))
+        num_classes=cnt(COUNT_CLASSES), truncated=bool(cnt(COUNT_TRUNCATED)),
+        event_signature=arrays[ARR_EVENT_SIG], num_canonical_events=cnt(COUNT_CANONICAL_EVENTS))
 
 
 class Engine:
@@ -381,7 +398,8 @@ class Engine:
                 cnt = lambda w: int(L.hgx_result_count(out, w))  # noqa: E731
                 return {"states": cnt(COUNT_STATES), "events": cnt(COUNT_EVENTS),
                         "classes": cnt(COUNT_CLASSES), "causal": cnt(COUNT_CAUSAL),
-                        "branchial": cnt(COUNT_BRANCHIAL), "truncated": bool(cnt(COUNT_TRUNCATED))}
+                        "branchial": cnt(COUNT_BRANCHIAL), "truncated": bool(cnt(COUNT_TRUNCATED)),
+                        "canonical_events": cnt(COUNT_CANONICAL_EVENTS)}
             finally:
                 L.hgx_result_free(out)
         finally:
@@ -487,6 +505,20 @@ class Hypergraph:
 
     def __init__(self):
         self.result: EvolveResult | None = None
+        self._event_keys = EVENT_SIG_NONE
+
+    def set_event_signature_keys(self, keys: int):
+        """Event canonicalisation (hypergraph.hpp:778): hgcommon EventSignatureKeys bits over the
+        WL hashes (1 input, 2 output, 4 step, 8 rule); read by the engine at evolve()."""
+        if int(keys) & ~0xF:
+            raise ValueError("edge-rank event keys need an exact canonical labelling (not provided)")
+        self._event_keys = int(keys)
+
+    def event_signature_keys(self) -> int:
+        return self._event_keys
+
+    def num_raw_events(self) -> int:
+        return 0 if self.result is None else self.result.num_events
 
     def num_states(self) -> int:
         """Raw states: every root plus one per event (hypergraph.hpp:567)."""
@@ -500,7 +532,13 @@ class Hypergraph:
         return 0 if self.result is None else int(self.result.num_classes)
 
     def num_events(self) -> int:
-        return 0 if self.result is None else self.result.num_events
+        """Canonical events when event canonicalisation is on (hypergraph.cpp:1639-1644)."""
+        if self.result is None:
+            return 0
+        return int(self.result.num_canonical_events) if self._event_keys else self.result.num_events
+
+    def get_canonical_event(self, eid: int) -> int:
+        return int(self.result.canonical_event()[eid])
 
     def get_or_compute_canonical_hash(self, sid: int) -> int:
         return int(self.result.state_hash[sid])
@@ -547,4 +585,5 @@ class ParallelEvolutionEngine:
             return
         roots = initial if initial and isinstance(initial[0][0], (list, tuple)) else [initial]
         rules = [(r.lhs, r.rhs) for r in sorted(self._rules, key=lambda r: r.index)]
+        self._engine.set_option(OPT_EVENT_SIGNATURE_KEYS, self._hg.event_signature_keys())
         self._hg.result = self._engine.evolve(rules, roots, steps, self._quotient, self._max_states)

@@ -21,8 +21,8 @@ struct hgx_result {
     hgx::EvolutionResult r;
     std::vector<uint32_t> events_flat;   // (in, out, rule, step) for vector-held results
     std::vector<uint32_t> prod_flat;     // (first, count)
-    const void* ptr[13] = {};            // every array, indexed by hgx_array
-    uint64_t count[13] = {};             // elements
+    const void* ptr[hgx::ResultArrays::kArrays] = {};   // every array, indexed by hgx_array
+    uint64_t count[hgx::ResultArrays::kArrays] = {};    // elements
 };
 
 namespace {
@@ -131,7 +131,7 @@ hgx_result* wrap(hgx::EvolutionResult&& r) {
     out->r = std::move(r);
     auto& x = out->r;
     if (x.flat) {
-        for (int i = 0; i < 13; ++i) {
+        for (int i = 0; i < hgx::ResultArrays::kArrays; ++i) {
             out->ptr[i] = x.flat->ptr[i];
             out->count[i] = x.flat->count[i];
         }
@@ -168,6 +168,7 @@ hgx_result* wrap(hgx::EvolutionResult&& r) {
     set(HGX_ARR_STATE_ARITY, x.state_arity);
     set(HGX_ARR_STATE_VERT_OFF, x.state_vert_off);
     set(HGX_ARR_STATE_VERTS, x.state_verts);
+    set(HGX_ARR_EVENT_SIG, x.ev_sig);
     return out;
 }
 
@@ -227,6 +228,13 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
             e->opt.forwarding = static_cast<uint32_t>(value);
             return HGX_OK;
         case HGX_OPT_CHUNK_MIN: e->opt.chunk_min = value; return HGX_OK;
+        case HGX_OPT_EVENT_SIGNATURE_KEYS:
+            if (value & ~uint64_t(0xF))
+                return fail(HGX_ERR_INVALID,
+                            "event signature keys: only input state (1), output state (2), step (4) "
+                            "and rule (8) are provided; edge-rank keys need an exact canonical labelling");
+            e->opt.event_keys = static_cast<uint32_t>(value);
+            return HGX_OK;
     }
     return fail(HGX_ERR_INVALID, "unknown option");
 }
@@ -333,6 +341,7 @@ uint64_t hgx_result_count(const hgx_result* res, hgx_count what) {
             case HGX_COUNT_CAUSAL: return r.n_causal;
             case HGX_COUNT_BRANCHIAL: return r.n_branchial;
             case HGX_COUNT_TRUNCATED: return r.truncated ? 1 : 0;
+            case HGX_COUNT_CANONICAL_EVENTS: return r.n_canonical_events;
             default: return 0;
         }
     }
@@ -347,14 +356,16 @@ uint64_t hgx_result_count(const hgx_result* res, hgx_count what) {
         case HGX_COUNT_STATE_EDGES: return res->count[HGX_ARR_STATE_EDGE_IDS];
         case HGX_COUNT_STATE_VERTS: return res->count[HGX_ARR_STATE_VERTS];
         case HGX_COUNT_RAW_STATES: return r.n_roots + res->count[HGX_ARR_EVENTS] / 4;
+        case HGX_COUNT_CANONICAL_EVENTS: return r.n_canonical_events;
     }
     return 0;
 }
 
 hgx_status hgx_result_copy(const hgx_result* res, hgx_array what, void* dst, size_t bytes) {
     if (!res || (!dst && bytes)) return fail(HGX_ERR_INVALID, "null argument");
-    if (static_cast<int>(what) < 0 || static_cast<int>(what) >= 13) return fail(HGX_ERR_INVALID, "unknown array");
-    const size_t need = res->count[what] * (what == HGX_ARR_STATE_HASH ? 8 : 4);
+    if (static_cast<int>(what) < 0 || static_cast<int>(what) >= hgx::ResultArrays::kArrays)
+        return fail(HGX_ERR_INVALID, "unknown array");
+    const size_t need = res->count[what] * ((what == HGX_ARR_STATE_HASH || what == HGX_ARR_EVENT_SIG) ? 8 : 4);
     if (bytes < need) return fail(HGX_ERR_INVALID, "hgx_result_copy: destination too small");
     if (need) std::memcpy(dst, res->ptr[what], need);
     return HGX_OK;
@@ -362,7 +373,8 @@ hgx_status hgx_result_copy(const hgx_result* res, hgx_array what, void* dst, siz
 
 hgx_status hgx_result_view(const hgx_result* res, hgx_array what, const void** ptr, uint64_t* count) {
     if (!res || !ptr || !count) return fail(HGX_ERR_INVALID, "null argument");
-    if (static_cast<int>(what) < 0 || static_cast<int>(what) >= 13) return fail(HGX_ERR_INVALID, "unknown array");
+    if (static_cast<int>(what) < 0 || static_cast<int>(what) >= hgx::ResultArrays::kArrays)
+        return fail(HGX_ERR_INVALID, "unknown array");
     *ptr = res->ptr[what];
     *count = res->count[what];
     return HGX_OK;

@@ -76,7 +76,26 @@ struct DevEvo {
     uint64_t table_off;      // slot offset of this evolution's dedup table
     uint64_t table_mask;     // capacity - 1 (power of two); slot mask+1 holds key 0
     uint64_t max_states;     // 0 = unlimited
+    uint64_t sig_off;        // event-signature table (event canonicalisation), same layout;
+    uint64_t sig_mask;       // sig_mask == 0: not allocated
 };
+
+// Event signature keys (hgcommon EventSignatureKeys bits, common/include/hgcommon/event_core.hpp:30-37)
+// that this path computes: the edge-rank keys (1 << 4, 1 << 5) need an exact canonical labelling.
+constexpr uint32_t kEvKeyInput = 1u << 0, kEvKeyOutput = 1u << 1, kEvKeyStep = 1u << 2,
+                   kEvKeyRule = 1u << 3, kEvKeysSupported = 0xFu;
+
+// Signature of one event from the selected keys, in the key order of hgcommon::event_signature
+// (common/include/hgcommon/event_core.hpp:64-84); 0 and the bare offset are reserved and map to 1.
+HGX_HD uint64_t event_signature(uint32_t keys, uint64_t in_hash, uint64_t out_hash,
+                                       uint32_t step, uint32_t rule) {
+    uint64_t sig = kFnvOffset;
+    if (keys & kEvKeyInput) sig = fnv(sig, in_hash);
+    if (keys & kEvKeyOutput) sig = fnv(sig, out_hash);
+    if (keys & kEvKeyStep) sig = fnv(sig, static_cast<uint64_t>(step));
+    if (keys & kEvKeyRule) sig = fnv(sig, static_cast<uint64_t>(rule));
+    return (sig == 0 || sig == kFnvOffset) ? 1 : sig;
+}
 
 // Device-side error channel (typed, host-visible; never a trap).
 enum ErrorBits : uint32_t {

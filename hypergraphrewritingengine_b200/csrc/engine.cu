@@ -50,6 +50,11 @@ struct DVec {
     size_t bytes() const { return cap * sizeof(T); }
 };
 
+// Bytes per element of result array i (the hashes and signatures are u64).
+inline uint64_t arr_elem_bytes(int i) {
+    return (i == HGX_ARR_STATE_HASH || i == HGX_ARR_EVENT_SIG) ? 8 : 4;
+}
+
 struct RuleMax {
     uint32_t rhs = 0, rhs_total = 0, fresh = 0, arity = 1, grow_e = 0, grow_o = 0, stride = 1,
              lhs = 1;
@@ -284,7 +289,7 @@ struct Engine::Impl {
     DVec<unsigned long long> stats, totals;
     DVec<uint8_t> fmode, fin;
     DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e, frng, slice_off;
-    DVec<unsigned long long> evo_new, ev_anc;
+    DVec<unsigned long long> evo_new, ev_anc, ev_sig, evo_sigs;
     DVec<uint64_t> fin_rng;
     // Per evolution: the contiguous id ranges it owns, one entry per level (roots first).
     struct EvoRanges {
@@ -364,6 +369,8 @@ struct Engine::Impl {
         slice_off.release(st);
         evo_new.release(st);
         ev_anc.release(st);
+        ev_sig.release(st);
+        evo_sigs.release(st);
         lvl_ranges.release(st);
         fin_ids.release(st);
         map_s.release(st);
@@ -429,6 +436,8 @@ struct Engine::Impl {
         P.ev_cons = ev_cons.p;
         P.ev_cprod = ev_cprod.p;
         P.ev_anc = ev_anc.p;
+        P.ev_sig = ev_sig.p;
+        P.evo_sigs = evo_sigs.p;
         P.state_of_arrival = state_of_arrival.p;
         P.tab_keys = tab_keys.p;
         P.tab_vals = tab_vals.p;
@@ -672,6 +681,8 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + evo0, &h_evos[evo0], nnew * sizeof(DevEvo), cudaMemcpyHostToDevice, st));
         evo_classes.ensure(nevo, evo0, st);
         evo_states.ensure(nevo, evo0, st);
+        evo_sigs.ensure(nevo, evo0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_sigs.p + evo0, 0, nnew * sizeof(unsigned long long), st));
         evo_cut.ensure(nevo, evo0, st);
         evo_first_ev.ensure(nevo, evo0, st);
         evo_last_ev.ensure(nevo, evo0, st);
@@ -758,23 +769,28 @@ struct Engine::Impl {
     }
 
     // Rebuild an evolution's dedup table at a larger capacity.
-    void regrow_table(uint32_t evo, uint64_t need) {
-        DevEvo& d = h_evos[evo];
-        const uint64_t cap = next_pow2(std::max<uint64_t>(need * 2, (d.table_mask + 1) * 2));
-        const uint64_t off = tab_slots;
+    // A new, larger table region for (off, mask) holding `need` keys at load <= 1/2; the old
+    // region (if any, mask != 0) is rehashed into it. The caller uploads the changed h_evos.
+    void regrow_region(uint64_t& off, uint64_t& mask, uint64_t need) {
+        const uint64_t cap = next_pow2(std::max<uint64_t>({need * 2, mask ? (mask + 1) * 2 : 0, 256}));
+        const uint64_t noff = tab_slots;
         const uint64_t new_slots = tab_slots + cap + 1;
         tab_keys.ensure(new_slots, tab_slots, st);
         tab_vals.ensure(new_slots, tab_slots, st);
-        HGX_CUDA_CHECK(cudaMemsetAsync(tab_keys.p + off, 0, (cap + 1) * sizeof(unsigned long long), st));
-        HGX_CUDA_CHECK(cudaMemsetAsync(tab_vals.p + off, 0xFF, (cap + 1) * sizeof(uint32_t), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_keys.p + noff, 0, (cap + 1) * sizeof(unsigned long long), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(tab_vals.p + noff, 0xFF, (cap + 1) * sizeof(uint32_t), st));
         tab_slots = new_slots;
-        DevEvo nd = d;
-        nd.table_off = off;
-        nd.table_mask = cap - 1;
-        const uint64_t old_n = d.table_mask + 2;
-        k_rehash<<<grid_for(old_n, 256), 256, 0, st>>>(tab_keys.p, tab_vals.p, d.table_off, d.table_mask, nd.table_off, nd.table_mask, err.p);
-        check_launch();
-        d = nd;   // the caller uploads the changed h_evos entries
+        if (mask) {
+            k_rehash<<<grid_for(mask + 2, 256), 256, 0, st>>>(tab_keys.p, tab_vals.p, off, mask, noff,
+                                                             cap - 1, err.p);
+            check_launch();
+        }
+        off = noff;
+        mask = cap - 1;
+    }
+
+    void regrow_table(uint32_t evo, uint64_t need) {
+        regrow_region(h_evos[evo].table_off, h_evos[evo].table_mask, need);
     }
 
     // Upload h_evos[lo, hi) (one copy for all the tables a level regrew).
@@ -835,14 +851,15 @@ struct Engine::Impl {
         const uint32_t C = E ? clast + h_rules[rlast].n_lhs - c0 : 0;
         const bool se = opt.keep_state_edges;
         // host block layout (hgx_array order), 16-byte aligned sections
+        const bool sg = opt.event_keys != 0;
         uint64_t count[ResultArrays::kArrays] = {
             S, S, 4ull * E, 3ull * K, 2 * B, uint64_t(E) + 1, C, 2ull * E,
-            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0};
+            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0, sg ? E : 0};
         uint64_t off[ResultArrays::kArrays];
         uint64_t total = 0;
         for (int i = 0; i < ResultArrays::kArrays; ++i) {
             off[i] = total;
-            total += (count[i] * (i == 0 ? 8 : 4) + 15) / 16 * 16;
+            total += (count[i] * arr_elem_bytes(i) + 15) / 16 * 16;
         }
         // device staging for the derived arrays (same layout; direct arrays are copied from
         // their own device buffers)
@@ -879,12 +896,13 @@ struct Engine::Impl {
         auto flat = std::make_shared<ResultArrays>();
         flat->owner = std::shared_ptr<void>(h, [pool, cap](void* p) { pool->put(p, cap); });
         auto d2h_from = [&](int i, const void* src) {
-            const size_t bytes = count[i] * (i == 0 ? 8 : 4);
+            const size_t bytes = count[i] * arr_elem_bytes(i);
             if (bytes) HGX_CUDA_CHECK(cudaMemcpyAsync(h + off[i], src, bytes, cudaMemcpyDeviceToHost, st));
         };
         d2h_from(0, st_hash.p);
         d2h_from(1, st_depth.p);
         d2h_from(6, ev_cons.p + c0);
+        if (sg) d2h_from(HGX_ARR_EVENT_SIG, ev_sig.p + R);
         if (se) {
             d2h_from(8, eoff);
             d2h_from(11, voff);
@@ -904,6 +922,13 @@ struct Engine::Impl {
         r.flat = flat;
         r.n_roots = R;
         r.num_classes = classes;
+        r.n_canonical_events = E;
+        if (sg) {
+            unsigned long long nsig = 0;
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&nsig, evo_sigs.p, 8, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            r.n_canonical_events = nsig;
+        }
         r.truncated = stopped != 0;
         if (r.truncated)
             r.warnings.push_back(
@@ -946,7 +971,9 @@ struct Engine::Impl {
         uint32_t* ecc = sno + S + 1;             // [E+1] -> coff
         uint32_t* ekc = ecc + E + 1;             // [E+1] -> koff
         const bool se = opt.keep_state_edges;
-        uint64_t hbytes = 8ull * S + 4ull * S;
+        // gathered hashes + depths at the front of `fin`; the staging block after them starts on
+        // a 16-byte boundary (its sections hold u64 arrays written by kernels)
+        const uint64_t hbytes = (8ull * S + 4ull * S + 15) / 16 * 16;
         fin.ensure(std::max<uint64_t>(hbytes, 16), 0, st);
         k_gather_states<<<grid_for(S, 256), 256, 0, st>>>(ptrs(), sids, S, reinterpret_cast<uint64_t*>(fin.p),
                                                           reinterpret_cast<uint32_t*>(fin.p + 8ull * S), sne, sno);
@@ -971,14 +998,20 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemcpyAsync(&classes, evo_classes.p + evo, 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         if (!opt.causal) K = 0;
+        const bool sg = opt.event_keys != 0;
+        unsigned long long nsig = E;
+        if (sg) {
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&nsig, evo_sigs.p + evo, 8, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        }
         uint64_t count[ResultArrays::kArrays] = {
             S, S, 4ull * E, 3ull * K, 2 * B, uint64_t(E) + 1, C, 2ull * E,
-            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0};
+            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0, sg ? E : 0};
         uint64_t off[ResultArrays::kArrays];
         uint64_t total = 0;
         for (int i = 0; i < ResultArrays::kArrays; ++i) {
             off[i] = total;
-            total += (count[i] * (i == 0 ? 8 : 4) + 15) / 16 * 16;
+            total += (count[i] * arr_elem_bytes(i) + 15) / 16 * 16;
         }
         // staging: hashes/depths were gathered at the front of `fin`; move them into place
         fin.ensure(total + hbytes, hbytes, st);
@@ -992,6 +1025,11 @@ struct Engine::Impl {
                                                               map_s.p, map_e.p, nullptr, nullptr, ecc, ekc,
                                                               dp(2), dp(6), dp(7),
                                                               opt.causal ? dp(3) : fin_scratch_causal(K), 1);
+            check_launch();
+        }
+        if (sg && E) {
+            k_gather_u64<<<grid_for(E, 256), 256, 0, st>>>(ev_sig.p, eids, E,
+                                                           reinterpret_cast<uint64_t*>(d + off[HGX_ARR_EVENT_SIG]));
             check_launch();
         }
         if (B) {
@@ -1025,6 +1063,7 @@ struct Engine::Impl {
         r.flat = flat;
         r.n_roots = er.roots;
         r.num_classes = classes;
+        r.n_canonical_events = nsig;
         r.truncated = stopped != 0;
         if (r.truncated)
             r.warnings.push_back(
@@ -1044,7 +1083,8 @@ struct Engine::Impl {
     // Counts only (results stay on the device): events and branchial pairs from the recorded
     // per-evolution ranges, states and classes from the device counters, causal triples by one
     // pass over the events.
-    void read_counts(const std::vector<uint32_t>& which, std::vector<EvolutionResult>& out) {
+    void read_counts(const std::vector<uint32_t>& which, std::vector<EvolutionResult>& out,
+                     bool signatures) {
         const size_t nevo = h_evos.size();
         totals.ensure(nevo, 0, st);
         HGX_CUDA_CHECK(cudaMemsetAsync(totals.p, 0, nevo * sizeof(unsigned long long), st));
@@ -1053,8 +1093,10 @@ struct Engine::Impl {
                                                                   totals.p);
             check_launch();
         }
-        std::vector<unsigned long long> causal(nevo), cls(nevo), sts(nevo);
+        std::vector<unsigned long long> causal(nevo), cls(nevo), sts(nevo), sig(nevo, 0);
         std::vector<uint32_t> stop(nevo);
+        if (signatures)
+            HGX_CUDA_CHECK(cudaMemcpyAsync(sig.data(), evo_sigs.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(causal.data(), totals.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(cls.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(sts.data(), evo_states.p, nevo * 8, cudaMemcpyDeviceToHost, st));
@@ -1070,6 +1112,7 @@ struct Engine::Impl {
             for (auto& q : evo_ranges[e].events) r.n_events += q.second - q.first;
             for (auto& q : evo_ranges[e].pairs) r.n_branchial += q.second - q.first;
             r.n_causal = causal[e];
+            r.n_canonical_events = signatures ? sig[e] : r.n_events;
             r.truncated = stop[e] != 0;
         }
     }
@@ -1131,6 +1174,7 @@ struct Engine::Impl {
         // ---- count
         const bool fwd = opt.forwarding != 0;
         A.fwd_mode = opt.forwarding;
+        A.ev_keys = opt.event_keys;
         const Layout Lc = make_layout(ne_bound, nocc_bound, rm, LayoutKind::Count, fwd);
         fmode.ensure(F, 0, st);
         A.fmode = fmode.p;
@@ -1167,7 +1211,9 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[4], level_max.p + 2, 8, cudaMemcpyDeviceToHost, st));
         const size_t nevo = h_evos.size();
         std::vector<uint32_t> h_first(nevo), h_last(nevo);
-        std::vector<unsigned long long> h_classes(nevo), h_states_ev(nevo);
+        std::vector<unsigned long long> h_classes(nevo), h_states_ev(nevo), h_sigs(nevo, 0);
+        if (opt.event_keys)
+            HGX_CUDA_CHECK(cudaMemcpyAsync(h_sigs.data(), evo_sigs.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(h_first.data(), evo_first_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(h_last.data(), evo_last_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(h_classes.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
@@ -1202,8 +1248,18 @@ struct Engine::Impl {
             if (h_evos[e].max_states) any_cap = true;
             const uint64_t lv = (h_last[e] >= h_first[e]) ? h_last[e] - h_first[e] : 0;
             const uint64_t need = h_classes[e] + lv + 1;
+            bool grown = false;
             if (2 * need > h_evos[e].table_mask + 1) {
                 regrow_table(static_cast<uint32_t>(e), need);
+                grown = true;
+            }
+            // event signatures: every distinct one so far plus every event of this level
+            const uint64_t need_s = h_sigs[e] + lv + 1;
+            if (opt.event_keys && (!h_evos[e].sig_mask || 2 * need_s > h_evos[e].sig_mask + 1)) {
+                regrow_region(h_evos[e].sig_off, h_evos[e].sig_mask, need_s);
+                grown = true;
+            }
+            if (grown) {
                 grown_lo = std::min(grown_lo, e);
                 grown_hi = e + 1;
             }
@@ -1475,6 +1531,13 @@ struct Engine::Impl {
             check_launch();
             k_outstate<<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
+            if (opt.event_keys) {
+                ev_sig.ensure(n_events + ne2, n_events, st);
+                for (int pass = 0; pass < 2; ++pass) {
+                    k_evsig<<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A, pass);
+                    check_launch();
+                }
+            }
             if (n_new) {
                 k_materialize<<<grid_for(uint64_t(n_new) * 32, 256), 256, 0, st>>>(ptrs(), A, n_new);
                 check_launch();
@@ -1560,6 +1623,9 @@ void Engine::Impl::read_results(const std::vector<uint32_t>& which, const RunOpt
     auto e_cprod = d2h(I.ev_cprod.p, I.n_cons, st);
     auto bp = d2h(I.bpairs.p, 2 * I.n_bpairs, st);
     auto evc = d2h(I.evo_classes.p, nevo, st);
+    const bool sg = opt.event_keys != 0;
+    auto e_sig = sg ? d2h(I.ev_sig.p, I.n_events, st) : std::vector<unsigned long long>{};
+    auto evsig = sg ? d2h(I.evo_sigs.p, nevo, st) : std::vector<unsigned long long>{};
     auto evs = d2h(I.evo_stopped.p, nevo, st);
     std::vector<uint64_t> s_off;
     std::vector<uint32_t> s_ne, s_nocc, arena;
@@ -1620,6 +1686,7 @@ void Engine::Impl::read_results(const std::vector<uint32_t>& which, const RunOpt
         r.ev_cons_off.push_back(static_cast<uint32_t>(r.ev_cons.size()));
         r.ev_prod_first.push_back(e_prod[e]);
         r.ev_prod_count.push_back(R.n_rhs);
+        if (sg) r.ev_sig.push_back(e_sig[e]);
     }
     for (auto& r : out)
         for (auto& se : r.state_event) se = (se < local_event.size() && local_event[se] != kNone) ? local_event[se] : kNone;
@@ -1647,6 +1714,7 @@ void Engine::Impl::read_results(const std::vector<uint32_t>& which, const RunOpt
     }
     for (size_t i = 0; i < which.size(); ++i) {
         out[i].num_classes = evc[which[i]];
+        out[i].n_canonical_events = sg ? evsig[which[i]] : out[i].ev_in.size();
         out[i].truncated = evs[which[i]] != 0;
         if (out[i].truncated)
             out[i].warnings.push_back(
@@ -1669,7 +1737,7 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
     const std::vector<uint32_t> ids = I.admit_many(ptrs);
     while (I.level(opt)) {}
     std::vector<EvolutionResult> out;
-    if (!opt.readback) I.read_counts(ids, out);
+    if (!opt.readback) I.read_counts(ids, out, opt.event_keys != 0);
     else if (ids.size() == 1) out.push_back(I.finalize_single(opt));
     else I.read_results(ids, opt, out);
     I.finish_times();
@@ -1693,7 +1761,7 @@ EvolutionResult Engine::collect(uint32_t evo, const RunOptions& opt) {
     if (evo >= impl_->h_evos.size()) throw std::invalid_argument("collect: unknown evolution id");
     if (opt.readback) return impl_->finalize_evo(evo, opt);
     std::vector<EvolutionResult> out;
-    impl_->read_counts({evo}, out);
+    impl_->read_counts({evo}, out, opt.event_keys != 0);
     return std::move(out[0]);
 }
 uint32_t Engine::active() const {

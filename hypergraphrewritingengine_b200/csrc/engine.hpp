@@ -44,7 +44,7 @@ struct EvolutionSpec {
 // A result's arrays in one host block (page-locked when the block came from the device in a
 // single copy), indexed like the C-ABI's hgx_array codes; `owner` frees the block.
 struct ResultArrays {
-    static constexpr int kArrays = 13;
+    static constexpr int kArrays = 14;
     std::shared_ptr<void> owner;
     const void* ptr[kArrays] = {};
     uint64_t count[kArrays] = {};   // elements (u64 for the hashes, u32 otherwise)
@@ -71,7 +71,9 @@ struct EvolutionResult {
     // Relations over local event ids.
     std::vector<uint32_t> causal;               // (producer, consumer, edge) triples
     std::vector<uint32_t> branchial;            // (a, b) pairs, a < b
+    std::vector<uint64_t> ev_sig;               // event signatures (event canonicalisation on)
     uint64_t num_classes = 0;
+    uint64_t n_canonical_events = 0;            // distinct event signatures (= events when off)
     bool truncated = false;
     std::vector<std::string> warnings;
     // Set when the run kept its results on the device (RunOptions::readback == false): the
@@ -93,6 +95,9 @@ struct RunOptions {
     uint64_t chunk_min = 8192;
     // Transitive reduction of the causal graph (evolutions of at most 64 levels).
     bool transitive_reduction = false;
+    // Event canonicalisation: hgcommon EventSignatureKeys bits 0-3 (input state, output state,
+    // step, rule); 0 = every application is its own event.
+    uint32_t event_keys = 0;
 };
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.

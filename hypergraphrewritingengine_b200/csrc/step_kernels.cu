@@ -92,8 +92,8 @@ __device__ __forceinline__ void warp_count(unsigned long long* counter, uint32_t
 // id (event id, or a root's pseudo-event id) that produced the key: the first arrival in
 // canonical order wins, whatever order the warps ran in.
 // ------------------------------------------------------------------------------------------
-__device__ void table_insert(const DevPtrs& P, const DevEvo& ev, uint64_t h, uint32_t arrival) {
-    const uint64_t base = ev.table_off, mask = ev.table_mask;
+__device__ void slot_insert(const DevPtrs& P, uint64_t base, uint64_t mask, uint64_t h,
+                            uint32_t arrival) {
     if (h == 0) { atomicMin(&P.tab_vals[base + mask + 1], arrival); return; }
     uint64_t slot = smix(h) & mask;
     for (uint64_t probe = 0; probe <= mask; ++probe) {
@@ -109,8 +109,7 @@ __device__ void table_insert(const DevPtrs& P, const DevEvo& ev, uint64_t h, uin
     atomicOr(P.err, kErrTableFull);
 }
 
-__device__ uint32_t table_lookup(const DevPtrs& P, const DevEvo& ev, uint64_t h) {
-    const uint64_t base = ev.table_off, mask = ev.table_mask;
+__device__ uint32_t slot_lookup(const DevPtrs& P, uint64_t base, uint64_t mask, uint64_t h) {
     if (h == 0) return P.tab_vals[base + mask + 1];
     uint64_t slot = smix(h) & mask;
     for (uint64_t probe = 0; probe <= mask; ++probe) {
@@ -120,6 +119,15 @@ __device__ uint32_t table_lookup(const DevPtrs& P, const DevEvo& ev, uint64_t h)
         slot = (slot + 1) & mask;
     }
     return kNone;
+}
+
+// The evolution's state dedup table (key = WL hash, value = first arrival).
+__device__ __forceinline__ void table_insert(const DevPtrs& P, const DevEvo& ev, uint64_t h,
+                                             uint32_t arrival) {
+    slot_insert(P, ev.table_off, ev.table_mask, h, arrival);
+}
+__device__ __forceinline__ uint32_t table_lookup(const DevPtrs& P, const DevEvo& ev, uint64_t h) {
+    return slot_lookup(P, ev.table_off, ev.table_mask, h);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1368,6 +1376,13 @@ __global__ void k_gather_events(DevPtrs P, const uint32_t* ids, uint32_t n, uint
 }
 
 // Branchial pairs of one evolution: the concatenation of `nr` ranges of the pair array.
+// out[i] = src[ids[i]] (64-bit values of the listed ids).
+__global__ void k_gather_u64(const unsigned long long* src, const uint32_t* ids, uint32_t n,
+                             uint64_t* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = src[ids[i]];
+}
+
 __global__ void k_gather_pairs(const uint32_t* pairs, const uint64_t* rstart, const uint64_t* rcum,
                                uint32_t nr, uint64_t n, const uint32_t* emap, uint32_t* out) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
@@ -1607,6 +1622,40 @@ __global__ void k_outstate(DevPtrs P, LevelArgs A) {
             if (w == kNone) { atomicOr(P.err, kErrTableFull); P.ev_out[e] = kNone; }
             else P.ev_out[e] = P.state_of_arrival[w];
         }
+    }
+}
+
+// Event canonicalisation (Hypergraph::create_event, hypergraph/src/hypergraph.cpp:449-500): the
+// signature of every kept event of the level from its input and output states' WL hashes, the
+// step of the output's canonical state -- the first state of its class, whose arrival the dedup
+// table holds (hypergraph.cpp:362-377) -- and its rule; pass 0 inserts it into the evolution's
+// signature table (smallest event id wins, so across levels the first event in canonical order is
+// the canonical one); pass 1 counts the winners per evolution.
+__global__ void k_evsig(DevPtrs P, LevelArgs A, int pass) {
+    for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < A.n_events; t0 += gridDim.x * blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        uint32_t evo = 0;
+        bool win = false;
+        if (t < A.n_events) {
+            const uint32_t e = A.ev_base + t;
+            if (P.ev_kept[e]) {
+                const uint32_t in = P.ev_in[e];
+                evo = P.st_evo[in];
+                const DevEvo& ev = P.evos[evo];
+                if (pass == 0) {
+                    const uint32_t first = table_lookup(P, ev, P.ev_hash[e]);
+                    const uint32_t fin = first == kNone ? kNone : P.ev_in[first];
+                    const uint32_t step = fin == kNone ? 0u : P.st_depth[fin] + 1;
+                    const uint64_t sig = event_signature(A.ev_keys, P.st_hash[in], P.ev_hash[e],
+                                                         step, P.ev_rule[e] - ev.rule_begin);
+                    P.ev_sig[e] = sig;
+                    slot_insert(P, ev.sig_off, ev.sig_mask, sig, e);
+                } else {
+                    win = slot_lookup(P, ev.sig_off, ev.sig_mask, P.ev_sig[e]) == e;
+                }
+            }
+        }
+        if (pass == 1) warp_count(P.evo_sigs, evo, win);
     }
 }
 

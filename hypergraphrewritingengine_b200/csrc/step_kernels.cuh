@@ -63,6 +63,9 @@ struct DevPtrs {
     // transitive reduction: per event, bit d set = an event at level d is a proper causal
     // ancestor (levels < 64; an event's ancestors lie on its input state's history chain)
     unsigned long long* ev_anc;
+    // event canonicalisation: per event its signature; per evolution the distinct signatures
+    unsigned long long* ev_sig;
+    unsigned long long* evo_sigs;
     // errors
     uint32_t* err;
     // expand-kernel counters, [0..3] lane-per-child kernel, [4..7] warp-per-child kernel:
@@ -94,6 +97,7 @@ struct LevelArgs {
     uint32_t n_sw;
     uint8_t* fmode;             // [F] bit 0: children hashed lane-per-child; bit 1: forwarding
     uint32_t fwd_mode;          // 0 off, 1 every eligible state, 2 states with >= 48 edges
+    uint32_t ev_keys;           // event signature keys (0 = no event canonicalisation)
     uint32_t* work;             // work-queue counters
     // select / assign
     uint32_t* flag_new;         // [n_events]

@@ -80,7 +80,15 @@ typedef enum hgx_option {
        of its events past every cut is built in rounds that stop at each evolution's cut, so the
        dropped events are never built (default 8192; 0 = whenever a cap can cut). No reference
        counterpart; results are identical for every value. */
-    HGX_OPT_CHUNK_MIN = 9
+    HGX_OPT_CHUNK_MIN = 9,
+    /* Event canonicalisation (Hypergraph::set_event_signature_keys, hypergraph.hpp:778;
+       EvolveInput::event_canonicalization): hgcommon EventSignatureKeys bits over the WL
+       canonical hashes -- 1 input state, 2 output state, 4 step, 8 rule (3 = the reference's
+       Full preset). Events with equal signatures are one canonical event (HGX_COUNT_CANONICAL_EVENTS,
+       HGX_ARR_EVENT_SIG); causal and branchial edges stay over every application, as in the
+       reference. The edge-rank keys (16, 32; the Automatic preset) need an exact canonical
+       labelling of every state and are rejected. Default 0. */
+    HGX_OPT_EVENT_SIGNATURE_KEYS = 10
 } hgx_option;
 
 /* One evolution of a batch or a served request. */
@@ -105,7 +113,10 @@ typedef enum hgx_count {
     HGX_COUNT_CONSUMED = 6,      /* total consumed-edge entries over all events */
     HGX_COUNT_STATE_EDGES = 7,   /* total edge entries over all state records */
     HGX_COUNT_STATE_VERTS = 8,   /* total vertex entries over all state records */
-    HGX_COUNT_RAW_STATES = 9     /* Hypergraph::num_states (hypergraph.hpp:567): roots + events */
+    HGX_COUNT_RAW_STATES = 9,    /* Hypergraph::num_states (hypergraph.hpp:567): roots + events */
+    HGX_COUNT_CANONICAL_EVENTS = 10 /* distinct event signatures under HGX_OPT_EVENT_SIGNATURE_KEYS
+                                       (Hypergraph::num_events with event canonicalisation on,
+                                       hypergraph.cpp:1639-1644); = EVENTS when off */
 } hgx_count;
 
 /* Arrays (hgx_result_copy); element type and length in brackets. */
@@ -122,7 +133,10 @@ typedef enum hgx_array {
     HGX_ARR_STATE_EDGE_IDS = 9,  /* [u32 x STATE_EDGES] */
     HGX_ARR_STATE_ARITY = 10,    /* [u32 x STATE_EDGES] */
     HGX_ARR_STATE_VERT_OFF = 11, /* [u32 x STATES+1] */
-    HGX_ARR_STATE_VERTS = 12     /* [u32 x STATE_VERTS] */
+    HGX_ARR_STATE_VERTS = 12,    /* [u32 x STATE_VERTS] */
+    HGX_ARR_EVENT_SIG = 13       /* [u64 x EVENTS] event signature (hg_gpu::Event::signature);
+                                    empty unless HGX_OPT_EVENT_SIGNATURE_KEYS is set. The canonical
+                                    event of a signature is its first event in this order. */
 } hgx_array;
 
 /* Message of the last failure on this thread ("" if none). */

@@ -21,6 +21,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../hgx.h"
@@ -169,12 +170,26 @@ public:
 
 class Hypergraph {
     detail::ResultPtr r_;
+    uint8_t event_keys_ = 0;
     friend class ParallelEvolutionEngine;
 
 public:
+    // Event canonicalisation (hypergraph.hpp:778): EventSignatureKeys bits over the WL hashes --
+    // 1 input state, 2 output state, 4 step, 8 rule (3 = Full). The edge-rank keys need an exact
+    // canonical labelling and are rejected.
+    void set_event_signature_keys(uint8_t keys) {
+        if (keys & ~0xFu) throw std::invalid_argument("event signature keys: edge ranks are not provided");
+        event_keys_ = keys;
+    }
+    uint8_t event_signature_keys() const { return event_keys_; }
     // Raw states: every root plus one per event (hypergraph.hpp:567).
     uint32_t num_states() const { return r_ ? static_cast<uint32_t>(hgx_result_count(r_.get(), HGX_COUNT_RAW_STATES)) : 0; }
-    uint32_t num_events() const { return r_ ? static_cast<uint32_t>(hgx_result_count(r_.get(), HGX_COUNT_EVENTS)) : 0; }
+    // Canonical events when event canonicalisation is on (hypergraph.cpp:1639-1644).
+    uint32_t num_events() const {
+        if (!r_) return 0;
+        return static_cast<uint32_t>(hgx_result_count(r_.get(), event_keys_ ? HGX_COUNT_CANONICAL_EVENTS : HGX_COUNT_EVENTS));
+    }
+    uint32_t num_raw_events() const { return r_ ? static_cast<uint32_t>(hgx_result_count(r_.get(), HGX_COUNT_EVENTS)) : 0; }
     // Distinct WL canonical hashes.
     size_t num_canonical_states() const { return r_ ? hgx_result_count(r_.get(), HGX_COUNT_CLASSES) : 0; }
     // The recorded states' WL hashes (every raw state in full multiway, one per class in quotient).
@@ -222,6 +237,7 @@ public:
 
 private:
     void run(const std::vector<uint32_t>& blob, size_t steps) {
+        detail::check(hgx_engine_set_option(eng_.get(), HGX_OPT_EVENT_SIGNATURE_KEYS, hg_->event_keys_));
         hgx_result* r = nullptr;
         detail::check(hgx_evolve(eng_.get(), blob.data(), blob.size(), static_cast<uint32_t>(steps), &r));
         hg_->r_.reset(r, detail::ResultDeleter());
@@ -249,12 +265,16 @@ struct RewriteRule {
     uint8_t num_rhs_vars = 0;
 };
 
+enum class EventCanonicalizationMode : uint8_t { None = 0, Full, Automatic };
+
 struct EvolveInput {
     std::vector<RewriteRule> rules;
     std::vector<std::vector<VertexId>> initial_state;
     std::vector<std::vector<std::vector<VertexId>>> initial_states;   // takes precedence
     uint32_t num_steps = 0;
     bool transitive_reduction = true;           // as the reference's default
+    // None / Full (input and output WL hashes); Automatic needs edge ranks and is rejected
+    EventCanonicalizationMode event_canonicalization = EventCanonicalizationMode::None;
     bool explore_from_canonical_states_only = true;
     bool edge_identity = true;                  // keep the state edge records
     uint64_t max_states = 0;
@@ -268,6 +288,8 @@ struct CanonicalState {
 
 struct Event {
     EventId id = 0xFFFFFFFFu;
+    EventId canonical_id = 0xFFFFFFFFu;   // first event with the same signature (= id when off)
+    uint64_t signature = 0;               // 0 under EventCanonicalizationMode::None
     StateId input_state = 0xFFFFFFFFu, output_state = 0xFFFFFFFFu;
     uint32_t rule = 0, step = 0;
     std::vector<EdgeId> consumed_edges, produced_edges;
@@ -301,6 +323,10 @@ inline EvolveResult evolve(const EvolveInput& in, int device = 0) {
     detail::check(hgx_engine_set_option(e, HGX_OPT_QUOTIENT, in.explore_from_canonical_states_only));
     detail::check(hgx_engine_set_option(e, HGX_OPT_KEEP_STATE_EDGES, in.edge_identity));
     detail::check(hgx_engine_set_option(e, HGX_OPT_MAX_STATES, in.max_states));
+    if (in.event_canonicalization == EventCanonicalizationMode::Automatic)
+        throw std::invalid_argument("event canonicalization Automatic needs edge ranks (not provided)");
+    detail::check(hgx_engine_set_option(e, HGX_OPT_EVENT_SIGNATURE_KEYS,
+                                        in.event_canonicalization == EventCanonicalizationMode::Full ? 3 : 0));
     const auto blob = in.initial_states.empty()
                           ? detail::roots_blob(std::vector<std::vector<std::vector<VertexId>>>{in.initial_state})
                           : detail::roots_blob(in.initial_states);
@@ -329,10 +355,17 @@ inline EvolveResult evolve(const EvolveInput& in, int device = 0) {
     auto coff = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENT_CONS_OFF);
     auto cons = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENT_CONS);
     auto prod = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENT_PROD);
+    auto sig = detail::copy_array<uint64_t>(rr, HGX_ARR_EVENT_SIG);
+    std::unordered_map<uint64_t, EventId> first_of;
     out.events.resize(ev.size() / 4);
     for (size_t i = 0; i < out.events.size(); ++i) {
         Event& x = out.events[i];
         x.id = static_cast<EventId>(i);
+        x.canonical_id = x.id;
+        if (sig.size() == out.events.size()) {
+            x.signature = sig[i];
+            x.canonical_id = first_of.emplace(sig[i], x.id).first->second;
+        }
         x.input_state = ev[4 * i];
         x.output_state = ev[4 * i + 1];
         x.rule = ev[4 * i + 2];

@@ -43,6 +43,34 @@ def event_keys(in_hash, out_hash, rule, step):
     return h
 
 
+def event_signatures(state_hash, state_depth, events, keys):
+    """Per event, hgcommon::event_signature (common/include/hgcommon/event_core.hpp:64-84) over
+    the WL hashes: keys bit 0 input state, 1 output state, 2 step, 3 rule, folded in that order;
+    0 and the bare offset map to 1. The step is that of the output's canonical state, the first
+    state created with its hash (Hypergraph::get_canonical_state_for_event,
+    hypergraph/src/hypergraph.cpp:362-377, read at :486-490): the class's smallest depth.
+    events: uint32 [n, 4] = (in, out, rule, step)."""
+    sh = np.asarray(state_hash, dtype=np.uint64)
+    sd = np.asarray(state_depth, dtype=np.uint64)
+    ev = np.asarray(events, dtype=np.uint32).reshape(-1, 4)
+    sig = np.full(len(ev), FNV_OFFSET, dtype=np.uint64)
+    if keys & 1:
+        sig = _fold(sig, sh[ev[:, 0]])
+    if keys & 2:
+        sig = _fold(sig, sh[ev[:, 1]])
+    if keys & 4:
+        first_depth = {}
+        for h, d in zip(sh.tolist(), sd.tolist()):
+            if d < first_depth.get(h, 1 << 62):
+                first_depth[h] = d
+        step = np.array([first_depth[h] for h in sh[ev[:, 1]].tolist()], dtype=np.uint64)
+        sig = _fold(sig, step)
+    if keys & 8:
+        sig = _fold(sig, ev[:, 2].astype(np.uint64))
+    sig[(sig == 0) | (sig == FNV_OFFSET)] = np.uint64(1)
+    return sig
+
+
 def directed_pair_keys(a, b):
     h = np.full(len(a), FNV_OFFSET, dtype=np.uint64)
     return _fold(_fold(h, np.asarray(a, dtype=np.uint64)), np.asarray(b, dtype=np.uint64))

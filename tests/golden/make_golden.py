@@ -17,8 +17,12 @@ Also records the reference's own golden-matrix rows for the None/None/full-multi
 (reference/golden_matrix.txt), read as text.
 
 The "tr" section re-runs the full-multiway cases with the causal graph's transitive reduction on
-(serial execution) and stores the reduced causal count and key digest. `python make_golden.py tr`
-recomputes only that section in the existing golden.json.
+(serial execution) and stores the reduced causal count and key digest. The "evsig" section re-runs
+them with event canonicalisation (signature keys 3 = Full and 15 = input|output|step|rule) and
+stores the canonical event count and the number of distinct state hashes the reference reports
+then (it switches to its exact IR hash when event keys are on, so the counts pin the WL path
+wherever IR and WL classes coincide). `python make_golden.py tr` (or `evsig`) recomputes only that
+section in the existing golden.json.
 """
 import json
 import os
@@ -47,12 +51,28 @@ def tr_section():
     return out
 
 
+def evsig_section():
+    out = {}
+    for name, rules, roots, steps in cases.all_full_cases():
+        entry = {"steps": steps}
+        for keys in (3, 15):
+            r = pyoracle.run_reference(rules, roots, steps, quotient=False, threads=0, evkeys=keys)
+            entry[str(keys)] = {"events": r["events"], "raw_events": r["raw_events"],
+                                "classes": r["wl_classes"]}
+        out[name] = entry
+        print("evsig", name, entry["3"], entry["15"], flush=True)
+    return out
+
+
+SECTIONS = {"tr": tr_section, "evsig": evsig_section}
+
+
 def main():
-    if sys.argv[1:] == ["tr"]:
+    if len(sys.argv) == 2 and sys.argv[1] in SECTIONS:
         path = os.path.join(HERE, "golden.json")
         with open(path) as fh:
             out = json.load(fh)
-        out["tr"] = tr_section()
+        out[sys.argv[1]] = SECTIONS[sys.argv[1]]()
         with open(path, "w") as fh:
             json.dump(out, fh, indent=0, sort_keys=True)
         return
@@ -84,6 +104,7 @@ def main():
                 out["matrix"][f[0]] = {"steps": int(f[4]), "states": int(f[5]), "events": int(f[6]),
                                        "causal": int(f[7]), "pairs": int(f[8]), "branchial": int(f[9])}
     out["tr"] = tr_section()
+    out["evsig"] = evsig_section()
     with open(os.path.join(HERE, "golden.json"), "w") as fh:
         json.dump(out, fh, indent=0, sort_keys=True)
 

@@ -42,6 +42,24 @@ def test_transitive_reduction_matches_reference(name, golden):
         assert np.array_equal(n["causal_keys"], np.array(g["causal_keys"], np.uint64)), name
 
 
+@pytest.mark.parametrize("keys", [3, 15])
+@pytest.mark.parametrize("name", sorted(FULL))
+def test_event_canonicalisation_matches_reference(name, keys, golden):
+    """Canonical event count under event signature keys. The reference hashes states exactly (IR)
+    once event keys are on; where its class count equals the WL class count the two partitions
+    coincide (isomorphic states share a WL hash), so the canonical event counts must agree."""
+    rules, roots, steps = FULL[name]
+    r = pyoracle.evolve(rules, roots, steps, quotient=False)
+    sig = pyoracle.event_signatures(r["state_hash"], r["state_depth"], r["events"], keys)
+    g = golden["evsig"][name][str(keys)]
+    assert g["raw_events"] == len(r["events"]), name
+    n = len(np.unique(sig))
+    if g["classes"] == golden["full"][name]["wl_classes"]:
+        assert n == g["events"], name
+    else:   # WL merged some IR classes: signatures can only merge further
+        assert n <= g["events"], name
+
+
 # WL classes the reference's IR-keyed quotient separates but the WL hash merges (a WL collision
 # at the deepest level). Events are unaffected: they come from the levels above.
 WL_COLLISIONS = {"c2-quot-5": 3, "c3-quot-5": 1}
