@@ -40,6 +40,10 @@ constexpr uint32_t kFwdCap = 256;
 constexpr uint32_t kFwdMaxLhs = 4;
 
 // States with more vertex occurrences than this number their vertices through a hash table.
+// Lane-parallel join: states of at most this many edges (positions fit one byte), rules of at
+// most kLaneJoinLhs LHS edges (four positions pack into one word), and per (state, rule) at most
+// kLaneJoinCap matches staged in shared memory by the expand kernel.
+constexpr uint32_t kLaneJoinLhs = 4, kLaneJoinCap = 256;
 constexpr uint32_t kHashOccMin = 96;
 
 HGX_HD uint64_t fnv(uint64_t h, uint64_t x) { return (h ^ x) * kFnvPrime; }
@@ -104,6 +108,7 @@ enum ErrorBits : uint32_t {
     kErrArenaFull = 1u << 2,
     kErrBadRule = 1u << 3,
     kErrTrDepth = 1u << 4,       // transitive reduction past 64 levels
+    kErrJoinCount = 1u << 5,     // a state's matches differ between the count and expand passes
 };
 
 }  // namespace hgx

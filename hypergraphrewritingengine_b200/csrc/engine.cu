@@ -205,6 +205,7 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.o_pnn = take(2 * kLaneVMax, 2);
         L.o_pdeg = take(2 * kLaneVMax, 2);
         L.o_batch = take(32 * L.SB, 1);
+        L.o_mlist = take(4 * kLaneJoinCap, 4);
     }
     L.bytes = align_up(off, 16);
     return L;
@@ -1146,8 +1147,6 @@ struct Engine::Impl {
         item_cons.ensure(NI + 1, 0, st);
         item_prod.ensure(NI + 1, 0, st);
         item_fresh.ensure(NI + 1, 0, st);
-        bcount.ensure(F, 0, st);
-        boff.ensure(F + 1, 0, st);
 
         LevelArgs A;
         std::memset(&A, 0, sizeof(A));
@@ -1161,8 +1160,6 @@ struct Engine::Impl {
         A.item_fresh = item_fresh.p;
         A.work = work.p;
         A.level_max = level_max.p;
-        A.bcount = bcount.p;
-        A.boff = boff.p;
         A.ev_base = static_cast<uint32_t>(n_events);
         A.cons_base = static_cast<uint32_t>(n_cons);
         A.prod_base = static_cast<uint32_t>(n_edges);
@@ -1465,15 +1462,19 @@ struct Engine::Impl {
         // frontier states whose events were built (all of them unless a chunked cut stopped early)
         A.n_frontier = F_eff;
         const uint32_t ne2 = A.n_events;
+        bcount.ensure(uint64_t(ne2) + 1, 0, st);
+        boff.ensure(uint64_t(ne2) + 1, 0, st);
+        A.bcount = bcount.p;
+        A.boff = boff.p;
         if (opt.branchial && ne2) {
             tic();
-            k_bcount<<<grid_for(uint64_t(F_eff) * 32, 256), 256, 0, st>>>(ptrs(), A);
+            k_bpairs<false><<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
-            scan(bcount.p, boff.p, F_eff);
+            scan(bcount.p, boff.p, ne2);
             toc(times.branchial);
         } else {
             // no pairs this level: every offset is 0 (the per-evolution pair ranges read them)
-            HGX_CUDA_CHECK(cudaMemsetAsync(boff.p, 0, (uint64_t(F_eff) + 1) * 4, st));
+            HGX_CUDA_CHECK(cudaMemsetAsync(boff.p, 0, (uint64_t(ne2) + 1) * 4, st));
         }
 
         // per-evolution ranges of this level (events kept, new states, branchial pairs)
@@ -1481,9 +1482,8 @@ struct Engine::Impl {
         A.bbase = static_cast<uint32_t>(n_bpairs);
         lvl_ranges.ensure(6 * nevo, 0, st);
         if (ne2 || F_eff) {
-            A.n_frontier = F;   // boundaries over the whole frontier; pair ranges clamp to F_eff
-            k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, evo_frange.p,
-                                                          F_eff, lvl_ranges.p);
+            A.n_frontier = F;   // boundaries over the whole frontier; event ranges clamp to ne2
+            k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, lvl_ranges.p);
             check_launch();
             A.n_frontier = F_eff;
         }
@@ -1494,7 +1494,7 @@ struct Engine::Impl {
         uint32_t s2[4];
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[0], flag_rep.p + ne2, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[1], flag_front.p + ne2, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + F_eff, 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + ne2, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[3], err.p, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         if (s2[3] & kErrTrDepth)
@@ -1549,7 +1549,7 @@ struct Engine::Impl {
             // pair offsets are absolute: shift by the running total
             A.boff = boff.p;
             A.bpairs = bpairs.p + 2ull * n_bpairs;
-            k_bemit<<<grid_for(uint64_t(F_eff) * 32, 256), 256, 0, st>>>(ptrs(), A);
+            k_bpairs<true><<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
             toc(times.branchial);
         }

@@ -364,6 +364,94 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
 }
 
 // ------------------------------------------------------------------------------------------
+// Lane-parallel join for small staged states (<= 64 edges, <= kLaneJoinLhs LHS edges). Lane i
+// takes state edge e0 at the first scheduled position and walks the remaining positions on its
+// own, depth first, edges ascending; no warp synchronisation inside the walk. A lane's matches
+// come out in the lexicographic order of their state positions taken in schedule order -- the
+// order warp_join enumerates -- and lanes hold ascending e0, so (e0, walk order) is the canonical
+// match order. on_match(packed) receives the pattern-order positions, one byte each.
+// ------------------------------------------------------------------------------------------
+template <class F>
+__device__ uint32_t lane_walk(const Layout& L, const char* sm, const DevRule& R, const Parent& pa,
+                              uint32_t e0, F&& on_match) {
+    const uint8_t* pear = smp<uint8_t>(const_cast<char*>(sm), L.o_pear);
+    const uint16_t* pevo = smp<uint16_t>(const_cast<char*>(sm), L.o_pevo);
+    const uint16_t* vloc = smp<uint16_t>(const_cast<char*>(sm), L.o_vloc);
+    const uint32_t n = R.n_lhs;
+    uint16_t bind[kMaxVars];
+    uint32_t bound = 0;
+    uint32_t newly[kLaneJoinLhs];
+    uint32_t pick[kLaneJoinLhs];
+    uint64_t used = 0;
+    // bind pattern position sched[d] to state edge j; on failure nothing stays bound
+    auto try_bind = [&](uint32_t d, uint32_t j) -> bool {
+        const uint32_t p = R.sched[d];
+        const uint32_t a = R.lhs_ar[p];
+        if (pear[j] != a) return false;
+        const uint8_t* pv = &R.lhs_vars[R.lhs_off[p]];
+        const uint32_t vo = pevo[j];
+        uint32_t nb = 0;
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t var = pv[q];
+            const uint16_t x = vloc[vo + q];
+            if ((bound >> var) & 1u) {
+                if (bind[var] != x) { bound &= ~nb; return false; }
+            } else {
+                bind[var] = x;
+                bound |= 1u << var;
+                nb |= 1u << var;
+            }
+        }
+        newly[d] = nb;
+        return true;
+    };
+    if (!try_bind(0, e0)) return 0;
+    pick[0] = e0;
+    used = 1ull << e0;
+    uint32_t found = 0;
+    uint32_t d = 1, j = 0;
+    while (d > 0) {
+        if (d == n) {
+            uint32_t packed = 0;
+            for (uint32_t k = 0; k < n; ++k) packed |= pick[k] << (8u * R.sched[k]);
+            on_match(packed);
+            ++found;
+            --d;
+            if (d == 0) break;
+            bound &= ~newly[d];
+            used &= ~(1ull << pick[d]);
+            j = pick[d] + 1;
+            continue;
+        }
+        bool ok = false;
+        for (; j < pa.ne; ++j)
+            if (!((used >> j) & 1ull) && try_bind(d, j)) { ok = true; break; }
+        if (ok) {
+            pick[d] = j;
+            used |= 1ull << j;
+            ++d;
+            j = 0;
+        } else {
+            --d;
+            if (d == 0) break;
+            bound &= ~newly[d];
+            used &= ~(1ull << pick[d]);
+            j = pick[d] + 1;
+        }
+    }
+    return found;
+}
+
+// Matches of (state, rule) by lane walks over every first edge, warp total.
+__device__ uint32_t lane_join_count(const Layout& L, const char* sm, const DevRule& R,
+                                    const Parent& pa) {
+    uint32_t c = 0;
+    for (uint32_t b = 0; b < pa.ne; b += 32)
+        if (b + lane_id() < pa.ne) c += lane_walk(L, sm, R, pa, b + lane_id(), [](uint32_t) {});
+    return warp_sum32(c);
+}
+
+// ------------------------------------------------------------------------------------------
 // Child construction in shared memory: parent edges minus the matched ones (ascending, so the
 // reference's ascending edge-id order is kept) followed by the produced edges in RHS order.
 // Vertices stay local: a matched variable takes its bound local id, the n-th fresh variable
@@ -970,6 +1058,7 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
                 const Fwd fw = fwd_prepare(P, A, L, sm, R, ev, pa, sid, true);
                 fwd_on = fw.on;
                 if (fw.on) cnt = fwd_count(P, L, sm, R, pa, fw);
+                else if (pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs) cnt = lane_join_count(L, sm, R, pa);
                 else warp_join(L, sm, R, pa, R.sched, -1, [&](uint32_t) { ++cnt; });
             }
             if (lane == 0) A.counts[f * A.rules_stride + r] = cnt;
@@ -1120,6 +1209,55 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                 n_rounds += info.rounds;
             };
             if constexpr (kLane) {
+              if (!fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= kLaneJoinCap) {
+                // stage the rule's matches in canonical order (lane walks: count, scan, emit),
+                // then hash them 32 at a time, one child per lane
+                uint32_t* mlist = smp<uint32_t>(sm, L.o_mlist);
+                const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+                const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+                uint32_t total = 0;
+                for (uint32_t b = 0; b < pa.ne; b += 32) {
+                    const uint32_t e0 = b + lane;
+                    const uint32_t c = e0 < pa.ne ? lane_walk(L, sm, R, pa, e0, [](uint32_t) {}) : 0u;
+                    const uint32_t inc = warp_incl_scan(c);
+                    uint32_t w = total + inc - c;
+                    if (c) lane_walk(L, sm, R, pa, e0, [&](uint32_t pk) {
+                        if (w < kLaneJoinCap) mlist[w] = pk;
+                        ++w;
+                    });
+                    total += __shfl_sync(0xFFFFFFFFu, inc, 31);
+                }
+                __syncwarp();
+                if (total != rn) {
+                    if (lane == 0) atomicOr(P.err, kErrJoinCount);
+                    continue;
+                }
+                for (uint32_t b = 0; b < rn; b += 32) {
+                    const uint32_t i = b + lane;
+                    if (i < rn) {
+                        uint8_t* slot = batch + lane * L.SB;
+                        const uint32_t pk = mlist[i];
+                        uint16_t bv[kMaxVars];
+                        for (uint32_t k = 0; k < R.n_lhs; ++k) {
+                            const uint32_t pos = (pk >> (8u * k)) & 0xFFu;
+                            slot[k] = static_cast<uint8_t>(pos);
+                            const uint32_t vo = pevo[pos];
+                            for (uint32_t q = 0; q < R.lhs_ar[k]; ++q)
+                                bv[R.lhs_vars[R.lhs_off[k] + q]] = vloc[vo + q];
+                        }
+                        for (uint32_t t = 0; t < R.rhs_total; ++t) {
+                            const uint32_t var = R.rhs_vars[t];
+                            slot[R.n_lhs + t] = static_cast<uint8_t>(((R.new_mask >> var) & 1u)
+                                                                     ? pa.nvp + R.fresh_rank[var]
+                                                                     : bv[var]);
+                        }
+                        WlInfo info;
+                        const uint64_t h = lane_wl<kLaneVMax, kLaneNMax>(L, sm, pa, R, slot, info);
+                        finish(i, h, info, slot);
+                    }
+                    __syncwarp();
+                }
+              } else {
                 uint32_t nb = 0, done = 0;
                 auto flush = [&]() {
                     if (lane < nb) {
@@ -1144,6 +1282,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                     if (++nb == 32) flush();
                 });
                 if (nb) flush();
+              }
             } else {
                 // this rule's children inside the unit's slice: [lo, hi) of its match order
                 const uint32_t lo = c_lo > rb ? c_lo - rb : 0u;
@@ -1281,8 +1420,7 @@ __global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t
 // Per evolution of the level: its kept events, its new states and its branchial pairs are each
 // one contiguous range (the frontier is grouped by evolution and everything is numbered in
 // frontier order). out[evo * 6 + {0..5}] = event first/end, state first/end, pair first/end.
-__global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last,
-                             const uint32_t* evo_frange, uint32_t n_built_front, uint32_t* out) {
+__global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last, uint32_t* out) {
     for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
          f += gridDim.x * blockDim.x) {
         const uint32_t evo = P.st_evo[A.frontier[f]];
@@ -1290,15 +1428,13 @@ __global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last,
         const uint32_t e0 = P.evo_first_ev[evo];
         uint32_t e1 = min(evo_last[evo], A.ev_base + A.n_events);
         e1 = max(e0, min(e1, P.evo_cut[evo]));
-        const uint32_t f0 = min(evo_frange[2 * evo], n_built_front);
-        const uint32_t f1 = min(evo_frange[2 * evo + 1], n_built_front);
         uint32_t* o = out + 6ull * evo;
         o[0] = e0;
         o[1] = e1;
         o[2] = A.state_base + A.flag_rep[e0 - A.ev_base];
         o[3] = A.state_base + A.flag_rep[e1 - A.ev_base];
-        o[4] = A.bbase + A.boff[f0];
-        o[5] = A.bbase + A.boff[f1];
+        o[4] = A.bbase + A.boff[e0 - A.ev_base];
+        o[5] = A.bbase + A.boff[e1 - A.ev_base];
     }
 }
 
@@ -1756,72 +1892,44 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
     }
 }
 
-// Branchial pairs: events of one input state (contiguous ids) that consumed a common edge.
+// Branchial pairs (CausalGraph::record_branchial_overlaps, hypergraph/src/causal_graph.cpp:324-350):
+// two kept events of the same input state that consumed a common edge, each unordered pair once
+// as (a, b), a < b. One thread per event a of the level: the events of one input state are
+// contiguous (they are numbered in frontier order), so a walks its successors until the input
+// state changes. Pass 0 counts a's pairs into bcount[t]; pass 1 writes them at the scanned offset
+// boff[t] in (a, then b) order.
 template <bool kEmit>
-__device__ void branchial_state(const DevPtrs& P, const LevelArgs& A, uint32_t f) {
-    const uint32_t lane = lane_id();
-    const uint32_t lo = A.ev_base + A.item_ev[f * A.rules_stride];
-    const uint32_t hi = A.ev_base + A.item_ev[(f + 1) * A.rules_stride];
-    uint32_t total = 0;
-    uint32_t out = kEmit ? A.boff[f] : 0u;
-    for (uint32_t b = lo; b < hi; b += 32) {
-        const uint32_t a = b + lane;
+__global__ void k_bpairs(DevPtrs P, LevelArgs A) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
+         t += gridDim.x * blockDim.x) {
+        const uint32_t a = A.ev_base + t;
+        const uint32_t end = A.ev_base + A.n_events;
         uint32_t cnt = 0;
-        uint32_t ca[kMaxPatternEdges];
-        uint32_t na = 0;
-        const bool live = a < hi && P.ev_kept[a];
-        if (live) {
-            na = P.rules[P.ev_rule[a]].n_lhs;
-            const uint32_t co = P.ev_coff[a];
-            for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[co + k];
-        }
-        // pass 1: count (pass 2 writes at the warp-scanned offset)
-        for (int pass = 0; pass < (kEmit ? 2 : 1); ++pass) {
-            uint32_t pos = 0;
-            if (kEmit && pass == 1) {
-                const uint32_t inc = warp_incl_scan(cnt);
-                pos = out + inc - cnt;
-                out += __shfl_sync(0xFFFFFFFFu, inc, 31);
-            }
-            cnt = 0;
-            if (live) {
-                for (uint32_t c = a + 1; c < hi; ++c) {
-                    if (!P.ev_kept[c]) continue;
-                    const uint32_t nc = P.rules[P.ev_rule[c]].n_lhs;
-                    const uint32_t co = P.ev_coff[c];
-                    bool share = false;
-                    for (uint32_t k = 0; k < nc && !share; ++k) {
-                        const uint32_t x = P.ev_cons[co + k];
-                        for (uint32_t m = 0; m < na; ++m) share |= (ca[m] == x);
-                    }
-                    if (share) {
-                        if (kEmit && pass == 1) {
-                            A.bpairs[2ull * (pos + cnt)] = a;
-                            A.bpairs[2ull * (pos + cnt) + 1] = c;
-                        }
-                        ++cnt;
-                    }
+        if (P.ev_kept[a]) {
+            const uint32_t in = P.ev_in[a];
+            const uint32_t na = P.rules[P.ev_rule[a]].n_lhs, ca0 = P.ev_coff[a];
+            uint32_t ca[kMaxPatternEdges];
+            for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[ca0 + k];
+            uint32_t out = kEmit ? A.boff[t] : 0u;
+            for (uint32_t c = a + 1; c < end && P.ev_in[c] == in; ++c) {
+                if (!P.ev_kept[c]) continue;
+                const uint32_t nc = P.rules[P.ev_rule[c]].n_lhs, cc0 = P.ev_coff[c];
+                bool share = false;
+                for (uint32_t k = 0; k < nc && !share; ++k) {
+                    const uint32_t x = P.ev_cons[cc0 + k];
+                    for (uint32_t m = 0; m < na; ++m) share |= (ca[m] == x);
                 }
+                if (!share) continue;
+                if (kEmit) {
+                    A.bpairs[2ull * out] = a;
+                    A.bpairs[2ull * out + 1] = c;
+                    ++out;
+                }
+                ++cnt;
             }
         }
-        total += cnt;
+        if (!kEmit) A.bcount[t] = cnt;
     }
-    if (!kEmit) {
-        total = warp_sum32(total);
-        if (lane == 0) A.bcount[f] = total;
-    }
-}
-
-__global__ void k_bcount(DevPtrs P, LevelArgs A) {
-    for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < A.n_frontier;
-         f += (gridDim.x * blockDim.x) >> 5)
-        branchial_state<false>(P, A, f);
-}
-
-__global__ void k_bemit(DevPtrs P, LevelArgs A) {
-    for (uint32_t f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < A.n_frontier;
-         f += (gridDim.x * blockDim.x) >> 5)
-        branchial_state<true>(P, A, f);
 }
 
 // ------------------------------------------------------------------------------------------

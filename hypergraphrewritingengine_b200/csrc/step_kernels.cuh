@@ -109,8 +109,8 @@ struct LevelArgs {
     uint32_t* next_frontier;
     uint32_t* level_max;        // [2] max ne, max nocc over new states
     // branchial
-    uint32_t* bcount;           // [F]
-    uint32_t* boff;             // [F+1]
+    uint32_t* bcount;           // [n_events] pairs (a, later b) per event a
+    uint32_t* boff;             // [n_events+1] exclusive scan of bcount
     uint32_t* bpairs;           // output pairs (a, b)
     uint32_t bbase;             // pair index base
 };
@@ -126,7 +126,7 @@ struct Layout {
     uint32_t o_rule;                                                // DevRule
     // lane-per-child path: parent occurrence lists by vertex, per-vertex degree / neighbour
     // counts, and a batch of up to 32 matches (removed positions + produced local vertices)
-    uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_batch;
+    uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_batch, o_mlist;
     // match forwarding: seeded schedule, creating event's consumed edges, delta matches (and a
     // sorted copy), a 32-match chunk of forwarded matches
     uint32_t o_sched2, o_fkc, o_dkey, o_dpos, o_dkey2, o_dpos2, o_fkey, o_fpos;
