@@ -1539,7 +1539,7 @@ struct Engine::Impl {
                 }
             }
             if (n_new) {
-                k_materialize<<<grid_for(uint64_t(n_new) * 32, 256), 256, 0, st>>>(ptrs(), A, n_new);
+                k_materialize<<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
                 check_launch();
             }
             toc(times.materialize);

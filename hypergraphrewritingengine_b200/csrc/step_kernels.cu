@@ -86,6 +86,23 @@ __device__ __forceinline__ void warp_count(unsigned long long* counter, uint32_t
         atomicAdd(&counter[key], static_cast<unsigned long long>(__popc(peers)));
 }
 
+// Dynamic work queue over item indices: a warp takes kWorkChunk consecutive items per atomic.
+// One item per grab measured best: neighbouring items (states of one evolution) have similar
+// costs, so larger grabs unbalance the tail.
+constexpr uint32_t kWorkChunk = 1;
+struct WarpWork {
+    uint32_t base = 0, k = kWorkChunk;
+    __device__ __forceinline__ uint32_t next(uint32_t* counter) {
+        if (k == kWorkChunk) {
+            uint32_t b = 0;
+            if (lane_id() == 0) b = atomicAdd(counter, kWorkChunk);
+            base = __shfl_sync(0xFFFFFFFFu, b, 0);
+            k = 0;
+        }
+        return base + k++;
+    }
+};
+
 // ------------------------------------------------------------------------------------------
 // Dedup table: open addressing, linear probing, per-evolution region. Key 0 is EMPTY; a WL hash
 // that is itself 0 lives in the extra slot after the region. The value is the smallest arrival
@@ -994,10 +1011,9 @@ __global__ void k_roots(DevPtrs P, const uint32_t* sids, uint32_t n, uint32_t* w
     extern __shared__ __align__(16) char smem[];
     char* sm = smem + (threadIdx.x >> 5) * L.bytes;
     const uint32_t lane = lane_id();
+    WarpWork q;
     while (true) {
-        uint32_t i = 0;
-        if (lane == 0) i = atomicAdd(work, 1u);
-        i = __shfl_sync(0xFFFFFFFFu, i, 0);
+        const uint32_t i = q.next(work);
         if (i >= n) break;
         const uint32_t sid = sids[i];
         const Parent pa = load_parent(P, L, sm, sid);
@@ -1025,10 +1041,9 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
     char* sm = smem + (threadIdx.x >> 5) * L.bytes;
     const uint32_t lane = lane_id();
     const DevRule& R = *smp<DevRule>(sm, L.o_rule);
+    WarpWork q;
     while (true) {
-        uint32_t f = 0;
-        if (lane == 0) f = atomicAdd(&A.work[0], 1u);
-        f = __shfl_sync(0xFFFFFFFFu, f, 0);
+        const uint32_t f = q.next(&A.work[0]);
         if (f >= A.n_frontier) break;
         const uint32_t sid = A.frontier[f];
         const Parent pa = load_parent(P, L, sm, sid);
@@ -1140,10 +1155,9 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
     uint8_t* batch = smp<uint8_t>(sm, L.o_batch);
     uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
     uint32_t* work = &A.work[kLane ? 1 : 2];
+    WarpWork q;
     while (true) {
-        uint32_t u = 0;
-        if (lane == 0) u = atomicAdd(work, 1u);
-        u = __shfl_sync(0xFFFFFFFFu, u, 0);
+        const uint32_t u = q.next(work);
         // the parent's children [c_lo, c_hi) (in its child order over all rules) built by this unit
         uint32_t f, c_lo = 0, c_hi = 0xFFFFFFFFu;
         if (kLane || !A.soff) {
@@ -1803,92 +1817,104 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
     const uint32_t w = threadIdx.x >> 5;
     uint32_t* bind = bind_sm[w];
     uint32_t* cons = cons_sm[w];
-    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < n_new;
-         j += (gridDim.x * blockDim.x) >> 5) {
-        const uint32_t e = A.new_state_event[j];
-        const uint32_t sid = A.state_base + j;
-        const uint32_t f = P.ev_in[e];
-        const DevRule& R = P.rules[P.ev_rule[e]];
-        const uint32_t pne = P.st_ne[f], pnocc = P.st_nocc[f];
-        const uint32_t* prec = P.arena + P.st_off[f];
-        const uint32_t paw = (pne + 3) >> 2;
-        const uint32_t ne = pne - R.n_lhs + R.n_rhs;
-        const uint32_t nocc = pnocc - R.lhs_total + R.rhs_total;
-        const uint32_t aw = (ne + 3) >> 2;
-        const uint32_t words = ne + aw + nocc;
-        unsigned long long off = 0;
-        if (lane == 0) off = atomicAdd(P.arena_top, static_cast<unsigned long long>(words));
-        off = __shfl_sync(0xFFFFFFFFu, off, 0);
-        if (off + words > P.arena_cap) {
+    // groups of 32 new states per warp: record sizes by lane, one arena reservation per group
+    for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g * 32ull < n_new;
+         g += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t jl = g * 32 + lane;
+        uint32_t words = 0, gne = 0, gnocc = 0;
+        if (jl < n_new) {
+            const uint32_t e = A.new_state_event[jl];
+            const uint32_t f = P.ev_in[e];
+            const DevRule& R = P.rules[P.ev_rule[e]];
+            gne = P.st_ne[f] - R.n_lhs + R.n_rhs;
+            gnocc = P.st_nocc[f] - R.lhs_total + R.rhs_total;
+            words = gne + ((gne + 3) >> 2) + gnocc;
+        }
+        const uint32_t inc = warp_incl_scan(words);
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+        gne = warp_max32(gne);
+        gnocc = warp_max32(gnocc);
+        unsigned long long base = 0;
+        if (lane == 0) {
+            base = atomicAdd(P.arena_top, static_cast<unsigned long long>(total));
+            atomicMax(&A.level_max[0], gne);
+            atomicMax(&A.level_max[1], gnocc);
+        }
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base + total > P.arena_cap) {
             if (lane == 0) atomicOr(P.err, kErrArenaFull);
             continue;
         }
-        uint32_t* rec = P.arena + off;
-        uint8_t* rar = reinterpret_cast<uint8_t*>(rec + ne);
-        uint32_t* rv = rec + ne + aw;
-        if (lane < R.n_lhs) cons[lane] = P.ev_cons[P.ev_coff[e] + lane];
-        for (uint32_t t = lane; t < aw; t += 32) rec[ne + t] = 0;   // arity padding bytes
-        __syncwarp();
-        // binding from the consumed edges (sorted parent ids -> binary search for positions)
-        if (lane < R.n_lhs) {
-            const uint32_t gid = cons[lane];
-            uint32_t lo = 0, hi = pne;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (prec[mid] < gid) lo = mid + 1; else hi = mid;
+        const unsigned long long my_off = base + inc - words;
+        const uint32_t cnt = min(32u, n_new - g * 32);
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t j = g * 32 + k;
+            const unsigned long long off = __shfl_sync(0xFFFFFFFFu, my_off, k);
+            const uint32_t e = A.new_state_event[j];
+            const uint32_t sid = A.state_base + j;
+            const uint32_t f = P.ev_in[e];
+            const DevRule& R = P.rules[P.ev_rule[e]];
+            const uint32_t pne = P.st_ne[f], pnocc = P.st_nocc[f];
+            const uint32_t* prec = P.arena + P.st_off[f];
+            const uint32_t paw = (pne + 3) >> 2;
+            const uint32_t ne = pne - R.n_lhs + R.n_rhs;
+            const uint32_t nocc = pnocc - R.lhs_total + R.rhs_total;
+            const uint32_t aw = (ne + 3) >> 2;
+            uint32_t* rec = P.arena + off;
+            uint8_t* rar = reinterpret_cast<uint8_t*>(rec + ne);
+            uint32_t* rv = rec + ne + aw;
+            if (lane < R.n_lhs) cons[lane] = P.ev_cons[P.ev_coff[e] + lane];
+            for (uint32_t t = lane; t < aw; t += 32) rec[ne + t] = 0;   // arity padding bytes
+            __syncwarp();
+            // kept parent edges; a consumed edge binds its pattern edge's variables instead
+            uint32_t run_e = 0, run_pv = 0, run_cv = 0;
+            for (uint32_t b = 0; b < pne; b += 32) {
+                const uint32_t i = b + lane;
+                uint32_t id = 0, a = 0, hit = kNone;
+                if (i < pne) {
+                    id = prec[i];
+                    a = (prec[pne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
+                    for (uint32_t k2 = 0; k2 < R.n_lhs; ++k2)
+                        if (cons[k2] == id) hit = k2;
+                }
+                const bool keep = i < pne && hit == kNone;
+                const uint32_t pinc = warp_incl_scan(a);
+                const uint32_t ka = keep ? a : 0u;
+                const uint32_t kinc = warp_incl_scan(ka);
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
+                const uint32_t src = run_pv + pinc - a;
+                if (keep) {
+                    const uint32_t c = run_e + __popc(bal & ((1u << lane) - 1u));
+                    rec[c] = id;
+                    rar[c] = static_cast<uint8_t>(a);
+                    const uint32_t dst = run_cv + kinc - ka;
+                    for (uint32_t q = 0; q < a; ++q) rv[dst + q] = prec[pne + paw + src + q];
+                } else if (hit != kNone) {
+                    for (uint32_t q = 0; q < a; ++q)
+                        bind[R.lhs_vars[R.lhs_off[hit] + q]] = prec[pne + paw + src + q];
+                }
+                run_e += __popc(bal);
+                run_pv += __shfl_sync(0xFFFFFFFFu, pinc, 31);
+                run_cv += __shfl_sync(0xFFFFFFFFu, kinc, 31);
             }
-            // vertex offset of parent edge `lo`: sum of the arities before it
-            uint32_t vo = 0;
-            for (uint32_t i = 0; i < lo; ++i) vo += (prec[pne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
-            const uint32_t a = R.lhs_ar[lane];
-            for (uint32_t q = 0; q < a; ++q) bind[R.lhs_vars[R.lhs_off[lane] + q]] = prec[pne + paw + vo + q];
-        }
-        __syncwarp();
-        // kept parent edges
-        uint32_t run_e = 0, run_pv = 0, run_cv = 0;
-        for (uint32_t b = 0; b < pne; b += 32) {
-            const uint32_t i = b + lane;
-            uint32_t id = 0, a = 0;
-            bool keep = false;
-            if (i < pne) {
-                id = prec[i];
-                a = (prec[pne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
-                keep = true;
-                for (uint32_t k = 0; k < R.n_lhs; ++k) keep &= (cons[k] != id);
+            __syncwarp();
+            // produced edges
+            const uint32_t pid = P.ev_prod[e], fid = P.ev_fresh[e];
+            for (uint32_t k2 = lane; k2 < R.n_rhs; k2 += 32) {
+                rec[run_e + k2] = pid + k2;
+                rar[run_e + k2] = R.rhs_ar[k2];
             }
-            const uint32_t pinc = warp_incl_scan(a);
-            const uint32_t ka = keep ? a : 0u;
-            const uint32_t kinc = warp_incl_scan(ka);
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
-            if (keep) {
-                const uint32_t c = run_e + __popc(bal & ((1u << lane) - 1u));
-                rec[c] = id;
-                rar[c] = static_cast<uint8_t>(a);
-                const uint32_t src = run_pv + pinc - a, dst = run_cv + kinc - ka;
-                for (uint32_t q = 0; q < a; ++q) rv[dst + q] = prec[pne + paw + src + q];
+            for (uint32_t t = lane; t < R.rhs_total; t += 32) {
+                const uint32_t var = R.rhs_vars[t];
+                rv[run_cv + t] = ((R.new_mask >> var) & 1u) ? fid + R.fresh_rank[var] : bind[var];
             }
-            run_e += __popc(bal);
-            run_pv += __shfl_sync(0xFFFFFFFFu, pinc, 31);
-            run_cv += __shfl_sync(0xFFFFFFFFu, kinc, 31);
+            if (lane == 0) {
+                P.st_off[sid] = off;
+                P.st_ne[sid] = ne;
+                P.st_nocc[sid] = nocc;
+            }
+            __syncwarp();
         }
-        // produced edges
-        const uint32_t pid = P.ev_prod[e], fid = P.ev_fresh[e];
-        for (uint32_t k = lane; k < R.n_rhs; k += 32) {
-            rec[run_e + k] = pid + k;
-            rar[run_e + k] = R.rhs_ar[k];
-        }
-        for (uint32_t t = lane; t < R.rhs_total; t += 32) {
-            const uint32_t var = R.rhs_vars[t];
-            rv[run_cv + t] = ((R.new_mask >> var) & 1u) ? fid + R.fresh_rank[var] : bind[var];
-        }
-        if (lane == 0) {
-            P.st_off[sid] = off;
-            P.st_ne[sid] = ne;
-            P.st_nocc[sid] = nocc;
-            atomicMax(&A.level_max[0], ne);
-            atomicMax(&A.level_max[1], nocc);
-        }
-        __syncwarp();
     }
 }
 
