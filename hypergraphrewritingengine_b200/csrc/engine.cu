@@ -264,7 +264,16 @@ struct Engine::Impl {
     cudaStream_t st = nullptr;
     bool timing = false;
     StageTimes times;
-    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // the join autotuner's measurement window
+    // Join autotuner for the lane expand kernel: per bucket b = floor(log2(children per frontier
+    // state)) and variant (0 warp join, 1 lane walk), the device time per child of large levels
+    // (exponential average). Each variant is tried until it has two samples in the bucket; then
+    // the faster one runs. Small levels use the measured default (walk from 32 children/state).
+    struct JoinTuner {
+        double ns[8][2] = {};
+        uint32_t n[8][2] = {};
+    } tuner;
+    static constexpr uint64_t kTuneMinChildren = 65536;
 
     // device arrays
     DVec<DevRule> rules;
@@ -327,7 +336,8 @@ struct Engine::Impl {
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
         for (const void* k : {(const void*)k_count, (const void*)k_expand<true>,
-                              (const void*)k_expand<false>, (const void*)k_roots})
+                              (const void*)k_expand<true, true>, (const void*)k_expand<false>,
+                              (const void*)k_roots})
             HGX_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 static_cast<int>(kMaxDynSmem)));
         arena_top.ensure(1, 0, st);
@@ -1274,19 +1284,37 @@ struct Engine::Impl {
         // frontier order are cut from the level; those of the others are voided (in-range ids,
         // never kept).
         uint32_t F_eff = F;
+        bool tune = false, walk = false;   // join autotuner: measure this level / variant used
+        uint32_t bucket = 0;
         if (n_ev) {
             const uint32_t mne = std::max<uint32_t>(fmax_ne, 1), mno = std::max<uint32_t>(fmax_nocc, 1);
             const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane, fwd);
             const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp, fwd);
-            LaunchShape sl = warp_shape(k_expand<true>, Ll, F);
+            // lane kernel join: autotuned per bucket of children per frontier state (the walk
+            // amortises its count-and-emit passes over many children per state)
+            const uint64_t per_state = n_ev / std::max<uint32_t>(F, 1);
+            while (bucket < 7 && (2ull << bucket) <= per_state) ++bucket;
+            walk = per_state >= 32;
+            if (opt.lane_join == 1) walk = false;
+            else if (opt.lane_join == 2) walk = true;
+            else {
+                const uint32_t* tn = tuner.n[bucket];
+                if (tn[0] >= 2 && tn[1] >= 2) walk = tuner.ns[bucket][1] < tuner.ns[bucket][0];
+                else if (n_ev >= kTuneMinChildren) walk = tn[1] < tn[0];   // the less-sampled one
+                tune = n_ev >= kTuneMinChildren;
+            }
+            LaunchShape sl = walk ? warp_shape(k_expand<true, true>, Ll, F) : warp_shape(k_expand<true>, Ll, F);
             LaunchShape sw = warp_shape(k_expand<false>, Lw, n_ev);   // work units: slices
             auto expand = [&](uint32_t n_work) {
                 A.f_begin = 0;
                 A.f_end = n_work;
                 HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, 2 * sizeof(uint32_t), st));
                 tic();
-                k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_a, st));
+                if (walk) k_expand<true, true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                else k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 check_launch();
+                if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_b, st));
                 toc(times.expand);
                 ++times.expand_launches;
                 tic();
@@ -1325,6 +1353,7 @@ struct Engine::Impl {
                 check_launch();
                 toc(times.select);
             } else {
+                tune = false;   // rounds: several launches, no single measurement window
                 std::vector<uint32_t> h_item(NI + 1), h_fr(2 * nevo);
                 HGX_CUDA_CHECK(cudaMemcpyAsync(h_item.data(), item_ev.p, (NI + 1) * 4, cudaMemcpyDeviceToHost, st));
                 HGX_CUDA_CHECK(cudaMemcpyAsync(h_fr.data(), evo_frange.p, 2 * nevo * 4, cudaMemcpyDeviceToHost, st));
@@ -1497,6 +1526,15 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + ne2, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[3], err.p, 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (tune) {
+            float ms = 0;
+            HGX_CUDA_CHECK(cudaEventElapsedTime(&ms, ev_a, ev_b));
+            const double x = double(ms) * 1e6 / double(n_ev);
+            double& avg = tuner.ns[bucket][walk ? 1 : 0];
+            uint32_t& cnt = tuner.n[bucket][walk ? 1 : 0];
+            avg = cnt ? 0.75 * avg + 0.25 * x : x;
+            ++cnt;
+        }
         if (s2[3] & kErrTrDepth)
             throw std::invalid_argument("transitive reduction supports evolutions of at most 64 levels");
         if (s2[3]) throw std::runtime_error("hgx: device error flags 0x" + std::to_string(s2[3]));

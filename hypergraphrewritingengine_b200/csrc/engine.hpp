@@ -98,6 +98,9 @@ struct RunOptions {
     // Event canonicalisation: hgcommon EventSignatureKeys bits 0-3 (input state, output state,
     // step, rule); 0 = every application is its own event.
     uint32_t event_keys = 0;
+    // Join of the lane (small-state) expand kernel: 0 = autotuned per bucket of children per
+    // frontier state, 1 = warp join, 2 = lane-parallel walk. Results are identical.
+    uint32_t lane_join = 0;
 };
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.

@@ -1143,7 +1143,10 @@ __global__ void k_slice_counts(LevelArgs A, uint32_t n, uint32_t* cnt) {
 // hash every child; insert the hash into the dedup table. Two instantiations over the same
 // frontier range: kLane hashes the children of the states flagged by k_count one per lane,
 // the other one child per warp (states too large for a lane's private arrays).
-template <bool kLane>
+// kWalk (lane kernel only): matches of small states come from the lane-parallel join, staged in
+// shared memory; without it the warp join enumerates them into the batch directly. The two are
+// separate instantiations because the walk's code costs the other path registers and issue slots.
+template <bool kLane, bool kWalk = false>
 __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layout L) {
     extern __shared__ __align__(16) char smem[];
     char* sm = smem + (threadIdx.x >> 5) * L.bytes;
@@ -1223,7 +1226,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                 n_rounds += info.rounds;
             };
             if constexpr (kLane) {
-              if (!fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= kLaneJoinCap) {
+              if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= kLaneJoinCap) {
                 // stage the rule's matches in canonical order (lane walks: count, scan, emit),
                 // then hash them 32 at a time, one child per lane
                 uint32_t* mlist = smp<uint32_t>(sm, L.o_mlist);

@@ -88,7 +88,11 @@ typedef enum hgx_option {
        HGX_ARR_EVENT_SIG); causal and branchial edges stay over every application, as in the
        reference. The edge-rank keys (16, 32; the Automatic preset) need an exact canonical
        labelling of every state and are rejected. Default 0. */
-    HGX_OPT_EVENT_SIGNATURE_KEYS = 10
+    HGX_OPT_EVENT_SIGNATURE_KEYS = 10,
+    /* Join of the small-state expand kernel: 0 (default) = chosen per level by the engine's
+       autotuner (device time per child, per bucket of children per frontier state), 1 = warp join,
+       2 = lane-parallel walk. No reference counterpart; results are identical. */
+    HGX_OPT_LANE_JOIN = 11
 } hgx_option;
 
 /* One evolution of a batch or a served request. */

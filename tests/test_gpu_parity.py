@@ -183,3 +183,21 @@ def test_capped_rounds_match_oracle(engine, chunk_min):
             assert_same(norm_gpu(res), norm_oracle(ref), f"single {ev.name}")
     finally:
         engine.set_option(api.OPT_CHUNK_MIN, 8192)
+
+
+@pytest.mark.parametrize("join", [1, 2])
+def test_lane_join_variants_match_oracle(engine, join):
+    """Both joins of the small-state expand kernel (the autotuner's choices) give the same result."""
+    from hypergraphrewritingengine_b200 import api
+    engine.set_option(api.OPT_LANE_JOIN, join)
+    try:
+        for ev in (W.config2(6), W.config3(5)):
+            res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} join={join}")
+        evs = W.config4(n=32, max_states=1024)
+        for ev, res in zip(evs, engine.evolve_batch(evs)):
+            ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} join={join}")
+    finally:
+        engine.set_option(api.OPT_LANE_JOIN, 0)
