@@ -184,6 +184,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the batched comparison")
     ap.add_argument("--levels", type=int, default=8)
+    ap.add_argument("--lane-join", type=int, default=0, choices=[0, 1, 2],
+                    help="small-state join: 0 autotuned (default), 1 warp join, 2 lane walk")
     ap.add_argument("--profile-run", action="store_true",
                     help="run the workload once, device-resident, and exit (for profilers)")
     args = ap.parse_args()
@@ -192,8 +194,11 @@ def main():
     if args.profile_run:
         from hypergraphrewritingengine_b200 import Engine
         from hypergraphrewritingengine_b200 import workloads as W
+        from hypergraphrewritingengine_b200 import api
         ev = W.config2(args.levels)
-        c = Engine(0).counts(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+        eng = Engine(0)
+        eng.set_option(api.OPT_LANE_JOIN, args.lane_join)
+        c = eng.counts(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
         print(json.dumps(c))
         return
 
@@ -214,6 +219,8 @@ def main():
 
     ev = W.config2(args.levels)
     eng = Engine(local)
+    from hypergraphrewritingengine_b200 import api as _api
+    eng.set_option(_api.OPT_LANE_JOIN, args.lane_join)
     stream = torch.cuda.ExternalStream(eng.stream(), device=torch.device("cuda", local))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")   # 256 MB > 126 MB L2
 
@@ -229,7 +236,7 @@ def main():
     from hypergraphrewritingengine_b200 import api
     eng.set_option(api.OPT_TIMING, 1)
     expand_ms = 0.0
-    expand_launches = 0
+    expand_launches = walk_launches = 0
     stage_bytes = hbm_bytes = children = rounds = 0
     launches = 0
     step_ms = []
@@ -249,6 +256,7 @@ def main():
             xs = eng.expand_stats()
             expand_ms += st["expand"]
             expand_launches += xs["launches"]
+            walk_launches += xs["walk_launches"]
             stage_bytes += xs["stage_bytes"]
             hbm_bytes += xs["hbm_bytes"]
             children += xs["children"]
@@ -308,6 +316,8 @@ def main():
                      "algorithmic_bytes_per_launch": per_launch_bytes,
                      "fused_hbm_bytes_per_launch": hbm_bytes / max(expand_launches, 1),
                      "launch_ms": per_launch_s * 1e3, "launches": expand_launches,
+                     "lane_join": {"walk_launches": walk_launches,
+                                   "warp_join_launches": expand_launches - walk_launches},
                      "children_hashed": children, "wl_rounds": rounds,
                      "stage_ms_last_step": {k: round(v, 3) for k, v in st.items()}},
         "gpu_launches": int(launches),

@@ -369,11 +369,11 @@ class Engine:
         return int(b.value)
 
     def expand_stats(self):
-        out = (ctypes.c_uint64 * 10)()
+        out = (ctypes.c_uint64 * 11)()
         _check(self._L.hgx_engine_expand_stats(self._h, out))
         return dict(zip(("stage_bytes", "hbm_bytes", "children", "wl_rounds", "launches",
                          "warp_stage_bytes", "warp_hbm_bytes", "warp_children", "warp_rounds",
-                         "warp_ns"), list(out)))
+                         "warp_ns", "walk_launches"), list(out)))
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

@@ -414,6 +414,7 @@ hgx_status hgx_engine_expand_stats(hgx_engine* e, uint64_t* out) {
     out[7] = t.warp_children;
     out[8] = t.warp_rounds;
     out[9] = static_cast<uint64_t>(t.expand_warp * 1e6);   // warp kernel time, ns
+    out[10] = t.walk_launches;
     return HGX_OK;
 }
 

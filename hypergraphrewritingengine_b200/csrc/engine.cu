@@ -267,8 +267,9 @@ struct Engine::Impl {
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // the join autotuner's measurement window
     // Join autotuner for the lane expand kernel: per bucket b = floor(log2(children per frontier
     // state)) and variant (0 warp join, 1 lane walk), the device time per child of large levels
-    // (exponential average). Each variant is tried until it has two samples in the bucket; then
-    // the faster one runs. Small levels use the measured default (walk from 32 children/state).
+    // (exponential average). Each variant is tried once in the bucket; then the faster one runs
+    // (and keeps being measured). Small levels use the measured default (walk from 32
+    // children/state).
     struct JoinTuner {
         double ns[8][2] = {};
         uint32_t n[8][2] = {};
@@ -1299,7 +1300,7 @@ struct Engine::Impl {
             else if (opt.lane_join == 2) walk = true;
             else {
                 const uint32_t* tn = tuner.n[bucket];
-                if (tn[0] >= 2 && tn[1] >= 2) walk = tuner.ns[bucket][1] < tuner.ns[bucket][0];
+                if (tn[0] >= 1 && tn[1] >= 1) walk = tuner.ns[bucket][1] < tuner.ns[bucket][0];
                 else if (n_ev >= kTuneMinChildren) walk = tn[1] < tn[0];   // the less-sampled one
                 tune = n_ev >= kTuneMinChildren;
             }
@@ -1317,6 +1318,7 @@ struct Engine::Impl {
                 if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_b, st));
                 toc(times.expand);
                 ++times.expand_launches;
+                if (walk) ++times.walk_launches;
                 tic();
                 slice_off.ensure(uint64_t(n_work) + 1, 0, st);
                 k_slice_counts<<<grid_for(n_work, 256), 256, 0, st>>>(A, n_work, slice_off.p);

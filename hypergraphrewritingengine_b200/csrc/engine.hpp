@@ -109,6 +109,7 @@ struct StageTimes {
            branchial = 0, roots = 0, total = 0;
     uint64_t launches = 0;   // kernels this engine launched during the run
     uint64_t expand_launches = 0;
+    uint64_t walk_launches = 0;      // lane-kernel launches that used the lane-parallel walk
     // lane-per-child expand kernel (k_expand<true>)
     uint64_t expand_bytes = 0;       // per-stage algorithmic bytes
     uint64_t expand_hbm_bytes = 0;   // bytes the fused kernel must move to/from HBM

@@ -211,7 +211,8 @@ HGX_API hgx_status hgx_engine_stage_times(hgx_engine* engine, double* out_ms, ui
    kernels). out[0..4], lane-per-child kernel: bytes by the per-stage figures (join + rewrite +
    WL + dedup counted as separate HBM streams), bytes the fused kernel itself must move to or
    from HBM, children hashed, WL refinement rounds, launches. out[5..8], warp-per-child kernel:
-   the same first four figures; out[9] its total device time in nanoseconds. */
+   the same first four figures; out[9] its total device time in nanoseconds; out[10] lane-kernel
+   launches that ran the lane-parallel walk (the join autotuner's choice; out has 11 entries). */
 HGX_API hgx_status hgx_engine_expand_stats(hgx_engine* engine, uint64_t* out);
 
 /* The CUDA stream (cudaStream_t) the engine launches on, for callers that time or order
