@@ -104,7 +104,9 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
     info.nbr = nbr;
     if (nv == 0) return 0;
 
-    uint64_t cur[VM], nxt[VM], buf[NM];
+    uint64_t cura[VM], curb[VM], buf[NM];
+    uint64_t* cur = cura;   // this round's colours
+    uint64_t* nxt = curb;   // the next round's (the two swap every round)
     // initial colours
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
@@ -168,8 +170,9 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
             for (uint32_t j = 0; j < n; ++j) h = fnv(h, buf[j]);
             nxt[v] = h;
         }
-                #pragma unroll 1
-        for (uint32_t v = 0; v < V; ++v) cur[v] = nxt[v];
+        uint64_t* t = cur;
+        cur = nxt;
+        nxt = t;
         const uint32_t d = lane_distinct<VM>(cur, deg, V);
         ++info.rounds;
         if (d == prev) break;
@@ -230,8 +233,14 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[prodv[o + q]]);
         es += smix(h);
     }
+    // one component (the usual case): its term folds every vertex and edge, no per-root scans
+    uint32_t roots = 0;
         #pragma unroll 1
-    for (uint32_t r = 0; r < V; ++r) {
+    for (uint32_t v = 0; v < V; ++v) roots += (deg[v] && comp[v] == v) ? 1u : 0u;
+    if (roots == 1)
+        cs = smix(fnv(fnv(kFnvOffset, (static_cast<uint64_t>(ne) << 32) | nv), vs));
+        #pragma unroll 1
+    for (uint32_t r = 0; r < V && roots != 1; ++r) {
         if (!deg[r] || comp[r] != r) continue;
         uint64_t col = 0, vc = 0, ec = 0;
                 #pragma unroll 1
