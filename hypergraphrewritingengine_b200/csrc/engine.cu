@@ -194,9 +194,9 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.o_vtid = take(2 * L.VT, 2);
     }
     if (wl) {
-        uint32_t n2 = 64;
-        while (n2 < L.V) n2 <<= 1;
-        L.o_srt = take(8 * n2, 8);
+        uint32_t n2 = 64;   // distinct-colour hash set: >= 2 slots per vertex, + a zero flag
+        while (n2 < 2 * L.V) n2 <<= 1;
+        L.o_srt = take(8 * (n2 + 1), 8);
     }
     if (lane) {
         L.SB = rm.lhs + rm.rhs_total;

@@ -530,27 +530,33 @@ __device__ uint32_t wl_distinct(const uint64_t* cur, const uint32_t* deg, uint32
         }
         return __popc(__ballot_sync(0xFFFFFFFFu, lead));
     }
-    // bitonic sort of the present colours (absent ones padded with the maximum), then count
-    // the distinct values among the first nv
+    // a shared-memory hash set of the present colours (>= 2 slots per vertex, linear probing,
+    // key 0 = empty; colour 0 itself is a flag in the slot after the table): every first insert
+    // of a colour counts once
+    (void)nv;
     uint32_t n2 = 64;
-    while (n2 < V) n2 <<= 1;
-    for (uint32_t i = lane; i < n2; i += 32) srt[i] = (i < V && deg[i]) ? cur[i] : ~0ull;
+    while (n2 < 2 * V) n2 <<= 1;
+    for (uint32_t i = lane; i <= n2; i += 32) srt[i] = 0;
     __syncwarp();
-    for (uint32_t k = 2; k <= n2; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = lane; i < n2; i += 32) {
-                const uint32_t l = i ^ j;
-                if (l > i) {
-                    const uint64_t a = srt[i], b = srt[l];
-                    if ((a > b) == ((i & k) == 0)) { srt[i] = b; srt[l] = a; }
-                }
-            }
-            __syncwarp();
+    uint32_t d = 0;
+    for (uint32_t v = lane; v < V; v += 32) {
+        if (!deg[v]) continue;
+        const unsigned long long c = cur[v];
+        if (c == 0) {
+            d += atomicExch(reinterpret_cast<unsigned long long*>(&srt[n2]), 1ull) == 0 ? 1u : 0u;
+            continue;
+        }
+        uint32_t slot = static_cast<uint32_t>(smix(c)) & (n2 - 1);
+        for (uint32_t probe = 0; probe < n2; ++probe) {
+            const unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long*>(&srt[slot]), 0ull, c);
+            if (old == 0) { ++d; break; }
+            if (old == c) break;
+            slot = (slot + 1) & (n2 - 1);
         }
     }
-    uint32_t d = 0;
-    for (uint32_t i = lane; i < nv; i += 32) d += (i == 0 || srt[i] != srt[i - 1]) ? 1u : 0u;
-    return warp_sum32(d);
+    const uint32_t total = warp_sum32(d);
+    __syncwarp();
+    return total;
 }
 
 __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, WlInfo& info) {
@@ -693,13 +699,19 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, 
         }
     }
     __syncwarp();
+    // one component (the usual case): its term folds every vertex and edge, so the per-root
+    // sums -- shared-memory atomics that would all hit the one root -- are skipped
+    uint32_t nroots = 0;
+    for (uint32_t v = lane; v < V; v += 32) nroots += (deg[v] && comp[v] == v) ? 1u : 0u;
+    const bool one = warp_sum32(nroots) == 1;
     uint64_t vs = 0, es = 0, cs = 0;
     for (uint32_t v = lane; v < V; v += 32) {
         if (!deg[v]) continue;
-        uint32_t r = v;
-        while (comp[r] != r) r = comp[r];
         const uint64_t m = smix(cur[v]);
         vs += m;
+        if (one) continue;
+        uint32_t r = v;
+        while (comp[r] != r) r = comp[r];
         atomicAdd(reinterpret_cast<unsigned long long*>(&csum[r]), static_cast<unsigned long long>(m));
         atomicAdd(reinterpret_cast<unsigned long long*>(&ccnt[r]), 1ull);
     }
@@ -708,18 +720,20 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, 
         uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(a));
         for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[vloc[vo + q]]);
         es += smix(h);
-        if (a) {
+        if (a && !one) {
             uint32_t r = vloc[vo];
             while (comp[r] != r) r = comp[r];
             atomicAdd(reinterpret_cast<unsigned long long*>(&ccnt[r]), 1ull << 32);
         }
     }
     __syncwarp();
-    for (uint32_t v = lane; v < V; v += 32)
-        if (deg[v] && comp[v] == v) cs += smix(fnv(fnv(kFnvOffset, ccnt[v]), csum[v]));
+    if (!one)
+        for (uint32_t v = lane; v < V; v += 32)
+            if (deg[v] && comp[v] == v) cs += smix(fnv(fnv(kFnvOffset, ccnt[v]), csum[v]));
     vs = warp_sum64(vs);
     es = warp_sum64(es);
-    cs = warp_sum64(cs);
+    cs = one ? smix(fnv(fnv(kFnvOffset, (static_cast<uint64_t>(ne) << 32) | nv), vs))
+             : warp_sum64(cs);
     uint64_t h = kFnvOffset;
     h = fnv(h, nv);
     h = fnv(h, ne);
