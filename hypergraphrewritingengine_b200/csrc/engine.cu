@@ -291,7 +291,7 @@ struct Engine::Impl {
     DVec<unsigned long long> tab_keys;
     DVec<uint32_t> tab_vals;
     DVec<unsigned long long> evo_classes, evo_states;
-    DVec<uint32_t> evo_cut, evo_first_ev, evo_last_ev, evo_stopped, evo_front;
+    DVec<uint32_t> evo_cut, evo_first_ev, evo_last_ev, evo_stopped;
     DVec<uint32_t> err;
     // level temporaries
     DVec<uint32_t> frontier, next_frontier, counts, item_ev, item_cons, item_prod, item_fresh;
@@ -358,7 +358,7 @@ struct Engine::Impl {
                  &edge_creator, &ev_in,
                  &ev_rule, &ev_coff, &ev_prod, &ev_fresh, &ev_out, &ev_cons, &ev_cprod,
                  &state_of_arrival, &tab_vals, &evo_cut, &evo_first_ev, &evo_last_ev,
-                 &evo_stopped, &evo_front, &err, &frontier, &next_frontier, &counts, &item_ev,
+                 &evo_stopped, &err, &frontier, &next_frontier, &counts, &item_ev,
                  &item_cons, &item_prod, &item_fresh, &work, &flag_new, &scan_new, &flag_rep,
                  &flag_front, &new_state_event, &level_max, &bcount, &boff, &bpairs, &scan_sums,
                  &sync_buf, &root_ids})
@@ -699,7 +699,6 @@ struct Engine::Impl {
         evo_first_ev.ensure(nevo, evo0, st);
         evo_last_ev.ensure(nevo, evo0, st);
         evo_stopped.ensure(nevo, evo0, st);
-        evo_front.ensure(nevo, evo0, st);
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_classes.p + evo0, 0, nnew * sizeof(unsigned long long), st));
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_states.p + evo0, 0, nnew * sizeof(unsigned long long), st));
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_cut.p + evo0, 0xFF, nnew * sizeof(uint32_t), st));
@@ -1511,15 +1510,15 @@ struct Engine::Impl {
         // per-evolution ranges of this level (events kept, new states, branchial pairs)
         A.state_base = static_cast<uint32_t>(n_states);
         A.bbase = static_cast<uint32_t>(n_bpairs);
-        lvl_ranges.ensure(6 * nevo, 0, st);
+        lvl_ranges.ensure(7 * nevo, 0, st);
         if (ne2 || F_eff) {
             A.n_frontier = F;   // boundaries over the whole frontier; event ranges clamp to ne2
             k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, lvl_ranges.p);
             check_launch();
             A.n_frontier = F_eff;
         }
-        std::vector<uint32_t> h_rng(6 * nevo);
-        HGX_CUDA_CHECK(cudaMemcpyAsync(h_rng.data(), lvl_ranges.p, 6 * nevo * 4, cudaMemcpyDeviceToHost, st));
+        std::vector<uint32_t> h_rng(7 * nevo);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(h_rng.data(), lvl_ranges.p, 7 * nevo * 4, cudaMemcpyDeviceToHost, st));
 
         // ---- sync 2: new states, next frontier, branchial pairs, errors
         uint32_t s2[4];
@@ -1543,7 +1542,7 @@ struct Engine::Impl {
         const uint32_t n_new = s2[0], n_front = s2[1], n_b = s2[2];
         for (size_t e = 0; e < nevo; ++e) {
             if (evo_done[e] || h_first[e] == kNone) continue;
-            const uint32_t* q = &h_rng[6 * e];
+            const uint32_t* q = &h_rng[7 * e];
             // ranges must lie inside what this level produced
             if (q[0] > q[1] || q[1] > n_events + ne2 || q[2] > q[3] || q[3] > n_states + n_new ||
                 q[4] > q[5] || q[5] > n_bpairs + n_b)
@@ -1594,20 +1593,9 @@ struct Engine::Impl {
             toc(times.branchial);
         }
 
-        // which evolutions still have a frontier
-        std::vector<uint8_t> present(nevo, 0);
-        if (n_front) {
-            evo_front.ensure(nevo, 0, st);
-            HGX_CUDA_CHECK(cudaMemsetAsync(evo_front.p, 0, nevo * 4, st));
-            k_mark_front<<<grid_for(n_front, 256), 256, 0, st>>>(ptrs(), next_frontier.p, n_front, evo_front.p);
-            check_launch();
-            std::vector<uint32_t> hf(nevo);
-            HGX_CUDA_CHECK(cudaMemcpyAsync(hf.data(), evo_front.p, nevo * 4, cudaMemcpyDeviceToHost, st));
-            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-            for (size_t e = 0; e < nevo; ++e) present[e] = hf[e] ? 1 : 0;
-        }
+        // which evolutions still have a frontier (their next-frontier counts came with sync 2)
         for (size_t e = 0; e < nevo; ++e)
-            if (!evo_done[e] && h_first[e] != kNone && !present[e]) {
+            if (!evo_done[e] && h_first[e] != kNone && h_rng[7 * e + 6] == 0) {
                 evo_done[e] = 1;
                 finished.push_back(static_cast<uint32_t>(e));
             }

@@ -1450,7 +1450,8 @@ __global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t
 
 // Per evolution of the level: its kept events, its new states and its branchial pairs are each
 // one contiguous range (the frontier is grouped by evolution and everything is numbered in
-// frontier order). out[evo * 6 + {0..5}] = event first/end, state first/end, pair first/end.
+// frontier order). out[evo * 7 + {0..6}] = event first/end, state first/end, pair first/end, and
+// the evolution's states in the next frontier.
 __global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last, uint32_t* out) {
     for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
          f += gridDim.x * blockDim.x) {
@@ -1459,13 +1460,14 @@ __global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last, u
         const uint32_t e0 = P.evo_first_ev[evo];
         uint32_t e1 = min(evo_last[evo], A.ev_base + A.n_events);
         e1 = max(e0, min(e1, P.evo_cut[evo]));
-        uint32_t* o = out + 6ull * evo;
+        uint32_t* o = out + 7ull * evo;
         o[0] = e0;
         o[1] = e1;
         o[2] = A.state_base + A.flag_rep[e0 - A.ev_base];
         o[3] = A.state_base + A.flag_rep[e1 - A.ev_base];
         o[4] = A.bbase + A.boff[e0 - A.ev_base];
         o[5] = A.bbase + A.boff[e1 - A.ev_base];
+        o[6] = A.flag_front[e1 - A.ev_base] - A.flag_front[e0 - A.ev_base];
     }
 }
 
@@ -1627,12 +1629,6 @@ __global__ void k_rehash(unsigned long long* keys, uint32_t* vals, uint64_t old_
         }
         if (!done) atomicOr(err, kErrTableFull);
     }
-}
-
-// Mark the evolutions that still have states to expand.
-__global__ void k_mark_front(DevPtrs P, const uint32_t* front, uint32_t n, uint32_t* mark) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        mark[P.st_evo[front[i]]] = 1;
 }
 
 // Is the child the first arrival of its WL class? (winner stored in ev_out until resolved)
