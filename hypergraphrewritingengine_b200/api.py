@@ -49,7 +49,8 @@ EXPORTS = (
     "hgx_last_error", "hgx_version", "hgx_engine_create", "hgx_engine_destroy",
     "hgx_engine_add_rule", "hgx_engine_clear_rules", "hgx_engine_set_option", "hgx_evolve",
     "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_admit_batch", "hgx_serve_step",
-    "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_device_bytes", "hgx_result_count",
+    "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_collect_batch", "hgx_serve_device_bytes",
+    "hgx_result_count",
     "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
     "hgx_engine_stream", "hgx_hash_states_noalloc", "hgx_result_view",
 )
@@ -97,6 +98,7 @@ def load_library(path: str = LIB_PATH):
         "hgx_serve_step": ([vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
         "hgx_serve_take_finished": ([vp, u32p, ctypes.c_uint32, u32p], ctypes.c_int),
         "hgx_serve_collect": ([vp, ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
+        "hgx_serve_collect_batch": ([vp, u32p, ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
         "hgx_serve_device_bytes": ([vp, u64p], ctypes.c_int),
         "hgx_result_count": ([vp, ctypes.c_int], ctypes.c_uint64),
         "hgx_result_copy": ([vp, ctypes.c_int, vp, ctypes.c_size_t], ctypes.c_int),
@@ -362,6 +364,16 @@ class Engine:
         out = ctypes.c_void_p()
         _check(self._L.hgx_serve_collect(self._h, int(evo), ctypes.byref(out)))
         return _read_result(out.value)
+
+    def serve_collect_batch(self, evos) -> list:
+        """Collect several finished evolutions with one device finalisation and one copy."""
+        n = len(evos)
+        if n == 0:
+            return []
+        ids = (ctypes.c_uint32 * n)(*[int(e) for e in evos])
+        outs = (ctypes.c_void_p * n)()
+        _check(self._L.hgx_serve_collect_batch(self._h, ids, n, outs))
+        return [_read_result(outs[i]) for i in range(n)]
 
     def device_bytes(self) -> int:
         b = ctypes.c_uint64()

@@ -320,6 +320,15 @@ hgx_status hgx_serve_take_finished(hgx_engine* e, uint32_t* ids, uint32_t cap, u
     });
 }
 
+hgx_status hgx_serve_collect_batch(hgx_engine* e, const uint32_t* ids, uint32_t n, hgx_result** out) {
+    if (!e || (n && (!ids || !out))) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        auto res = e->engine.collect(std::vector<uint32_t>(ids, ids + n), e->opt);
+        for (uint32_t i = 0; i < n; ++i) out[i] = wrap(std::move(res[i]));
+        return HGX_OK;
+    });
+}
+
 hgx_status hgx_serve_collect(hgx_engine* e, uint32_t evo, hgx_result** out) {
     if (!e || !out) return fail(HGX_ERR_INVALID, "null argument");
     return guarded([&] {

@@ -302,6 +302,8 @@ struct Engine::Impl {
     DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e, frng, slice_off;
     DVec<unsigned long long> evo_new, ev_anc, ev_sig, evo_sigs;
     DVec<uint64_t> fin_rng;
+    DVec<uint32_t> fin_tab;   // many-evolution finalisation: bases, rule starts, boundary values
+    DVec<uint64_t> fin_sec;   // many-evolution finalisation: section offsets
     // Per evolution: the contiguous id ranges it owns, one entry per level (roots first).
     struct EvoRanges {
         std::vector<std::pair<uint32_t, uint32_t>> states, events;
@@ -388,7 +390,8 @@ struct Engine::Impl {
         map_s.release(st);
         map_e.release(st);
         fin_rng.release(st);
-        causal_scratch.release(st);
+        fin_tab.release(st);
+        fin_sec.release(st);
         rules.release(st);
         evos.release(st);
         cudaStreamSynchronize(st);
@@ -811,8 +814,6 @@ struct Engine::Impl {
                                            cudaMemcpyHostToDevice, st));
     }
 
-    void read_results(const std::vector<uint32_t>& which, const RunOptions& opt,
-                      std::vector<EvolutionResult>& out);
 
 
     // Single-evolution result, finalised on the device and copied to a pinned block at once.
@@ -949,147 +950,186 @@ struct Engine::Impl {
     }
 
 
-    // One evolution of many, finalised on the device from its recorded id ranges.
-    EvolutionResult finalize_evo(uint32_t evo, const RunOptions& opt) {
-        EvolutionResult r;
-        const EvoRanges& er = evo_ranges.at(evo);
-        std::vector<uint32_t> ids;
-        for (auto& q : er.states) for (uint32_t i = q.first; i < q.second; ++i) ids.push_back(i);
-        const uint32_t S = static_cast<uint32_t>(ids.size());
-        for (auto& q : er.events) for (uint32_t i = q.first; i < q.second; ++i) ids.push_back(i);
-        const uint32_t E = static_cast<uint32_t>(ids.size()) - S;
-        std::vector<uint64_t> rng;   // pair ranges: starts, then cumulative counts
-        uint64_t B = 0;
-        for (auto& q : er.pairs) rng.push_back(q.first);
-        for (auto& q : er.pairs) { rng.push_back(B); B += q.second - q.first; }
-        const uint32_t NR = static_cast<uint32_t>(er.pairs.size());
-        fin_ids.ensure(ids.size() + 1, 0, st);
-        HGX_CUDA_CHECK(cudaMemcpyAsync(fin_ids.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
-        const uint32_t* sids = fin_ids.p;
-        const uint32_t* eids = fin_ids.p + S;
+    // Many evolutions finalised on the device at once, from their recorded id ranges: one set of
+    // launches, one staging block, one copy into one page-locked block that every result shares.
+    std::vector<EvolutionResult> finalize_many(const std::vector<uint32_t>& which, const RunOptions& opt) {
+        const uint32_t K = static_cast<uint32_t>(which.size());
+        std::vector<EvolutionResult> out(K);
+        if (!K) return out;
+        const bool se = opt.keep_state_edges, sg = opt.event_keys != 0;
+        // concatenated id ranges (states, events, pairs) and each evolution's start in them
+        std::vector<uint64_t> rs, rc, re, rce, rp, rcp;
+        std::vector<uint32_t> tab(4 * (K + 1) + K, 0);
+        uint32_t* sb = tab.data();
+        uint32_t* eb = sb + (K + 1);
+        uint32_t* pb = eb + (K + 1);
+        uint32_t* rb = pb + (K + 1);
+        uint64_t S = 0, E = 0, B = 0;
+        for (uint32_t k = 0; k < K; ++k) {
+            const EvoRanges& er = evo_ranges.at(which[k]);
+            sb[k] = static_cast<uint32_t>(S);
+            eb[k] = static_cast<uint32_t>(E);
+            pb[k] = static_cast<uint32_t>(B);
+            rb[k] = h_evos[which[k]].rule_begin;
+            for (auto& q : er.states) { rs.push_back(q.first); rc.push_back(S); S += q.second - q.first; }
+            for (auto& q : er.events) { re.push_back(q.first); rce.push_back(E); E += q.second - q.first; }
+            if (opt.branchial)
+                for (auto& q : er.pairs) { rp.push_back(q.first); rcp.push_back(B); B += q.second - q.first; }
+        }
+        if (S + E >= 0xFFFFFFF0ull || B >= 0xFFFFFFF0ull)
+            throw std::runtime_error("hgx: result too large for one finalisation");
+        sb[K] = static_cast<uint32_t>(S);
+        eb[K] = static_cast<uint32_t>(E);
+        pb[K] = static_cast<uint32_t>(B);
+        const uint32_t NS = static_cast<uint32_t>(S), NE = static_cast<uint32_t>(E);
+        // device tables: ranges (u64) and bases (u32)
+        std::vector<uint64_t> rng;
+        const uint64_t o_rs = 0, o_rc = rs.size(), o_re = 2 * rs.size(), o_rce = o_re + re.size(),
+                       o_rp = o_rce + re.size(), o_rcp = o_rp + rp.size();
+        rng.reserve(o_rcp + rp.size());
+        for (auto* v : {&rs, &rc, &re, &rce, &rp, &rcp}) rng.insert(rng.end(), v->begin(), v->end());
+        fin_rng.ensure(std::max<size_t>(rng.size(), 1), 0, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(fin_rng.p, rng.data(), rng.size() * 8, cudaMemcpyHostToDevice, st));
+        fin_tab.ensure(tab.size() + 4 * (K + 1), 0, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(fin_tab.p, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, st));
+        const uint32_t* d_sb = fin_tab.p;
+        const uint32_t* d_eb = d_sb + (K + 1);
+        const uint32_t* d_pb = d_eb + (K + 1);
+        const uint32_t* d_rb = d_pb + (K + 1);
+        uint32_t* d_bounds = fin_tab.p + tab.size();
+        // ids, global -> local maps
+        fin_ids.ensure(S + E + 1, 0, st);
+        uint32_t* sids = fin_ids.p;
+        uint32_t* eids = fin_ids.p + S;
+        k_expand_ranges<<<grid_for(S, 256), 256, 0, st>>>(fin_rng.p + o_rs, fin_rng.p + o_rc,
+                                                          static_cast<uint32_t>(rs.size()), S, sids);
+        check_launch();
+        if (E) {
+            k_expand_ranges<<<grid_for(E, 256), 256, 0, st>>>(fin_rng.p + o_re, fin_rng.p + o_rce,
+                                                              static_cast<uint32_t>(re.size()), E, eids);
+            check_launch();
+        }
         map_s.ensure(n_states, 0, st);
         map_e.ensure(n_events, 0, st);
-        k_map_ids<<<grid_for(S, 256), 256, 0, st>>>(sids, S, map_s.p);
+        k_map_multi<<<grid_for(S, 256), 256, 0, st>>>(sids, NS, d_sb, K, map_s.p);
         check_launch();
         if (E) {
-            k_map_ids<<<grid_for(E, 256), 256, 0, st>>>(eids, E, map_e.p);
+            k_map_multi<<<grid_for(E, 256), 256, 0, st>>>(eids, NE, d_eb, K, map_e.p);
             check_launch();
         }
-        // counts: ne / nocc per state, consumed / causal per event, then their scans
-        fin_cnt.ensure(4ull * (S + 1) + 4ull * (E + 1), 0, st);
-        uint32_t* sne = fin_cnt.p;               // [S+1] -> eoff
-        uint32_t* sno = sne + S + 1;             // [S+1] -> voff
-        uint32_t* ecc = sno + S + 1;             // [E+1] -> coff
-        uint32_t* ekc = ecc + E + 1;             // [E+1] -> koff
-        const bool se = opt.keep_state_edges;
-        // gathered hashes + depths at the front of `fin`; the staging block after them starts on
-        // a 16-byte boundary (its sections hold u64 arrays written by kernels)
-        const uint64_t hbytes = (8ull * S + 4ull * S + 15) / 16 * 16;
-        fin.ensure(std::max<uint64_t>(hbytes, 16), 0, st);
-        k_gather_states<<<grid_for(S, 256), 256, 0, st>>>(ptrs(), sids, S, reinterpret_cast<uint64_t*>(fin.p),
-                                                          reinterpret_cast<uint32_t*>(fin.p + 8ull * S), sne, sno);
+        // sizes and their scans: state edges / occurrences, event consumed / causal entries
+        fin_cnt.ensure(2ull * (S + 1) + 2ull * (E + 1), 0, st);
+        uint32_t* sne = fin_cnt.p;
+        uint32_t* sno = sne + S + 1;
+        uint32_t* ecc = sno + S + 1;
+        uint32_t* ekc = ecc + E + 1;
+        k_fin_states_multi<<<grid_for(S, 256), 256, 0, st>>>(ptrs(), sids, NS, d_sb, K, nullptr, nullptr, sne, sno);
         check_launch();
-        scan(sne, sne, S);
-        scan(sno, sno, S);
+        scan(sne, sne, NS);
+        scan(sno, sno, NS);
         if (E) {
-            k_gather_events<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), eids, E, h_evos[evo].rule_begin,
-                                                              map_s.p, map_e.p, ecc, ekc, nullptr, nullptr,
-                                                              nullptr, nullptr, nullptr, nullptr, 0);
+            k_fin_events_multi<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), eids, NE, d_eb, K, d_rb, map_s.p, map_e.p,
+                                                                 ecc, ekc, nullptr, nullptr, nullptr, nullptr,
+                                                                 0, opt.causal ? 1 : 0, 0);
             check_launch();
         }
-        scan(ecc, ecc, E);
-        scan(ekc, ekc, E);
-        uint32_t T = 0, V = 0, C = 0, K = 0, stopped = 0;
-        unsigned long long classes = 0;
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&T, sne + S, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&V, sno + S, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&C, ecc + E, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&K, ekc + E, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&stopped, evo_stopped.p + evo, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&classes, evo_classes.p + evo, 8, cudaMemcpyDeviceToHost, st));
+        scan(ecc, ecc, NE);
+        scan(ekc, ekc, NE);
+        k_fin_bounds<<<grid_for(K + 1, 256), 256, 0, st>>>(sne, d_sb, K, d_bounds);
+        k_fin_bounds<<<grid_for(K + 1, 256), 256, 0, st>>>(sno, d_sb, K, d_bounds + (K + 1));
+        k_fin_bounds<<<grid_for(K + 1, 256), 256, 0, st>>>(ecc, d_eb, K, d_bounds + 2 * (K + 1));
+        k_fin_bounds<<<grid_for(K + 1, 256), 256, 0, st>>>(ekc, d_eb, K, d_bounds + 3 * (K + 1));
+        check_launch();
+        std::vector<uint32_t> bnd(4 * (K + 1));
+        const size_t nevo = h_evos.size();
+        std::vector<unsigned long long> cls(nevo), sigs(nevo, 0);
+        std::vector<uint32_t> stop(nevo);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(bnd.data(), d_bounds, bnd.size() * 4, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(cls.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(stop.data(), evo_stopped.p, nevo * 4, cudaMemcpyDeviceToHost, st));
+        if (sg) HGX_CUDA_CHECK(cudaMemcpyAsync(sigs.data(), evo_sigs.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-        if (!opt.causal) K = 0;
-        const bool sg = opt.event_keys != 0;
-        unsigned long long nsig = E;
-        if (sg) {
-            HGX_CUDA_CHECK(cudaMemcpyAsync(&nsig, evo_sigs.p + evo, 8, cudaMemcpyDeviceToHost, st));
-            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-        }
-        uint64_t count[ResultArrays::kArrays] = {
-            S, S, 4ull * E, 3ull * K, 2 * B, uint64_t(E) + 1, C, 2ull * E,
-            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0, sg ? E : 0};
-        uint64_t off[ResultArrays::kArrays];
+        // sections: each evolution's arrays, in hgx_array order, 16-byte aligned
+        std::vector<uint64_t> sec(uint64_t(K) * kArr), cnt(uint64_t(K) * kArr);
         uint64_t total = 0;
-        for (int i = 0; i < ResultArrays::kArrays; ++i) {
-            off[i] = total;
-            total += (count[i] * arr_elem_bytes(i) + 15) / 16 * 16;
+        for (uint32_t k = 0; k < K; ++k) {
+            const uint64_t Sk = sb[k + 1] - sb[k], Ek = eb[k + 1] - eb[k], Bk = pb[k + 1] - pb[k];
+            const uint64_t Tk = bnd[k + 1] - bnd[k], Vk = bnd[K + 1 + k + 1] - bnd[K + 1 + k];
+            const uint64_t Ck = bnd[2 * (K + 1) + k + 1] - bnd[2 * (K + 1) + k];
+            const uint64_t Kk = bnd[3 * (K + 1) + k + 1] - bnd[3 * (K + 1) + k];
+            const uint64_t c[kArr] = {Sk, Sk, 4 * Ek, 3 * Kk, 2 * Bk, Ek + 1, Ck, 2 * Ek,
+                                      se ? Sk + 1 : 1, se ? Tk : 0, se ? Tk : 0, se ? Sk + 1 : 1,
+                                      se ? Vk : 0, sg ? Ek : 0};
+            for (uint32_t a = 0; a < kArr; ++a) {
+                sec[uint64_t(k) * kArr + a] = total;
+                cnt[uint64_t(k) * kArr + a] = c[a];
+                total += (c[a] * arr_elem_bytes(static_cast<int>(a)) + 15) / 16 * 16;
+            }
         }
-        // staging: hashes/depths were gathered at the front of `fin`; move them into place
-        fin.ensure(total + hbytes, hbytes, st);
-        uint8_t* d = fin.p + hbytes;
-        auto dp = [&](int i) { return reinterpret_cast<uint32_t*>(d + off[i]); };
-        HGX_CUDA_CHECK(cudaMemcpyAsync(d + off[0], fin.p, 8ull * S, cudaMemcpyDeviceToDevice, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(d + off[1], fin.p + 8ull * S, 4ull * S, cudaMemcpyDeviceToDevice, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(dp(5), ecc, 4ull * (E + 1), cudaMemcpyDeviceToDevice, st));
-        if (E) {
-            k_gather_events<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), eids, E, h_evos[evo].rule_begin,
-                                                              map_s.p, map_e.p, nullptr, nullptr, ecc, ekc,
-                                                              dp(2), dp(6), dp(7),
-                                                              opt.causal ? dp(3) : fin_scratch_causal(K), 1);
+        fin.ensure(std::max<uint64_t>(total, 16), 0, st);
+        fin_sec.ensure(sec.size(), 0, st);
+        HGX_CUDA_CHECK(cudaMemcpyAsync(fin_sec.p, sec.data(), sec.size() * 8, cudaMemcpyHostToDevice, st));
+        uint8_t* stage = fin.p;
+        const uint64_t* d_sec = fin_sec.p;
+        // emit
+        k_fin_states_multi<<<grid_for(S, 256), 256, 0, st>>>(ptrs(), sids, NS, d_sb, K, stage, d_sec, nullptr, nullptr);
+        check_launch();
+        if (se) {
+            k_fin_offsets_multi<<<grid_for(S + K, 256), 256, 0, st>>>(sne, NS, d_sb, K, stage, d_sec, HGX_ARR_STATE_EDGE_OFF);
+            k_fin_offsets_multi<<<grid_for(S + K, 256), 256, 0, st>>>(sno, NS, d_sb, K, stage, d_sec, HGX_ARR_STATE_VERT_OFF);
+            check_launch();
+            k_fin_records_multi<<<grid_for(S * 32, 256), 256, 0, st>>>(ptrs(), sids, NS, d_sb, K, sne, sno, stage, d_sec);
+            check_launch();
+        } else {
+            k_fin_zero_multi<<<grid_for(K, 256), 256, 0, st>>>(stage, d_sec, K, HGX_ARR_STATE_EDGE_OFF);
+            k_fin_zero_multi<<<grid_for(K, 256), 256, 0, st>>>(stage, d_sec, K, HGX_ARR_STATE_VERT_OFF);
             check_launch();
         }
-        if (sg && E) {
-            k_gather_u64<<<grid_for(E, 256), 256, 0, st>>>(ev_sig.p, eids, E,
-                                                           reinterpret_cast<uint64_t*>(d + off[HGX_ARR_EVENT_SIG]));
+        k_fin_offsets_multi<<<grid_for(E + K, 256), 256, 0, st>>>(ecc, NE, d_eb, K, stage, d_sec, HGX_ARR_EVENT_CONS_OFF);
+        check_launch();
+        if (E) {
+            k_fin_events_multi<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), eids, NE, d_eb, K, d_rb, map_s.p, map_e.p,
+                                                                 nullptr, nullptr, ecc, ekc, stage, d_sec,
+                                                                 1, opt.causal ? 1 : 0, sg ? 1 : 0);
             check_launch();
         }
         if (B) {
-            fin_rng.ensure(rng.size(), 0, st);
-            HGX_CUDA_CHECK(cudaMemcpyAsync(fin_rng.p, rng.data(), rng.size() * 8, cudaMemcpyHostToDevice, st));
-            k_gather_pairs<<<grid_for(B, 256), 256, 0, st>>>(bpairs.p, fin_rng.p, fin_rng.p + NR, NR, B,
-                                                             map_e.p, dp(4));
+            k_fin_pairs_multi<<<grid_for(B, 256), 256, 0, st>>>(bpairs.p, fin_rng.p + o_rp, fin_rng.p + o_rcp,
+                                                                static_cast<uint32_t>(rp.size()), B, d_pb, K,
+                                                                map_e.p, stage, d_sec);
             check_launch();
-        }
-        if (se) {
-            HGX_CUDA_CHECK(cudaMemcpyAsync(dp(8), sne, 4ull * (S + 1), cudaMemcpyDeviceToDevice, st));
-            HGX_CUDA_CHECK(cudaMemcpyAsync(dp(11), sno, 4ull * (S + 1), cudaMemcpyDeviceToDevice, st));
-            k_gather_records<<<grid_for(uint64_t(S) * 32, 256), 256, 0, st>>>(ptrs(), sids, S, sne, sno,
-                                                                              dp(9), dp(10), dp(12));
-            check_launch();
-        } else {
-            HGX_CUDA_CHECK(cudaMemsetAsync(dp(8), 0, 4, st));
-            HGX_CUDA_CHECK(cudaMemsetAsync(dp(11), 0, 4, st));
         }
         size_t cap = 0;
-        uint8_t* h = static_cast<uint8_t*>(pinned->get(total, cap));
+        uint8_t* h = static_cast<uint8_t*>(pinned->get(std::max<uint64_t>(total, 16), cap));
         auto pool = pinned;
-        auto flat = std::make_shared<ResultArrays>();
-        flat->owner = std::shared_ptr<void>(h, [pool, cap](void* p) { pool->put(p, cap); });
-        HGX_CUDA_CHECK(cudaMemcpyAsync(h, d, total, cudaMemcpyDeviceToHost, st));
+        std::shared_ptr<void> owner(h, [pool, cap](void* p) { pool->put(p, cap); });
+        if (total) HGX_CUDA_CHECK(cudaMemcpyAsync(h, stage, total, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-        for (int i = 0; i < ResultArrays::kArrays; ++i) {
-            flat->ptr[i] = h + off[i];
-            flat->count[i] = count[i];
+        for (uint32_t k = 0; k < K; ++k) {
+            const uint32_t evo = which[k];
+            auto flat = std::make_shared<ResultArrays>();
+            flat->owner = owner;
+            for (uint32_t a = 0; a < kArr; ++a) {
+                flat->ptr[a] = h + sec[uint64_t(k) * kArr + a];
+                flat->count[a] = cnt[uint64_t(k) * kArr + a];
+            }
+            EvolutionResult& r = out[k];
+            r.flat = flat;
+            r.n_roots = evo_ranges[evo].roots;
+            r.num_classes = cls[evo];
+            r.truncated = stop[evo] != 0;
+            r.n_canonical_events = sg ? sigs[evo] : (eb[k + 1] - eb[k]);
+            if (r.truncated)
+                r.warnings.push_back(
+                    "capacity limit reached: the state cap stopped the evolution; the states, events "
+                    "and relations returned are valid and incomplete");
         }
-        r.flat = flat;
-        r.n_roots = er.roots;
-        r.num_classes = classes;
-        r.n_canonical_events = nsig;
-        r.truncated = stopped != 0;
-        if (r.truncated)
-            r.warnings.push_back(
-                "capacity limit reached: the state cap stopped the evolution; the states, events "
-                "and relations returned are valid and incomplete");
-        return r;
+        return out;
     }
+
 
     // Causal triples are written even when the caller did not ask for them; they then land in
     // this scratch instead of the result.
-    DVec<uint32_t> causal_scratch;
-    uint32_t* fin_scratch_causal(uint32_t K) {
-        causal_scratch.ensure(3ull * K + 3, 0, st);
-        return causal_scratch.p;
-    }
 
     // Counts only (results stay on the device): events and branchial pairs from the recorded
     // per-evolution ranges, states and classes from the device counters, causal triples by one
@@ -1618,140 +1658,6 @@ struct Engine::Impl {
 };
 
 // ==========================================================================================
-// Result readback (bulk copy, then split by evolution on the host).
-// ==========================================================================================
-
-namespace {
-
-template <class T>
-std::vector<T> d2h(const T* p, size_t n, cudaStream_t st) {
-    std::vector<T> v(n);
-    if (n) HGX_CUDA_CHECK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, st));
-    return v;
-}
-
-}  // namespace
-
-void Engine::Impl::read_results(const std::vector<uint32_t>& which, const RunOptions& opt,
-                                std::vector<EvolutionResult>& out) {
-    Impl& I = *this;
-    cudaStream_t st = I.st;
-    const size_t nevo = I.h_evos.size();
-    auto s_evo = d2h(I.st_evo.p, I.n_states, st);
-    auto s_depth = d2h(I.st_depth.p, I.n_states, st);
-    auto s_hash = d2h(I.st_hash.p, I.n_states, st);
-    auto s_event = d2h(I.st_event.p, I.n_states, st);
-    auto e_in = d2h(I.ev_in.p, I.n_events, st);
-    auto e_out = d2h(I.ev_out.p, I.n_events, st);
-    auto e_rule = d2h(I.ev_rule.p, I.n_events, st);
-    auto e_kept = d2h(I.ev_kept.p, I.n_events, st);
-    auto e_coff = d2h(I.ev_coff.p, I.n_events, st);
-    auto e_prod = d2h(I.ev_prod.p, I.n_events, st);
-    auto e_cons = d2h(I.ev_cons.p, I.n_cons, st);
-    auto e_cprod = d2h(I.ev_cprod.p, I.n_cons, st);
-    auto bp = d2h(I.bpairs.p, 2 * I.n_bpairs, st);
-    auto evc = d2h(I.evo_classes.p, nevo, st);
-    const bool sg = opt.event_keys != 0;
-    auto e_sig = sg ? d2h(I.ev_sig.p, I.n_events, st) : std::vector<unsigned long long>{};
-    auto evsig = sg ? d2h(I.evo_sigs.p, nevo, st) : std::vector<unsigned long long>{};
-    auto evs = d2h(I.evo_stopped.p, nevo, st);
-    std::vector<uint64_t> s_off;
-    std::vector<uint32_t> s_ne, s_nocc, arena;
-    if (opt.keep_state_edges) {
-        s_off = d2h(I.st_off.p, I.n_states, st);
-        s_ne = d2h(I.st_ne.p, I.n_states, st);
-        s_nocc = d2h(I.st_nocc.p, I.n_states, st);
-        unsigned long long top = 0;
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&top, I.arena_top.p, sizeof(top), cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-        arena = d2h(I.arena.p, top, st);
-    }
-    HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-
-    std::vector<int32_t> slot(nevo, -1);
-    out.assign(which.size(), EvolutionResult{});
-    for (size_t i = 0; i < which.size(); ++i) slot[which[i]] = static_cast<int32_t>(i);
-
-    // local state ids
-    std::vector<uint32_t> local_state(I.n_states, kNone);
-    for (uint64_t s = 0; s < I.n_states; ++s) {
-        const int32_t k = slot[s_evo[s]];
-        if (k < 0) continue;
-        EvolutionResult& r = out[k];
-        local_state[s] = static_cast<uint32_t>(r.state_hash.size());
-        r.state_hash.push_back(s_hash[s]);
-        r.state_depth.push_back(s_depth[s]);
-        r.state_event.push_back(s_event[s]);   // global arrival, remapped below
-        if (opt.keep_state_edges) {
-            if (r.state_edge_off.empty()) { r.state_edge_off.push_back(0); r.state_vert_off.push_back(0); }
-            const uint32_t* rec = arena.data() + s_off[s];
-            const uint32_t ne = s_ne[s], aw = (ne + 3) / 4;
-            for (uint32_t i = 0; i < ne; ++i) {
-                r.state_edge_ids.push_back(rec[i]);
-                r.state_arity.push_back((rec[ne + i / 4] >> ((i % 4) * 8)) & 0xFFu);
-            }
-            r.state_verts.insert(r.state_verts.end(), rec + ne + aw, rec + ne + aw + s_nocc[s]);
-            r.state_edge_off.push_back(static_cast<uint32_t>(r.state_edge_ids.size()));
-            r.state_vert_off.push_back(static_cast<uint32_t>(r.state_verts.size()));
-        }
-    }
-    // local event ids
-    std::vector<uint32_t> local_event(I.n_events, kNone);
-    for (uint64_t e = 0; e < I.n_events; ++e) {
-        if (e_in[e] == kNone || !e_kept[e]) continue;
-        const uint32_t in = e_in[e];
-        const int32_t k = slot[s_evo[in]];
-        if (k < 0) continue;
-        EvolutionResult& r = out[k];
-        local_event[e] = static_cast<uint32_t>(r.ev_in.size());
-        r.ev_in.push_back(local_state[in]);
-        r.ev_out.push_back(e_out[e] < I.n_states ? local_state[e_out[e]] : kNone);
-        r.ev_rule.push_back(e_rule[e] - I.h_evos[s_evo[in]].rule_begin);
-        r.ev_step.push_back(s_depth[in] + 1);
-        const DevRule& R = I.h_rules[e_rule[e]];
-        if (r.ev_cons_off.empty()) r.ev_cons_off.push_back(0);
-        for (uint32_t k2 = 0; k2 < R.n_lhs; ++k2) r.ev_cons.push_back(e_cons[e_coff[e] + k2]);
-        r.ev_cons_off.push_back(static_cast<uint32_t>(r.ev_cons.size()));
-        r.ev_prod_first.push_back(e_prod[e]);
-        r.ev_prod_count.push_back(R.n_rhs);
-        if (sg) r.ev_sig.push_back(e_sig[e]);
-    }
-    for (auto& r : out)
-        for (auto& se : r.state_event) se = (se < local_event.size() && local_event[se] != kNone) ? local_event[se] : kNone;
-    // causal triples
-    if (opt.causal) {
-        for (uint64_t e = 0; e < I.n_events; ++e) {
-            if (local_event[e] == kNone) continue;
-            EvolutionResult& r = out[slot[s_evo[e_in[e]]]];
-            const DevRule& R = I.h_rules[e_rule[e]];
-            for (uint32_t k2 = 0; k2 < R.n_lhs; ++k2) {
-                const uint32_t p = e_cprod[e_coff[e] + k2];
-                if (p == kNone || local_event[p] == kNone) continue;
-                r.causal.push_back(local_event[p]);
-                r.causal.push_back(local_event[e]);
-                r.causal.push_back(e_cons[e_coff[e] + k2]);
-            }
-        }
-    }
-    for (uint64_t i = 0; i < I.n_bpairs; ++i) {
-        const uint32_t a = bp[2 * i], b = bp[2 * i + 1];
-        const int32_t k = slot[s_evo[e_in[a]]];
-        if (k < 0) continue;
-        out[k].branchial.push_back(local_event[a]);
-        out[k].branchial.push_back(local_event[b]);
-    }
-    for (size_t i = 0; i < which.size(); ++i) {
-        out[i].num_classes = evc[which[i]];
-        out[i].n_canonical_events = sg ? evsig[which[i]] : out[i].ev_in.size();
-        out[i].truncated = evs[which[i]] != 0;
-        if (out[i].truncated)
-            out[i].warnings.push_back(
-                "capacity limit reached: the state cap stopped the evolution; the states, events "
-                "and relations returned are valid and incomplete");
-    }
-}
-
-// ==========================================================================================
 
 Engine::Engine(int device) : impl_(new Impl(device)) {}
 Engine::~Engine() = default;
@@ -1767,7 +1673,7 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
     std::vector<EvolutionResult> out;
     if (!opt.readback) I.read_counts(ids, out, opt.event_keys != 0);
     else if (ids.size() == 1) out.push_back(I.finalize_single(opt));
-    else I.read_results(ids, opt, out);
+    else out = I.finalize_many(ids, opt);
     I.finish_times();
     return out;
 }
@@ -1787,10 +1693,15 @@ std::vector<uint32_t> Engine::take_finished() {
 }
 EvolutionResult Engine::collect(uint32_t evo, const RunOptions& opt) {
     if (evo >= impl_->h_evos.size()) throw std::invalid_argument("collect: unknown evolution id");
-    if (opt.readback) return impl_->finalize_evo(evo, opt);
+    return std::move(collect(std::vector<uint32_t>{evo}, opt)[0]);
+}
+std::vector<EvolutionResult> Engine::collect(const std::vector<uint32_t>& evos, const RunOptions& opt) {
+    for (uint32_t evo : evos)
+        if (evo >= impl_->h_evos.size()) throw std::invalid_argument("collect: unknown evolution id");
+    if (opt.readback) return impl_->finalize_many(evos, opt);
     std::vector<EvolutionResult> out;
-    impl_->read_counts({evo}, out, opt.event_keys != 0);
-    return std::move(out[0]);
+    impl_->read_counts(evos, out, opt.event_keys != 0);
+    return out;
 }
 uint32_t Engine::active() const {
     uint32_t n = 0;

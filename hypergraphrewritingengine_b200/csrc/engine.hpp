@@ -140,6 +140,8 @@ public:
     bool step(const RunOptions& opt = {});          // one level for every active evolution
     std::vector<uint32_t> take_finished();          // evolutions that completed since last call
     EvolutionResult collect(uint32_t evo, const RunOptions& opt = {});
+    // several finished evolutions, finalised together (one set of launches and one copy)
+    std::vector<EvolutionResult> collect(const std::vector<uint32_t>& evos, const RunOptions& opt = {});
     uint32_t active() const;
     uint64_t device_bytes_in_use() const;
     static uint64_t estimate_bytes(const EvolutionSpec& spec);

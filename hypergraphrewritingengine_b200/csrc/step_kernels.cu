@@ -1471,97 +1471,178 @@ __global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last, u
     }
 }
 
-// Result finalisation of one evolution of many: ids -> local ids through maps filled here.
-__global__ void k_map_ids(const uint32_t* ids, uint32_t n, uint32_t* map) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        map[ids[i]] = i;
+// ------------------------------------------------------------------------------------------
+// Result finalisation for many evolutions at once. Their states (and events, pairs) are listed
+// back to back, evolution after evolution; bases[k] is where evolution k's run starts (K + 1
+// entries). Every output array of evolution k lives in its own section of one staging block:
+// sec[k * kArr + a] is the byte offset of array a (hgx_array order). Local ids restart at 0 per
+// evolution; a global id belongs to one evolution, so one global -> local map serves them all.
+// ------------------------------------------------------------------------------------------
+constexpr uint32_t kArr = 14;
+
+__device__ __forceinline__ uint32_t seg_of(const uint32_t* bases, uint32_t K, uint32_t i) {
+    uint32_t a = 0, b = K;   // largest k < K with bases[k] <= i
+    while (b - a > 1) {
+        const uint32_t m = (a + b) >> 1;
+        if (bases[m] <= i) a = m; else b = m;
+    }
+    return a;
 }
 
-__global__ void k_gather_states(DevPtrs P, const uint32_t* ids, uint32_t n, uint64_t* hash,
-                                uint32_t* depth, uint32_t* ne, uint32_t* nocc) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t s = ids[i];
-        hash[i] = P.st_hash[s];
-        depth[i] = P.st_depth[s];
-        ne[i] = P.st_ne[s];
-        nocc[i] = P.st_nocc[s];
+template <class T>
+__device__ __forceinline__ T* sec_ptr(uint8_t* stage, const uint64_t* sec, uint32_t k, uint32_t a) {
+    return reinterpret_cast<T*>(stage + sec[uint64_t(k) * kArr + a]);
+}
+
+// out[i] = rstart[r] + (i - rcum[r]) over nr ranges with exclusive prefix rcum (ids of many ranges).
+__global__ void k_expand_ranges(const uint64_t* rstart, const uint64_t* rcum, uint32_t nr, uint64_t n,
+                                uint32_t* out) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t a = 0, b = nr;
+        while (b - a > 1) {
+            const uint32_t m = (a + b) >> 1;
+            if (rcum[m] <= i) a = m; else b = m;
+        }
+        out[i] = static_cast<uint32_t>(rstart[a] + (i - rcum[a]));
     }
 }
 
-__global__ void k_gather_records(DevPtrs P, const uint32_t* sids, uint32_t n, const uint32_t* eoff,
-                                 const uint32_t* voff, uint32_t* oids, uint32_t* oar, uint32_t* overts) {
+__global__ void k_map_multi(const uint32_t* ids, uint32_t n, const uint32_t* bases, uint32_t K,
+                            uint32_t* map) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        map[ids[i]] = i - bases[seg_of(bases, K, i)];
+}
+
+// States: hash and depth into their sections (stage set), or edge / occurrence counts for the
+// CSR scans (stage null).
+__global__ void k_fin_states_multi(DevPtrs P, const uint32_t* sids, uint32_t n, const uint32_t* sb,
+                                   uint32_t K, uint8_t* stage, const uint64_t* sec, uint32_t* ne,
+                                   uint32_t* nocc) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = sids[i];
+        if (stage) {
+            const uint32_t k = seg_of(sb, K, i), j = i - sb[k];
+            sec_ptr<uint64_t>(stage, sec, k, 0)[j] = P.st_hash[s];
+            sec_ptr<uint32_t>(stage, sec, k, 1)[j] = P.st_depth[s];
+        } else {
+            ne[i] = P.st_ne[s];
+            nocc[i] = P.st_nocc[s];
+        }
+    }
+}
+
+// The CSR offsets of one array kind relative to each evolution's start (entries 0..n_k).
+__global__ void k_fin_offsets_multi(const uint32_t* scan, uint32_t n, const uint32_t* bases,
+                                    uint32_t K, uint8_t* stage, const uint64_t* sec, uint32_t arr) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n + K; i += gridDim.x * blockDim.x) {
+        // i < n: entry j of its evolution; i >= n: the closing entry of evolution i - n
+        uint32_t k, j, at;
+        if (i < n) { k = seg_of(bases, K, i); j = i - bases[k]; at = i; }
+        else { k = i - n; j = bases[k + 1] - bases[k]; at = bases[k + 1]; }
+        sec_ptr<uint32_t>(stage, sec, k, arr)[j] = scan[at] - scan[bases[k]];
+    }
+}
+
+__global__ void k_fin_records_multi(DevPtrs P, const uint32_t* sids, uint32_t n, const uint32_t* sb,
+                                    uint32_t K, const uint32_t* eoff, const uint32_t* voff,
+                                    uint8_t* stage, const uint64_t* sec) {
     const uint32_t lane = lane_id();
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
          i += (gridDim.x * blockDim.x) >> 5) {
-        const uint32_t s = sids[i];
+        const uint32_t s = sids[i], k = seg_of(sb, K, i);
+        const uint32_t e0 = eoff[i] - eoff[sb[k]], v0 = voff[i] - voff[sb[k]];
+        uint32_t* oids = sec_ptr<uint32_t>(stage, sec, k, 9);
+        uint32_t* oar = sec_ptr<uint32_t>(stage, sec, k, 10);
+        uint32_t* overts = sec_ptr<uint32_t>(stage, sec, k, 12);
         const uint32_t ne = P.st_ne[s], nocc = P.st_nocc[s], aw = (ne + 3) >> 2;
         const uint32_t* rec = P.arena + P.st_off[s];
-        for (uint32_t k = lane; k < ne; k += 32) {
-            oids[eoff[i] + k] = rec[k];
-            oar[eoff[i] + k] = (rec[ne + (k >> 2)] >> ((k & 3u) * 8u)) & 0xFFu;
+        for (uint32_t t = lane; t < ne; t += 32) {
+            oids[e0 + t] = rec[t];
+            oar[e0 + t] = (rec[ne + (t >> 2)] >> ((t & 3u) * 8u)) & 0xFFu;
         }
-        for (uint32_t j = lane; j < nocc; j += 32) overts[voff[i] + j] = rec[ne + aw + j];
+        for (uint32_t t = lane; t < nocc; t += 32) overts[v0 + t] = rec[ne + aw + t];
     }
 }
 
-// Events of one evolution (ids: global event ids in canonical order). pass 0: consumed and
-// causal counts; pass 1: tuples, consumed lists, produced ranges and causal triples.
-__global__ void k_gather_events(DevPtrs P, const uint32_t* ids, uint32_t n, uint32_t rule_begin,
-                                const uint32_t* smap, const uint32_t* emap, uint32_t* ccount,
-                                uint32_t* kcount, const uint32_t* coff, const uint32_t* koff,
-                                uint32_t* tup, uint32_t* cons, uint32_t* prod, uint32_t* causal,
-                                int pass) {
+// Events. pass 0: consumed and causal counts (for the scans); pass 1: tuples, consumed lists,
+// produced ranges, causal triples and signatures into their evolutions' sections.
+__global__ void k_fin_events_multi(DevPtrs P, const uint32_t* eids, uint32_t n, const uint32_t* eb,
+                                   uint32_t K, const uint32_t* rule_begin, const uint32_t* smap,
+                                   const uint32_t* emap, uint32_t* ccount, uint32_t* kcount,
+                                   const uint32_t* coff, const uint32_t* koff, uint8_t* stage,
+                                   const uint64_t* sec, int pass, int causal, int sig) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t e = ids[i];
+        const uint32_t e = eids[i];
         const uint32_t r = P.ev_rule[e];
         const DevRule& R = P.rules[r];
         const uint32_t co = P.ev_coff[e];
         if (!pass) {
-            uint32_t k = 0;
-            for (uint32_t j = 0; j < R.n_lhs; ++j) k += P.ev_cprod[co + j] != kNone ? 1u : 0u;
+            uint32_t c = 0;
+            for (uint32_t j = 0; j < R.n_lhs; ++j) c += P.ev_cprod[co + j] != kNone ? 1u : 0u;
             ccount[i] = R.n_lhs;
-            kcount[i] = k;
+            kcount[i] = causal ? c : 0u;
             continue;
         }
+        const uint32_t k = seg_of(eb, K, i), li = i - eb[k];
         const uint32_t in = P.ev_in[e];
-        tup[4 * i] = smap[in];
-        tup[4 * i + 1] = smap[P.ev_out[e]];
-        tup[4 * i + 2] = r - rule_begin;
-        tup[4 * i + 3] = P.st_depth[in] + 1;
-        prod[2 * i] = P.ev_prod[e];
-        prod[2 * i + 1] = R.n_rhs;
-        uint32_t w = koff[i];
+        uint32_t* tup = sec_ptr<uint32_t>(stage, sec, k, 2);
+        tup[4 * li] = smap[in];
+        tup[4 * li + 1] = smap[P.ev_out[e]];
+        tup[4 * li + 2] = r - rule_begin[k];
+        tup[4 * li + 3] = P.st_depth[in] + 1;
+        uint32_t* prod = sec_ptr<uint32_t>(stage, sec, k, 7);
+        prod[2 * li] = P.ev_prod[e];
+        prod[2 * li + 1] = R.n_rhs;
+        if (sig) sec_ptr<uint64_t>(stage, sec, k, 13)[li] = P.ev_sig[e];
+        uint32_t* cons = sec_ptr<uint32_t>(stage, sec, k, 6);
+        uint32_t* tri = sec_ptr<uint32_t>(stage, sec, k, 3);
+        const uint32_t c0 = coff[i] - coff[eb[k]];
+        uint32_t w = koff[i] - koff[eb[k]];
         for (uint32_t j = 0; j < R.n_lhs; ++j) {
             const uint32_t c = P.ev_cons[co + j];
-            cons[coff[i] + j] = c;
+            cons[c0 + j] = c;
             const uint32_t p = P.ev_cprod[co + j];
-            if (p == kNone) continue;
-            causal[3 * w] = emap[p];
-            causal[3 * w + 1] = i;
-            causal[3 * w + 2] = c;
+            if (!causal || p == kNone) continue;
+            tri[3 * w] = emap[p];
+            tri[3 * w + 1] = li;
+            tri[3 * w + 2] = c;
             ++w;
         }
     }
 }
 
-// Branchial pairs of one evolution: the concatenation of `nr` ranges of the pair array.
-// out[i] = src[ids[i]] (64-bit values of the listed ids).
-__global__ void k_gather_u64(const unsigned long long* src, const uint32_t* ids, uint32_t n,
-                             uint64_t* out) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        out[i] = src[ids[i]];
-}
-
-__global__ void k_gather_pairs(const uint32_t* pairs, const uint64_t* rstart, const uint64_t* rcum,
-                               uint32_t nr, uint64_t n, const uint32_t* emap, uint32_t* out) {
+// Branchial pairs of every listed evolution: nr ranges of the pair array (exclusive prefix rcum);
+// evolution k owns the pair run [pb[k], pb[k+1]) of the concatenation.
+__global__ void k_fin_pairs_multi(const uint32_t* pairs, const uint64_t* rstart, const uint64_t* rcum,
+                                  uint32_t nr, uint64_t n, const uint32_t* pb, uint32_t K,
+                                  const uint32_t* emap, uint8_t* stage, const uint64_t* sec) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n;
          i += uint64_t(gridDim.x) * blockDim.x) {
-        uint32_t k = 0;
-        while (k + 1 < nr && rcum[k + 1] <= i) ++k;
-        const uint64_t g = rstart[k] + (i - rcum[k]);
-        out[2 * i] = emap[pairs[2 * g]];
-        out[2 * i + 1] = emap[pairs[2 * g + 1]];
+        uint32_t a = 0, b = nr;
+        while (b - a > 1) {
+            const uint32_t m = (a + b) >> 1;
+            if (rcum[m] <= i) a = m; else b = m;
+        }
+        const uint64_t g = rstart[a] + (i - rcum[a]);
+        const uint32_t k = seg_of(pb, K, static_cast<uint32_t>(i));
+        uint32_t* out = sec_ptr<uint32_t>(stage, sec, k, 4);
+        const uint64_t li = i - pb[k];
+        out[2 * li] = emap[pairs[2 * g]];
+        out[2 * li + 1] = emap[pairs[2 * g + 1]];
     }
+}
+
+// A single zero entry per evolution (the offset arrays of state records not kept).
+__global__ void k_fin_zero_multi(uint8_t* stage, const uint64_t* sec, uint32_t K, uint32_t arr) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
+        sec_ptr<uint32_t>(stage, sec, k, arr)[0] = 0;
+}
+
+// Values of a scanned array at every evolution boundary (K + 1 of them), for the host.
+__global__ void k_fin_bounds(const uint32_t* scan, const uint32_t* bases, uint32_t K, uint32_t* out) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k <= K; k += gridDim.x * blockDim.x)
+        out[k] = scan[bases[k]];
 }
 
 // Each frontier state's event range (its matches, in canonical order), for its children's

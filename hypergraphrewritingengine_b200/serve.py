@@ -71,10 +71,15 @@ class Server:
 
         def collect_finished():
             nonlocal reserved
-            for evo in eng.serve_take_finished():
+            done = eng.serve_take_finished()
+            if not done:
+                return
+            results = eng.serve_collect_batch(done)   # one finalisation for all of them
+            t_done = now()
+            for evo, res in zip(done, results):
                 i = active.pop(evo)
-                recs[i].result = eng.serve_collect(evo)
-                recs[i].finished = now()
+                recs[i].result = res
+                recs[i].finished = t_done
                 reserved -= recs[i].meta.pop("est")
                 keep.pop(i, None)
 

@@ -187,6 +187,9 @@ HGX_API hgx_status hgx_serve_admit_batch(hgx_engine* engine, const hgx_job* jobs
 HGX_API hgx_status hgx_serve_step(hgx_engine* engine, int* still_active);
 HGX_API hgx_status hgx_serve_take_finished(hgx_engine* engine, uint32_t* ids, uint32_t cap, uint32_t* n);
 HGX_API hgx_status hgx_serve_collect(hgx_engine* engine, uint32_t evolution_id, hgx_result** out);
+/* Collect n finished evolutions at once (one device finalisation and one copy for all of them). */
+HGX_API hgx_status hgx_serve_collect_batch(hgx_engine* engine, const uint32_t* evolution_ids, uint32_t n,
+                                           hgx_result** out);
 HGX_API hgx_status hgx_serve_device_bytes(hgx_engine* engine, uint64_t* bytes);
 
 /* Result accessors. Replace Hypergraph::num_states / num_events / num_canonical_states
