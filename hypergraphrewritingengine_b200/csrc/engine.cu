@@ -338,6 +338,10 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        // (the cross-parent lane kernel also has ~2 KB of static shared memory per block)
+        for (const void* k : {(const void*)k_expand_lanes2<false>, (const void*)k_expand_lanes2<true>})
+            HGX_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                static_cast<int>(kMaxDynSmem - 8192)));
         for (const void* k : {(const void*)k_count, (const void*)k_expand<true>,
                               (const void*)k_expand<true, true>, (const void*)k_expand<false>,
                               (const void*)k_roots})
@@ -1343,7 +1347,14 @@ struct Engine::Impl {
                 else if (n_ev >= kTuneMinChildren) walk = tn[1] < tn[0];   // the less-sampled one
                 tune = n_ev >= kTuneMinChildren;
             }
-            LaunchShape sl = walk ? warp_shape(k_expand<true, true>, Ll, F) : warp_shape(k_expand<true>, Ll, F);
+            // single-rule evolutions: batches of children cross parents (two parent regions per warp)
+            Layout Ll2 = Ll;
+            Ll2.bytes = 2 * Ll.bytes;
+            const bool cross = rm.stride == 1 && Ll2.bytes <= (kMaxDynSmem - 8192) / 2;
+            LaunchShape sl = cross ? (walk ? warp_shape(k_expand_lanes2<true>, Ll2, F)
+                                           : warp_shape(k_expand_lanes2<false>, Ll2, F))
+                                   : (walk ? warp_shape(k_expand<true, true>, Ll, F)
+                                           : warp_shape(k_expand<true>, Ll, F));
             LaunchShape sw = warp_shape(k_expand<false>, Lw, n_ev);   // work units: slices
             auto expand = [&](uint32_t n_work) {
                 A.f_begin = 0;
@@ -1351,7 +1362,9 @@ struct Engine::Impl {
                 HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, 2 * sizeof(uint32_t), st));
                 tic();
                 if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_a, st));
-                if (walk) k_expand<true, true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                if (cross && walk) k_expand_lanes2<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                else if (cross) k_expand_lanes2<false><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                else if (walk) k_expand<true, true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 else k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 check_launch();
                 if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_b, st));

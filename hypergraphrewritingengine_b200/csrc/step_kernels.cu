@@ -1472,6 +1472,199 @@ __global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last, u
 }
 
 // ------------------------------------------------------------------------------------------
+// Lane-per-child expansion with batches that cross parents (single-rule evolutions). A warp keeps
+// two parent regions in shared memory and one 32-child batch: the children of the parent staged
+// in one region are appended while the other region's leftover children are still waiting, so a
+// parent with 38 children and the next one fill two batches instead of three. A region is
+// restaged only once the batch holds none of its children. Children keep their own event ids,
+// so the order in which batches are hashed changes nothing in the result.
+// ------------------------------------------------------------------------------------------
+struct LaneRegion {
+    uint32_t sid, ev0, cons0, prod0, fresh0, rule_g, ne, nocc, nvp;
+    uint64_t table_off, table_mask;
+};
+
+template <bool kWalk>
+__global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A, Layout L) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ LaneRegion rinfo_sm[8][2];
+    __shared__ uint32_t meta_sm[8][32];
+    const uint32_t w = threadIdx.x >> 5;
+    const uint32_t lane = lane_id();
+    char* rg[2] = {smem + w * 2 * L.bytes, smem + w * 2 * L.bytes + L.bytes};
+    LaneRegion* rinfo = rinfo_sm[w];
+    uint32_t* meta = meta_sm[w];            // slot -> (region << 31) | child index in its parent
+    uint8_t* batch = smp<uint8_t>(rg[0], L.o_batch);
+    uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
+    uint32_t nb = 0, held = 0, cur = 0;     // children in the batch, regions they come from
+    auto flush = [&]() {
+        if (lane < nb) {
+            const uint32_t m = meta[lane], r = m >> 31, idx = m & 0x7FFFFFFFu;
+            const LaneRegion ri = rinfo[r];
+            char* rs = rg[r];
+            const DevRule& R = *smp<DevRule>(rs, L.o_rule);
+            const Parent pa{ri.ne, ri.nocc, ri.nvp};
+            const uint8_t* slot = batch + lane * L.SB;
+            WlInfo info;
+            const uint64_t h = lane_wl<kLaneVMax, kLaneNMax>(L, rs, pa, R, slot, info);
+            const uint32_t e = ri.ev0 + idx;
+            const uint32_t coff = ri.cons0 + idx * R.n_lhs;
+            const uint32_t pid = ri.prod0 + idx * R.n_rhs;
+            const uint32_t* peid = smp<uint32_t>(rs, L.o_peid);
+            P.ev_in[e] = ri.sid;
+            P.ev_rule[e] = ri.rule_g;
+            P.ev_coff[e] = coff;
+            P.ev_prod[e] = pid;
+            P.ev_fresh[e] = ri.fresh0 + idx * R.n_fresh;
+            P.ev_hash[e] = h;
+            for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = peid[slot[k]];
+            for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
+            slot_insert(P, ri.table_off, ri.table_mask, h, e);
+            const uint64_t k = R.n_lhs, rr = R.n_rhs;
+            const uint32_t nec = pa.ne - R.n_lhs + R.n_rhs;
+            b_stage += 4 * k + 8;
+            b_stage += 4ull * pa.ne + 4ull * nec + 4ull * R.rhs_total + 12 * rr + 16 + 4 * k + 4 * rr;
+            b_stage += 5ull * info.nocc + 8ull * info.nv +
+                       uint64_t(info.rounds) * (8ull * info.nbr + 5ull * info.nocc + 16ull * info.nv) +
+                       8ull * info.nv + 8ull * info.nocc;
+            b_stage += 16;
+            b_hbm += 20 + 8 + 8 * k + 4 * rr + 16;
+            n_child += 1;
+            n_rounds += info.rounds;
+        }
+        __syncwarp();
+        nb = 0;
+        held = 0;
+    };
+    WarpWork q;
+    while (true) {
+        const uint32_t u = q.next(&A.work[1]);
+        if (u >= A.f_end - A.f_begin) break;
+        const uint32_t f = frontier_at(A, A.f_begin + u);
+        const uint8_t fm = A.fmode[f];
+        if (!(fm & 1u)) continue;
+        const uint32_t rn = A.counts[f];              // single-rule evolutions: item = f
+        const uint32_t sid = A.frontier[f];
+        const uint32_t evo = P.st_evo[sid];
+        const DevEvo ev = P.evos[evo];
+        if (rn == 0 || ev.rule_count == 0) {   // nothing to build: count what the join reads
+            if (lane == 0) {
+                const uint64_t ne = P.st_ne[sid], nocc = P.st_nocc[sid];
+                b_hbm += 4 * (ne + (ne + 3) / 4 + nocc) + 20;
+                b_stage += 4 * ne + 4 * nocc;
+            }
+            continue;
+        }
+        if ((held >> cur) & 1u) flush();             // the region still feeds the batch
+        char* sm = rg[cur];
+        const Parent pa = load_parent(P, L, sm, sid);
+        build_parent_csr(L, sm, pa);
+        load_rule(sm, L, &P.rules[ev.rule_begin]);
+        const DevRule& R = *smp<DevRule>(sm, L.o_rule);
+        if (lane == 0) {
+            b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
+            b_stage += 4ull * pa.ne + 4ull * pa.nocc;
+            LaneRegion ri;
+            ri.sid = sid;
+            ri.ev0 = A.ev_base + A.item_ev[f];
+            ri.cons0 = A.cons_base + A.item_cons[f];
+            ri.prod0 = A.prod_base + A.item_prod[f];
+            ri.fresh0 = A.fresh_base + A.item_fresh[f];
+            ri.rule_g = ev.rule_begin;
+            ri.ne = pa.ne;
+            ri.nocc = pa.nocc;
+            ri.nvp = pa.nvp;
+            ri.table_off = ev.table_off;
+            ri.table_mask = ev.table_mask;
+            rinfo[cur] = ri;
+        }
+        __syncwarp();
+        const Fwd fwd = fwd_prepare(P, A, L, sm, R, ev, pa, sid, (fm & 2u) != 0);
+        if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= kLaneJoinCap) {
+            uint32_t* mlist = smp<uint32_t>(sm, L.o_mlist);
+            const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+            const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+            uint32_t total = 0;
+            for (uint32_t b = 0; b < pa.ne; b += 32) {
+                const uint32_t e0 = b + lane;
+                const uint32_t c = e0 < pa.ne ? lane_walk(L, sm, R, pa, e0, [](uint32_t) {}) : 0u;
+                const uint32_t inc = warp_incl_scan(c);
+                uint32_t wpos = total + inc - c;
+                if (c) lane_walk(L, sm, R, pa, e0, [&](uint32_t pk) {
+                    if (wpos < kLaneJoinCap) mlist[wpos] = pk;
+                    ++wpos;
+                });
+                total += __shfl_sync(0xFFFFFFFFu, inc, 31);
+            }
+            __syncwarp();
+            if (total != rn) {
+                if (lane == 0) atomicOr(P.err, kErrJoinCount);
+                continue;
+            }
+            for (uint32_t i0 = 0; i0 < rn;) {
+                const uint32_t take = min(rn - i0, 32u - nb);
+                if (lane < take) {
+                    const uint32_t i = i0 + lane, sl = nb + lane;
+                    uint8_t* slot = batch + sl * L.SB;
+                    const uint32_t pk = mlist[i];
+                    uint16_t bv[kMaxVars];
+                    for (uint32_t k = 0; k < R.n_lhs; ++k) {
+                        const uint32_t pos = (pk >> (8u * k)) & 0xFFu;
+                        slot[k] = static_cast<uint8_t>(pos);
+                        const uint32_t vo = pevo[pos];
+                        for (uint32_t qq = 0; qq < R.lhs_ar[k]; ++qq)
+                            bv[R.lhs_vars[R.lhs_off[k] + qq]] = vloc[vo + qq];
+                    }
+                    for (uint32_t t = 0; t < R.rhs_total; ++t) {
+                        const uint32_t var = R.rhs_vars[t];
+                        slot[R.n_lhs + t] = static_cast<uint8_t>(((R.new_mask >> var) & 1u)
+                                                                 ? pa.nvp + R.fresh_rank[var]
+                                                                 : bv[var]);
+                    }
+                    meta[sl] = (cur << 31) | i;
+                }
+                __syncwarp();
+                nb += take;
+                i0 += take;
+                held |= 1u << cur;
+                if (nb == 32) flush();
+            }
+        } else {
+            const uint16_t* match = smp<uint16_t>(sm, L.o_match);
+            const uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
+            uint32_t idx = 0;
+            enumerate_matches(P, L, sm, R, pa, fwd, [&](uint32_t nm) {
+                uint8_t* slot = batch + nb * L.SB;
+                if (lane < R.n_lhs) slot[lane] = static_cast<uint8_t>(match[lane]);
+                for (uint32_t t = lane; t < R.rhs_total; t += 32) {
+                    const uint32_t var = R.rhs_vars[t];
+                    slot[R.n_lhs + t] = static_cast<uint8_t>(((nm >> var) & 1u) ? bind[var]
+                                                             : pa.nvp + R.fresh_rank[var]);
+                }
+                if (lane == 0) meta[nb] = (cur << 31) | idx;
+                __syncwarp();
+                ++idx;
+                ++nb;
+                held |= 1u << cur;
+                if (nb == 32) flush();
+            });
+        }
+        cur ^= 1u;
+    }
+    if (nb) flush();
+    b_stage = warp_sum64(b_stage);
+    b_hbm = warp_sum64(b_hbm);
+    n_child = warp_sum64(n_child);
+    n_rounds = warp_sum64(n_rounds);
+    if (lane == 0 && b_hbm) {
+        atomicAdd(&P.stats[0], static_cast<unsigned long long>(b_stage));
+        atomicAdd(&P.stats[1], static_cast<unsigned long long>(b_hbm));
+        atomicAdd(&P.stats[2], static_cast<unsigned long long>(n_child));
+        atomicAdd(&P.stats[3], static_cast<unsigned long long>(n_rounds));
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // Result finalisation for many evolutions at once. Their states (and events, pairs) are listed
 // back to back, evolution after evolution; bases[k] is where evolution k's run starts (K + 1
 // entries). Every output array of evolution k lives in its own section of one staging block:
