@@ -18,6 +18,8 @@ namespace {
 
 constexpr int kNumSMs = 148;
 constexpr size_t kMaxDynSmem = 227 * 1024;
+// Parent regions per warp of the cross-parent lane kernel (measured: 2 beats 4 on C2 and C4).
+constexpr uint32_t kLaneRegions = 2;
 
 uint64_t next_pow2(uint64_t x) {
     uint64_t p = 1;
@@ -339,7 +341,8 @@ struct Engine::Impl {
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
         // (the cross-parent lane kernel also has ~2 KB of static shared memory per block)
-        for (const void* k : {(const void*)k_expand_lanes2<false>, (const void*)k_expand_lanes2<true>})
+        for (const void* k : {(const void*)k_expand_lanes2<false, kLaneRegions>,
+                              (const void*)k_expand_lanes2<true, kLaneRegions>})
             HGX_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 static_cast<int>(kMaxDynSmem - 8192)));
         for (const void* k : {(const void*)k_count, (const void*)k_expand<true>,
@@ -1349,10 +1352,10 @@ struct Engine::Impl {
             }
             // single-rule evolutions: batches of children cross parents (two parent regions per warp)
             Layout Ll2 = Ll;
-            Ll2.bytes = 2 * Ll.bytes;
+            Ll2.bytes = kLaneRegions * Ll.bytes;
             const bool cross = rm.stride == 1 && Ll2.bytes <= (kMaxDynSmem - 8192) / 2;
-            LaunchShape sl = cross ? (walk ? warp_shape(k_expand_lanes2<true>, Ll2, F)
-                                           : warp_shape(k_expand_lanes2<false>, Ll2, F))
+            LaunchShape sl = cross ? (walk ? warp_shape(k_expand_lanes2<true, kLaneRegions>, Ll2, F)
+                                           : warp_shape(k_expand_lanes2<false, kLaneRegions>, Ll2, F))
                                    : (walk ? warp_shape(k_expand<true, true>, Ll, F)
                                            : warp_shape(k_expand<true>, Ll, F));
             LaunchShape sw = warp_shape(k_expand<false>, Lw, n_ev);   // work units: slices
@@ -1362,8 +1365,8 @@ struct Engine::Impl {
                 HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, 2 * sizeof(uint32_t), st));
                 tic();
                 if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_a, st));
-                if (cross && walk) k_expand_lanes2<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
-                else if (cross) k_expand_lanes2<false><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                if (cross && walk) k_expand_lanes2<true, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                else if (cross) k_expand_lanes2<false, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 else if (walk) k_expand<true, true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 else k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 check_launch();

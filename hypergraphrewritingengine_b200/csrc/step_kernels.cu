@@ -1473,10 +1473,10 @@ __global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last, u
 
 // ------------------------------------------------------------------------------------------
 // Lane-per-child expansion with batches that cross parents (single-rule evolutions). A warp keeps
-// two parent regions in shared memory and one 32-child batch: the children of the parent staged
-// in one region are appended while the other region's leftover children are still waiting, so a
-// parent with 38 children and the next one fill two batches instead of three. A region is
-// restaged only once the batch holds none of its children. Children keep their own event ids,
+// kReg parent regions in shared memory (used in turn) and one 32-child batch: the children of the
+// parent staged in one region are appended while other regions' leftover children are still
+// waiting, so a parent with 38 children and the next one fill two batches instead of three. A
+// region is restaged only once the batch holds none of its children. Children keep their own event ids,
 // so the order in which batches are hashed changes nothing in the result.
 // ------------------------------------------------------------------------------------------
 struct LaneRegion {
@@ -1484,24 +1484,25 @@ struct LaneRegion {
     uint64_t table_off, table_mask;
 };
 
-template <bool kWalk>
+template <bool kWalk, int kReg = 2>
 __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A, Layout L) {
     extern __shared__ __align__(16) char smem[];
-    __shared__ LaneRegion rinfo_sm[8][2];
+    __shared__ LaneRegion rinfo_sm[8][kReg];
     __shared__ uint32_t meta_sm[8][32];
     const uint32_t w = threadIdx.x >> 5;
     const uint32_t lane = lane_id();
-    char* rg[2] = {smem + w * 2 * L.bytes, smem + w * 2 * L.bytes + L.bytes};
+    char* const wbase = smem + w * kReg * L.bytes;
+    auto rg = [&](uint32_t r) { return wbase + r * L.bytes; };
     LaneRegion* rinfo = rinfo_sm[w];
-    uint32_t* meta = meta_sm[w];            // slot -> (region << 31) | child index in its parent
-    uint8_t* batch = smp<uint8_t>(rg[0], L.o_batch);
+    uint32_t* meta = meta_sm[w];            // slot -> (region << 29) | child index in its parent
+    uint8_t* batch = smp<uint8_t>(rg(0), L.o_batch);
     uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
     uint32_t nb = 0, held = 0, cur = 0;     // children in the batch, regions they come from
     auto flush = [&]() {
         if (lane < nb) {
-            const uint32_t m = meta[lane], r = m >> 31, idx = m & 0x7FFFFFFFu;
+            const uint32_t m = meta[lane], r = m >> 29, idx = m & 0x1FFFFFFFu;
             const LaneRegion ri = rinfo[r];
-            char* rs = rg[r];
+            char* rs = rg(r);
             const DevRule& R = *smp<DevRule>(rs, L.o_rule);
             const Parent pa{ri.ne, ri.nocc, ri.nvp};
             const uint8_t* slot = batch + lane * L.SB;
@@ -1556,7 +1557,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
             continue;
         }
         if ((held >> cur) & 1u) flush();             // the region still feeds the batch
-        char* sm = rg[cur];
+        char* sm = rg(cur);
         const Parent pa = load_parent(P, L, sm, sid);
         build_parent_csr(L, sm, pa);
         load_rule(sm, L, &P.rules[ev.rule_begin]);
@@ -1621,7 +1622,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
                                                                  ? pa.nvp + R.fresh_rank[var]
                                                                  : bv[var]);
                     }
-                    meta[sl] = (cur << 31) | i;
+                    meta[sl] = (cur << 29) | i;
                 }
                 __syncwarp();
                 nb += take;
@@ -1641,7 +1642,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
                     slot[R.n_lhs + t] = static_cast<uint8_t>(((nm >> var) & 1u) ? bind[var]
                                                              : pa.nvp + R.fresh_rank[var]);
                 }
-                if (lane == 0) meta[nb] = (cur << 31) | idx;
+                if (lane == 0) meta[nb] = (cur << 29) | idx;
                 __syncwarp();
                 ++idx;
                 ++nb;
@@ -1649,7 +1650,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
                 if (nb == 32) flush();
             });
         }
-        cur ^= 1u;
+        cur = cur + 1 == kReg ? 0u : cur + 1;
     }
     if (nb) flush();
     b_stage = warp_sum64(b_stage);
