@@ -123,7 +123,7 @@ def max_over_ranks(dist, value: float, device: str = "cuda") -> float:
 
 
 def profile_traffic():
-    """dram bytes per k_expand launch from the committed ncu summary, if present."""
+    """dram bytes per lane-expand launch from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", "k_expand.c2-8step.txt")
     if not os.path.exists(p):
         return None
@@ -310,7 +310,7 @@ def main():
         "unique_states_per_s": world * states / (t_ms / 1e3),
         "e2e": {"value": world * events / e2e_t, "unit": "events/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},
-        "roofline": {"bound": "hbm", "kernel": "k_expand", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_expand_lanes2 (lane expand)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (copy bandwidth)",
                      "algorithmic_bytes_per_launch": per_launch_bytes,
