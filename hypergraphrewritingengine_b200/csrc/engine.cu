@@ -541,20 +541,28 @@ struct Engine::Impl {
         return s;
     }
 
-    void scan(const uint32_t* in, uint32_t* out, uint32_t n) {
-        if (n == 0) {
-            HGX_CUDA_CHECK(cudaMemsetAsync(out, 0, sizeof(uint32_t), st));
+    // Exclusive scans of k <= 4 arrays of length n (out[n] = total) with the same launches: one
+    // launch when n fits one tile, three otherwise.
+    void scan_multi(std::initializer_list<std::pair<const uint32_t*, uint32_t*>> arrays, uint32_t n) {
+        ScanSet S{};
+        uint32_t k = 0;
+        for (const auto& a : arrays) { S.in[k] = a.first; S.out[k] = a.second; ++k; }
+        const uint32_t nb = (n + kScanTile - 1) / kScanTile;
+        if (nb <= 1) {
+            k_scan_down<<<dim3(1, k), kScanThreads, 0, st>>>(S, n, nullptr, 0);
+            check_launch();
             return;
         }
-        const uint32_t nb = (n + kScanTile - 1) / kScanTile;
-        scan_sums.ensure(nb + 1, 0, st);
-        k_scan_reduce<<<nb, kScanThreads, 0, st>>>(in, n, scan_sums.p);
+        scan_sums.ensure(uint64_t(k) * (nb + 1), 0, st);
+        k_scan_reduce<<<dim3(nb, k), kScanThreads, 0, st>>>(S, n, scan_sums.p, nb);
         check_launch();
-        k_scan_sums<<<1, kScanThreads, 0, st>>>(scan_sums.p, nb);
+        k_scan_sums<<<k, kScanThreads, 0, st>>>(scan_sums.p, nb);
         check_launch();
-        k_scan_down<<<nb, kScanThreads, 0, st>>>(in, out, n, scan_sums.p, nb);
+        k_scan_down<<<dim3(nb, k), kScanThreads, 0, st>>>(S, n, scan_sums.p, nb);
         check_launch();
     }
+
+    void scan(const uint32_t* in, uint32_t* out, uint32_t n) { scan_multi({{in, out}}, n); }
 
     // ---- admission ------------------------------------------------------------------------
     //
@@ -1247,10 +1255,8 @@ struct Engine::Impl {
         tic();
         k_item_sizes<<<grid_for(NI, 256), 256, 0, st>>>(ptrs(), A);
         check_launch();
-        scan(item_ev.p, item_ev.p, NI);
-        scan(item_cons.p, item_cons.p, NI);
-        scan(item_prod.p, item_prod.p, NI);
-        scan(item_fresh.p, item_fresh.p, NI);
+        scan_multi({{item_ev.p, item_ev.p}, {item_cons.p, item_cons.p}, {item_prod.p, item_prod.p},
+                    {item_fresh.p, item_fresh.p}}, NI);
         k_fwd_record<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A);
         check_launch();
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_first_ev.p, 0xFF, h_evos.size() * 4, st));
@@ -1542,8 +1548,7 @@ struct Engine::Impl {
             }
             k_rep<<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
-            scan(flag_rep.p, flag_rep.p, ne2);
-            scan(flag_front.p, flag_front.p, ne2);
+            scan_multi({{flag_rep.p, flag_rep.p}, {flag_front.p, flag_front.p}}, ne2);
             toc(times.select);
         } else {
             HGX_CUDA_CHECK(cudaMemsetAsync(flag_rep.p, 0, 4, st));

@@ -2361,20 +2361,7 @@ __device__ uint32_t block_excl_scan(uint32_t x, uint32_t* sh, uint32_t& total) {
     return r;
 }
 
-__global__ void k_scan_reduce(const uint32_t* in, uint32_t n, uint32_t* sums) {
-    __shared__ uint32_t sh[33];
-    const uint32_t base = blockIdx.x * kScanTile;
-    uint32_t s = 0;
-    for (uint32_t k = 0; k < kScanPer; ++k) {
-        const uint32_t i = base + k * kScanThreads + threadIdx.x;
-        if (i < n) s += in[i];
-    }
-    uint32_t total;
-    block_excl_scan(s, sh, total);
-    if (threadIdx.x == 0) sums[blockIdx.x] = total;
-}
-
-__global__ void k_scan_sums(uint32_t* sums, uint32_t nb) {
+__device__ void k_scan_sums_body(uint32_t* sums, uint32_t nb) {
     __shared__ uint32_t sh[33];
     uint32_t carry = 0;
     for (uint32_t b = 0; b < nb; b += kScanThreads) {
@@ -2388,9 +2375,37 @@ __global__ void k_scan_sums(uint32_t* sums, uint32_t nb) {
     if (threadIdx.x == 0) sums[nb] = carry;
 }
 
-__global__ void k_scan_down(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_t* sums,
-                            uint32_t nb) {
+// Several arrays of the same length scanned by the same launches (blockIdx.y = array).
+struct ScanSet {
+    const uint32_t* in[4];
+    uint32_t* out[4];
+};
+
+__global__ void k_scan_reduce(ScanSet S, uint32_t n, uint32_t* sums, uint32_t nb) {
     __shared__ uint32_t sh[33];
+    const uint32_t* in = S.in[blockIdx.y];
+    const uint32_t base = blockIdx.x * kScanTile;
+    uint32_t s = 0;
+    for (uint32_t k = 0; k < kScanPer; ++k) {
+        const uint32_t i = base + k * kScanThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    uint32_t total;
+    block_excl_scan(s, sh, total);
+    if (threadIdx.x == 0) sums[blockIdx.y * (nb + 1) + blockIdx.x] = total;
+}
+
+__global__ void k_scan_sums(uint32_t* sums, uint32_t nb) {
+    k_scan_sums_body(sums + blockIdx.x * (nb + 1), nb);
+}
+
+// Exclusive scan of one tile per block with the tile carries in `sums` (null: a single tile),
+// writing the total at out[n].
+__global__ void k_scan_down(ScanSet S, uint32_t n, const uint32_t* sums, uint32_t nb) {
+    __shared__ uint32_t sh[33];
+    const uint32_t* in = S.in[blockIdx.y];
+    uint32_t* out = S.out[blockIdx.y];
+    const uint32_t* sm = sums ? sums + blockIdx.y * (nb + 1) : nullptr;
     const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
     uint32_t v[kScanPer];
     uint32_t s = 0;
@@ -2400,13 +2415,13 @@ __global__ void k_scan_down(const uint32_t* in, uint32_t* out, uint32_t n, const
         s += v[k];
     }
     uint32_t total;
-    uint32_t ex = block_excl_scan(s, sh, total) + sums[blockIdx.x];
+    uint32_t ex = block_excl_scan(s, sh, total) + (sm ? sm[blockIdx.x] : 0u);
     for (uint32_t k = 0; k < kScanPer; ++k) {
         const uint32_t i = base + k;
         if (i < n) out[i] = ex;
         ex += v[k];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = sums[nb];
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = sm ? sm[nb] : total;
 }
 
 }  // namespace hgx
