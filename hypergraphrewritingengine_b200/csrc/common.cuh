@@ -55,12 +55,18 @@ HGX_HD uint64_t smix(uint64_t z) {
     return z ^ (z >> 31);
 }
 
+// Rule flag: the RHS edges form one connected hypergraph holding every LHS variable. Then a child
+// is connected exactly when its parent is: every component left after removing the matched edges
+// touches a matched vertex, and the produced edges join all of those.
+constexpr uint8_t kRuleRhsJoinsLhs = 1u << 0;
+
 // A rewrite rule as the kernels read it: one fixed-size record, copied to shared memory by
 // the warp that applies it. `sched` is the binding order of the LHS positions; matches are
 // enumerated in lexicographic order of their edges' state positions taken in that order.
 struct DevRule {
     uint8_t n_lhs, n_rhs, n_fresh, lhs_total, rhs_total;
-    uint8_t pad[3];
+    uint8_t flags;           // kRule* bits
+    uint8_t pad[2];
     uint32_t new_mask;       // variables that occur only on the RHS
     uint8_t lhs_ar[kMaxPatternEdges], lhs_off[kMaxPatternEdges];
     uint8_t rhs_ar[kMaxPatternEdges], rhs_off[kMaxPatternEdges];
@@ -68,6 +74,7 @@ struct DevRule {
     uint8_t fresh_rank[kMaxVars];   // n-th fresh variable -> n (ascending variable order)
     uint8_t lhs_vars[kMaxSideVars];
     uint8_t rhs_vars[kMaxSideVars];
+    uint8_t rhs_pos_edge[kMaxSideVars];   // RHS position -> its edge
 };
 static_assert(sizeof(DevRule) % 4 == 0, "rule record must be word aligned");
 

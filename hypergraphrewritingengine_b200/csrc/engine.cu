@@ -89,6 +89,7 @@ DevRule pack_rule(const RuleSpec& r) {
         if (e.empty() || e.size() > kMaxArity) throw std::invalid_argument("rule: RHS edge arity must be 1..16");
         d.rhs_ar[i] = static_cast<uint8_t>(e.size());
         d.rhs_off[i] = static_cast<uint8_t>(off);
+        for (size_t q = 0; q < e.size(); ++q) d.rhs_pos_edge[off + q] = static_cast<uint8_t>(i);
         for (uint8_t v : e) {
             if (v >= kMaxVars) throw std::invalid_argument("rule: pattern variable must be < 32");
             if (off >= kMaxSideVars) throw std::invalid_argument("rule: RHS has more than 64 positions");
@@ -98,6 +99,18 @@ DevRule pack_rule(const RuleSpec& r) {
     }
     d.rhs_total = static_cast<uint8_t>(off);
     d.new_mask = rhs_mask & ~lhs_mask;
+    {
+        // RHS connectivity over its variables (union-find on 32 labels)
+        uint8_t up[kMaxVars];
+        for (uint32_t v = 0; v < kMaxVars; ++v) up[v] = static_cast<uint8_t>(v);
+        auto root = [&](uint32_t x) { while (up[x] != x) x = up[x]; return x; };
+        for (const auto& e : r.rhs)
+            for (size_t q = 1; q < e.size(); ++q) up[root(e[q])] = static_cast<uint8_t>(root(e[0]));
+        uint32_t roots = 0;
+        for (uint32_t v = 0; v < kMaxVars; ++v)
+            if (((rhs_mask >> v) & 1u) && root(v) == v) ++roots;
+        if (roots == 1 && (lhs_mask & ~rhs_mask) == 0) d.flags |= kRuleRhsJoinsLhs;
+    }
     uint32_t rank = 0;
     for (uint32_t v = 0; v < kMaxVars; ++v)
         if ((d.new_mask >> v) & 1u) d.fresh_rank[v] = static_cast<uint8_t>(rank++);
@@ -204,7 +217,10 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.SB = rm.lhs + rm.rhs_total;
         L.o_poff = take(2 * (kLaneVMax + 1), 2);
         L.o_pocc = take(2 * NOCC, 2);
+        L.o_pnoff = take(2 * (kLaneVMax + 1), 2);
+        L.o_pnbr = take(2 * NOCC * (rm.arity - 1), 2);
         L.o_pnn = take(2 * kLaneVMax, 2);
+        L.o_pconn = take(4, 4);
         L.o_pdeg = take(2 * kLaneVMax, 2);
         L.o_batch = take(32 * L.SB, 1);
         L.o_mlist = take(4 * kLaneJoinCap, 4);

@@ -6,9 +6,11 @@
 //
 // A child is given relative to its parent: the parent's edges (arity pear[e], vertex offset
 // pevo[e] into vloc), the parent's per-vertex occurrence lists in edge order (poff/pocc, entries
-// e << 4 | position), per-vertex degree pdeg and neighbour count pnn (sum of arity - 1), and a
-// slot holding the parent positions the match removes (pattern order) followed by the local
-// vertex ids of the produced edges (RHS order). Local ids: parent vertices [0, nvp), the n-th
+// e << 4 | position), per-vertex degree pdeg and neighbour count pnn (sum of arity - 1), the
+// parent's per-vertex neighbour lists (pnoff/pnbr, entries lane_nbr_entry(e, u, k): vertex u at
+// position k of edge e, one per other position of every occurrence), and a slot holding the
+// parent positions the match removes (pattern order) followed by the local vertex ids of the
+// produced edges (RHS order). Local ids: parent vertices [0, nvp), the n-th
 // fresh variable nvp + n. The child's edge order is the parent's minus the removed edges,
 // then the produced ones -- the order the reference hashes a state's edges in.
 //
@@ -24,6 +26,36 @@ namespace hgx {
 struct WlInfo {
     uint32_t rounds, nv, nocc, nbr;   // refinement rounds run, vertices, occurrences, sum a(a-1)
 };
+
+// One neighbour entry of a parent vertex: the edge it comes from (< 64, tested against the removed
+// positions), the neighbour's local id (< 64) and its position in that edge (< 16).
+HGX_HD uint16_t lane_nbr_entry(uint32_t e, uint32_t u, uint32_t k) {
+    return static_cast<uint16_t>((e << 10) | (u << 4) | k);
+}
+
+HGX_HD uint32_t lane_ctz64(uint64_t m) {
+#ifdef __CUDA_ARCH__
+    return static_cast<uint32_t>(__ffsll(static_cast<long long>(m)) - 1);
+#else
+    return static_cast<uint32_t>(__builtin_ctzll(m));
+#endif
+}
+
+// Host form of the parent neighbour lists (the expand kernel builds them warp-parallel).
+inline void lane_build_nbr(const uint8_t* pear, const uint16_t* pevo, const uint16_t* vloc,
+                           uint32_t pne, uint32_t nvp, uint16_t* pnoff, uint16_t* pnbr) {
+    uint32_t w = 0;
+    for (uint32_t v = 0; v < nvp; ++v) {
+        pnoff[v] = static_cast<uint16_t>(w);
+        for (uint32_t e = 0; e < pne; ++e)
+            for (uint32_t q = 0; q < pear[e]; ++q) {
+                if (vloc[pevo[e] + q] != v) continue;
+                for (uint32_t k = 0; k < pear[e]; ++k)
+                    if (k != q) pnbr[w++] = lane_nbr_entry(e, vloc[pevo[e] + k], k);
+            }
+    }
+    pnoff[nvp] = static_cast<uint16_t>(w);
+}
 
 HGX_HD void lane_isort64(uint64_t* a, uint32_t n) {
         #pragma unroll 1
@@ -53,7 +85,8 @@ HGX_HD uint32_t lane_distinct(const uint64_t* cur, const uint16_t* deg, uint32_t
 template <int VM, int NM>
 HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const uint16_t* vloc,
                              const uint16_t* poff, const uint16_t* pocc, const uint16_t* pdeg,
-                             const uint16_t* pnn, uint32_t pne, uint32_t nvp, const DevRule& R,
+                             const uint16_t* pnn, const uint16_t* pnoff, const uint16_t* pnbr,
+                             bool pconn, uint32_t pne, uint32_t nvp, const DevRule& R,
                              const uint8_t* slot, WlInfo& info) {
     const uint8_t* rpos = slot;
     const uint8_t* prodv = slot + R.n_lhs;
@@ -103,6 +136,13 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
     info.nocc = nocc;
     info.nbr = nbr;
     if (nv == 0) return 0;
+    // produced occurrences by vertex: bit p of pm[v] <=> RHS position p holds v (ascending p is
+    // RHS edge order, then position order)
+    uint64_t pm[VM];
+        #pragma unroll 1
+    for (uint32_t v = 0; v < V; ++v) pm[v] = 0;
+        #pragma unroll 1
+    for (uint32_t p = 0; p < R.rhs_total; ++p) pm[prodv[p]] |= 1ull << p;
 
     uint64_t cura[VM], curb[VM], buf[NM];
     uint64_t* cur = cura;   // this round's colours
@@ -121,11 +161,9 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
             buf[n++] = (static_cast<uint64_t>(pear[e]) << 8) | (x & 15u);
         }
                 #pragma unroll 1
-        for (uint32_t k = 0; k < R.n_rhs; ++k) {
-            const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
-                        #pragma unroll 1
-            for (uint32_t q = 0; q < a && n < cap; ++q)
-                if (prodv[o + q] == v) buf[n++] = (static_cast<uint64_t>(a) << 8) | q;
+        for (uint64_t m = pm[v]; m && n < cap; m &= m - 1) {
+            const uint32_t p = lane_ctz64(m), k = R.rhs_pos_edge[p];
+            buf[n++] = (static_cast<uint64_t>(R.rhs_ar[k]) << 8) | (p - R.rhs_off[k]);
         }
         lane_isort64(buf, n);
         uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(deg[v]));
@@ -142,27 +180,22 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
                 #pragma unroll 1
         for (uint32_t v = 0; v < V; ++v) {
             if (!deg[v]) { nxt[v] = 0; continue; }
+            // the neighbour multiset; nn[v] <= cap entries, so the reference's cap never cuts here
             uint32_t n = 0;
-            const uint32_t j0 = v < nvp ? poff[v] : 0u, j1 = v < nvp ? poff[v + 1] : 0u;
+            const uint32_t j0 = v < nvp ? pnoff[v] : 0u, j1 = v < nvp ? pnoff[v + 1] : 0u;
                         #pragma unroll 1
             for (uint32_t j = j0; j < j1; ++j) {
-                const uint32_t x = pocc[j], e = x >> 4;
-                if ((rmask >> e) & 1ull) continue;
-                const uint32_t q = x & 15u, a = pear[e], vo = pevo[e];
-                                #pragma unroll 1
-                for (uint32_t k = 0; k < a; ++k)
-                    if (k != q && n < cap) buf[n++] = fnv(cur[vloc[vo + k]], k);
+                const uint32_t x = pnbr[j];
+                if ((rmask >> (x >> 10)) & 1ull) continue;
+                buf[n++] = fnv(cur[(x >> 4) & 63u], x & 15u);
             }
                         #pragma unroll 1
-            for (uint32_t kk = 0; kk < R.n_rhs; ++kk) {
-                const uint32_t a = R.rhs_ar[kk], o = R.rhs_off[kk];
+            for (uint64_t m = pm[v]; m; m &= m - 1) {
+                const uint32_t p = lane_ctz64(m), kk = R.rhs_pos_edge[p];
+                const uint32_t a = R.rhs_ar[kk], o = R.rhs_off[kk], q = p - o;
                                 #pragma unroll 1
-                for (uint32_t q = 0; q < a; ++q) {
-                    if (prodv[o + q] != v) continue;
-                                        #pragma unroll 1
-                    for (uint32_t t = 0; t < a; ++t)
-                        if (t != q && n < cap) buf[n++] = fnv(cur[prodv[o + t]], t);
-                }
+                for (uint32_t t = 0; t < a; ++t)
+                    if (t != q) buf[n++] = fnv(cur[prodv[o + t]], t);
             }
             lane_isort64(buf, n);
             uint64_t h = cur[v];
@@ -179,16 +212,18 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         prev = d;
     }
 
-    // components (partition), then the commutative folds
+    // components (partition), then the commutative folds. A connected parent and a rule whose RHS
+    // joins every LHS vertex give a connected child: no partition needed.
+    const bool one = pconn && (R.flags & kRuleRhsJoinsLhs);
     uint8_t comp[VM];
         #pragma unroll 1
-    for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(v);
+    for (uint32_t v = 0; v < V && !one; ++v) comp[v] = static_cast<uint8_t>(v);
     auto find = [&](uint32_t x) -> uint32_t {
         while (comp[x] != x) { comp[x] = comp[comp[x]]; x = comp[x]; }
         return x;
     };
         #pragma unroll 1
-    for (uint32_t e = 0; e < pne; ++e) {
+    for (uint32_t e = 0; e < pne && !one; ++e) {
         if ((rmask >> e) & 1ull) continue;
         const uint32_t a = pear[e], vo = pevo[e];
         const uint32_t r = find(vloc[vo]);
@@ -199,7 +234,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         }
     }
         #pragma unroll 1
-    for (uint32_t k = 0; k < R.n_rhs; ++k) {
+    for (uint32_t k = 0; k < R.n_rhs && !one; ++k) {
         const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
         const uint32_t r = find(prodv[o]);
                 #pragma unroll 1
@@ -209,7 +244,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         }
     }
         #pragma unroll 1
-    for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(find(v));
+    for (uint32_t v = 0; v < V && !one; ++v) comp[v] = static_cast<uint8_t>(find(v));
     uint64_t vs = 0, es = 0, cs = 0;
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
@@ -234,9 +269,9 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         es += smix(h);
     }
     // one component (the usual case): its term folds every vertex and edge, no per-root scans
-    uint32_t roots = 0;
+    uint32_t roots = one ? 1u : 0u;
         #pragma unroll 1
-    for (uint32_t v = 0; v < V; ++v) roots += (deg[v] && comp[v] == v) ? 1u : 0u;
+    for (uint32_t v = 0; v < V && !one; ++v) roots += (deg[v] && comp[v] == v) ? 1u : 0u;
     if (roots == 1)
         cs = smix(fnv(fnv(kFnvOffset, (static_cast<uint64_t>(ne) << 32) | nv), vs));
         #pragma unroll 1

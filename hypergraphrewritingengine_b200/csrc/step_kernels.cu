@@ -979,27 +979,51 @@ __device__ uint32_t build_parent_csr(const Layout& L, char* sm, const Parent& pa
     uint16_t* pocc = smp<uint16_t>(sm, L.o_pocc);
     uint16_t* pdeg = smp<uint16_t>(sm, L.o_pdeg);
     uint16_t* pnn = smp<uint16_t>(sm, L.o_pnn);
+    uint16_t* pnoff = smp<uint16_t>(sm, L.o_pnoff);
+    uint16_t* pnbr = smp<uint16_t>(sm, L.o_pnbr);
     const uint32_t v = lane;
-    uint32_t d = 0, nn = 0;
+    uint32_t d = 0, nn = 0, adj = 0;   // adj: vertices sharing an edge with v (nvp <= 32)
     if (v < pa.nvp)
         for (uint32_t e = 0; e < pa.ne; ++e) {
             const uint32_t a = pear[e], vo = pevo[e];
             for (uint32_t q = 0; q < a; ++q)
-                if (vloc[vo + q] == v) { ++d; nn += a - 1; }
+                if (vloc[vo + q] == v) {
+                    ++d;
+                    nn += a - 1;
+                    for (uint32_t k = 0; k < a; ++k) adj |= 1u << vloc[vo + k];
+                }
         }
+    // connectivity: grow the set reached from vertex 0 (at most nvp rounds)
+    uint32_t reach = pa.nvp ? 1u : 0u;
+    for (uint32_t it = 0; it < pa.nvp; ++it) {
+        const uint32_t nr = reach | __reduce_or_sync(0xFFFFFFFFu, ((reach >> lane) & 1u) ? adj : 0u);
+        if (nr == reach) break;
+        reach = nr;
+    }
     const uint32_t inc = warp_incl_scan(d);
+    const uint32_t incn = warp_incl_scan(nn);
     if (v < pa.nvp) {
         poff[v] = static_cast<uint16_t>(inc - d);
         pdeg[v] = static_cast<uint16_t>(d);
         pnn[v] = static_cast<uint16_t>(nn);
-        uint32_t w = inc - d;
+        pnoff[v] = static_cast<uint16_t>(incn - nn);
+        uint32_t w = inc - d, wn = incn - nn;
         for (uint32_t e = 0; e < pa.ne; ++e) {
             const uint32_t a = pear[e], vo = pevo[e];
-            for (uint32_t q = 0; q < a; ++q)
-                if (vloc[vo + q] == v) pocc[w++] = static_cast<uint16_t>((e << 4) | q);
+            for (uint32_t q = 0; q < a; ++q) {
+                if (vloc[vo + q] != v) continue;
+                pocc[w++] = static_cast<uint16_t>((e << 4) | q);
+                for (uint32_t k = 0; k < a; ++k)
+                    if (k != q) pnbr[wn++] = lane_nbr_entry(e, vloc[vo + k], k);
+            }
         }
     }
-    if (lane == 31) poff[pa.nvp] = static_cast<uint16_t>(inc);
+    if (lane == 31) {
+        poff[pa.nvp] = static_cast<uint16_t>(inc);
+        pnoff[pa.nvp] = static_cast<uint16_t>(incn);
+        const uint32_t all = pa.nvp >= 32 ? 0xFFFFFFFFu : (1u << pa.nvp) - 1u;
+        *smp<uint32_t>(sm, L.o_pconn) = (pa.nvp && reach == all) ? 1u : 0u;
+    }
     const uint32_t nnmax = warp_max32(nn);
     __syncwarp();
     return nnmax;
@@ -1011,7 +1035,9 @@ __device__ __forceinline__ uint64_t lane_wl(const Layout& L, char* sm, const Par
     return lane_wl_core<VM, NM>(smp<uint8_t>(sm, L.o_pear), smp<uint16_t>(sm, L.o_pevo),
                                 smp<uint16_t>(sm, L.o_vloc), smp<uint16_t>(sm, L.o_poff),
                                 smp<uint16_t>(sm, L.o_pocc), smp<uint16_t>(sm, L.o_pdeg),
-                                smp<uint16_t>(sm, L.o_pnn), pa.ne, pa.nvp, R, slot, info);
+                                smp<uint16_t>(sm, L.o_pnn), smp<uint16_t>(sm, L.o_pnoff),
+                                smp<uint16_t>(sm, L.o_pnbr), *smp<uint32_t>(sm, L.o_pconn) != 0,
+                                pa.ne, pa.nvp, R, slot, info);
 }
 
 }  // namespace

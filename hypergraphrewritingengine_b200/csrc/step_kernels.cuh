@@ -127,9 +127,11 @@ struct Layout {
     uint32_t o_pevo, o_vloc, o_cvo, o_bind, o_match, o_mdepth;      // u16
     uint32_t o_pear, o_car;                                         // u8
     uint32_t o_rule;                                                // DevRule
-    // lane-per-child path: parent occurrence lists by vertex, per-vertex degree / neighbour
-    // counts, and a batch of up to 32 matches (removed positions + produced local vertices)
-    uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_batch, o_mlist;
+    // lane-per-child path: parent occurrence and neighbour lists by vertex, per-vertex degree /
+    // neighbour counts, and a batch of up to 32 matches (removed positions + produced local
+    // vertices)
+    uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_pnoff, o_pnbr, o_batch, o_mlist;
+    uint32_t o_pconn;   // u32: 1 when the parent is connected
     // match forwarding: seeded schedule, creating event's consumed edges, delta matches (and a
     // sorted copy), a 32-match chunk of forwarded matches
     uint32_t o_sched2, o_fkc, o_dkey, o_dpos, o_dkey2, o_dpos2, o_fkey, o_fpos;

@@ -16,7 +16,7 @@ int main(int argc, char** argv) {
     const int trials = argc > 1 ? atoi(argv[1]) : 20000;
     std::mt19937_64 rng(12345);
     auto U = [&](int lo, int hi) { return lo + int(rng() % uint64_t(hi - lo + 1)); };
-    int fails = 0;
+    int fails = 0, shortcut = 0;
     for (int t = 0; t < trials; ++t) {
         // parent: ne edges of arity in [amin, amax] over nverts labels
         const int amin = U(1, 3), amax = amin + U(0, 2);
@@ -55,6 +55,8 @@ int main(int argc, char** argv) {
                     }
         }
         poff[nvp] = uint16_t(pocc.size());
+        std::vector<uint16_t> pnoff(nvp + 1, 0), pnbr(pocc.size() * 16);
+        lane_build_nbr(pear.data(), pevo.data(), vloc.data(), uint32_t(ne), nvp, pnoff.data(), pnbr.data());
         // a "match": n_lhs distinct removed positions; produced edges over parent + fresh
         DevRule R;
         std::memset(&R, 0, sizeof(R));
@@ -72,6 +74,7 @@ int main(int argc, char** argv) {
             const int a = U(amin, amax);
             R.rhs_ar[k] = uint8_t(a);
             R.rhs_off[k] = uint8_t(off);
+            for (int q = 0; q < a; ++q) R.rhs_pos_edge[off + q] = uint8_t(k);
             std::vector<uint32_t> pe;
             for (int q = 0; q < a; ++q) {
                 const uint32_t lv = uint32_t(U(0, int(nvp + R.n_fresh) - 1));
@@ -81,6 +84,7 @@ int main(int argc, char** argv) {
             prod.push_back(pe);
             off += a;
         }
+        R.rhs_total = uint8_t(off);
         // explicit child in the reference's edge order
         std::vector<std::vector<uint32_t>> child;
         for (int e = 0; e < ne; ++e) {
@@ -94,17 +98,42 @@ int main(int argc, char** argv) {
         for (uint32_t v = 0; v < nvp; ++v) bound = std::max<uint32_t>(bound, pnn[v]);
         for (int k = 0; k < R.n_rhs; ++k) gain += uint32_t(R.rhs_ar[k]) * (R.rhs_ar[k] - 1u);
         if (bound + gain > 256 || nvp + R.n_fresh > 32) continue;
+        // parent connectivity, and the connectivity shortcut's condition on this child: the
+        // produced edges are connected and hold every vertex of the removed edges
+        std::vector<uint32_t> up(nvp + R.n_fresh);
+        for (uint32_t v = 0; v < up.size(); ++v) up[v] = v;
+        auto root = [&](uint32_t x) { while (up[x] != x) x = up[x]; return x; };
+        for (int e = 0; e < ne; ++e)
+            for (int q = 1; q < pear[e]; ++q) up[root(vloc[pevo[e] + q])] = root(vloc[pevo[e]]);
+        uint32_t proots = 0;
+        for (uint32_t v = 0; v < nvp; ++v) proots += root(v) == v;
+        const bool pconn = proots == 1;
+        for (uint32_t v = 0; v < up.size(); ++v) up[v] = v;
+        std::vector<bool> inp(nvp + R.n_fresh, false);
+        for (int k = 0; k < R.n_rhs; ++k)
+            for (int q = 0; q < R.rhs_ar[k]; ++q) {
+                const uint32_t x = slot[R.n_lhs + R.rhs_off[k] + q];
+                inp[x] = true;
+                up[root(x)] = root(slot[R.n_lhs + R.rhs_off[k]]);
+            }
+        uint32_t rroots = 0;
+        for (uint32_t v = 0; v < up.size(); ++v) rroots += inp[v] && root(v) == v;
+        bool covers = true;
+        for (int k = 0; k < R.n_lhs; ++k)
+            for (int q = 0; q < pear[slot[k]]; ++q) covers = covers && inp[vloc[pevo[slot[k]] + q]];
+        if (R.n_lhs > 0 && rroots == 1 && covers) R.flags |= kRuleRhsJoinsLhs;
         WlInfo info;
         const uint64_t got = lane_wl_core<32, 256>(pear.data(), pevo.data(), vloc.data(), poff.data(),
-                                                   pocc.data(), pdeg.data(), pnn.data(), uint32_t(ne),
-                                                   nvp, R, slot.data(), info);
+                                                   pocc.data(), pdeg.data(), pnn.data(), pnoff.data(),
+                                                   pnbr.data(), pconn, uint32_t(ne), nvp, R, slot.data(), info);
         const uint64_t want = hgx_oracle::wl_hash(child);
+        shortcut += pconn && (R.flags & kRuleRhsJoinsLhs) ? 1 : 0;
         if (got != want) {
             if (fails < 5) std::printf("trial %d: lane %016llx oracle %016llx (ne %d nvp %u)\n", t,
                                        (unsigned long long)got, (unsigned long long)want, ne, nvp);
             ++fails;
         }
     }
-    std::printf("%d / %d mismatches\n", fails, trials);
+    std::printf("%d / %d mismatches (%d with the connectivity shortcut)\n", fails, trials, shortcut);
     return fails ? 1 : 0;
 }

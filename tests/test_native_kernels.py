@@ -22,6 +22,8 @@ def test_lane_wl_matches_oracle(tmp_path):
     out = subprocess.run([str(exe), "20000"], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "0 / 20000 mismatches" in out.stdout
+    # children hashed through the connectivity shortcut (connected parent, joining RHS)
+    assert int(out.stdout.split("(")[1].split()[0]) > 1000, out.stdout
 
 
 def _build_compat(tmp_path):
