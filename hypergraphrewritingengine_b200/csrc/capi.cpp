@@ -221,7 +221,10 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
         case HGX_OPT_RECORD_CAUSAL: e->opt.causal = value != 0; return HGX_OK;
         case HGX_OPT_RECORD_BRANCHIAL: e->opt.branchial = value != 0; return HGX_OK;
         case HGX_OPT_KEEP_STATE_EDGES: e->opt.keep_state_edges = value != 0; return HGX_OK;
-        case HGX_OPT_TIMING: e->engine.set_timing(value != 0); return HGX_OK;
+        case HGX_OPT_TIMING:
+            if (value > 2) return fail(HGX_ERR_INVALID, "timing: 0 off, 1 every stage, 2 the expand kernel only");
+            e->engine.set_timing(static_cast<int>(value));
+            return HGX_OK;
         case HGX_OPT_READBACK: e->opt.readback = value != 0; return HGX_OK;
         case HGX_OPT_FORWARDING:
             if (value > 2) return fail(HGX_ERR_INVALID, "forwarding mode must be 0, 1 or 2");

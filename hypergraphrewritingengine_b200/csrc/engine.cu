@@ -280,7 +280,7 @@ struct PinnedPool {
 struct Engine::Impl {
     int device = 0;
     cudaStream_t st = nullptr;
-    bool timing = false;
+    int timing = 0;   // 0 off, 1 every stage, 2 the expand kernel only
     StageTimes times;
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;   // the join autotuner's measurement window
     // Join autotuner for the lane expand kernel: per bucket b = floor(log2(children per frontier
@@ -332,6 +332,21 @@ struct Engine::Impl {
     std::vector<EvoRanges> evo_ranges;
     std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     uint64_t n_roots_admitted = 0;
+    // the per-level read-backs: packed on the device, one copy each into a page-locked block
+    DVec<unsigned long long> sync_pack;
+    unsigned long long* h_sync = nullptr;
+    size_t h_sync_words = 0;
+    unsigned long long* sync_host(size_t words) {
+        if (words > h_sync_words) {
+            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            if (h_sync) HGX_CUDA_CHECK(cudaFreeHost(h_sync));
+            h_sync = nullptr;
+            const size_t nw = std::max<size_t>(words, 2 * h_sync_words);
+            HGX_CUDA_CHECK(cudaMallocHost(reinterpret_cast<void**>(&h_sync), nw * 8));
+            h_sync_words = nw;
+        }
+        return h_sync;
+    }
 
     // host mirrors
     std::vector<DevRule> h_rules;
@@ -417,6 +432,8 @@ struct Engine::Impl {
         fin_rng.release(st);
         fin_tab.release(st);
         fin_sec.release(st);
+        sync_pack.release(st);
+        if (h_sync) cudaFreeHost(h_sync);
         rules.release(st);
         evos.release(st);
         cudaStreamSynchronize(st);
@@ -508,13 +525,13 @@ struct Engine::Impl {
         }
         return ev_pool[ev_used++];
     }
-    void tic() {
-        if (!timing) return;
+    void tic(bool expand_kernel = false) {
+        if (!(timing == 1 || (timing == 2 && expand_kernel))) return;
         cur_a = next_event();
         HGX_CUDA_CHECK(cudaEventRecord(cur_a, st));
     }
-    void toc(double& acc) {
-        if (!timing) return;
+    void toc(double& acc, bool expand_kernel = false) {
+        if (!(timing == 1 || (timing == 2 && expand_kernel))) return;
         cudaEvent_t b = next_event();
         HGX_CUDA_CHECK(cudaEventRecord(b, st));
         pending.push_back({cur_a, b, &acc});
@@ -1282,22 +1299,26 @@ struct Engine::Impl {
         toc(times.scan);
 
         // ---- sync 1: level totals, per-evolution event ranges, exact frontier maxima
-        uint32_t tot[6];
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[0], item_ev.p + NI, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[1], item_cons.p + NI, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[2], item_prod.p + NI, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[3], item_fresh.p + NI, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&tot[4], level_max.p + 2, 8, cudaMemcpyDeviceToHost, st));
         const size_t nevo = h_evos.size();
-        std::vector<uint32_t> h_first(nevo), h_last(nevo);
-        std::vector<unsigned long long> h_classes(nevo), h_states_ev(nevo), h_sigs(nevo, 0);
-        if (opt.event_keys)
-            HGX_CUDA_CHECK(cudaMemcpyAsync(h_sigs.data(), evo_sigs.p, nevo * 8, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(h_first.data(), evo_first_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(h_last.data(), evo_last_ev.p, nevo * 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(h_classes.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(h_states_ev.data(), evo_states.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+        const size_t w1 = 3 + 4 * nevo;
+        sync_pack.ensure(w1, 0, st);
+        unsigned long long* hs = sync_host(std::max<size_t>(w1, (7 * nevo + 4 + 1) / 2));
+        k_sync1_pack<<<grid_for(std::max<size_t>(nevo, 1), 256), 256, 0, st>>>(
+            item_ev.p, item_cons.p, item_prod.p, item_fresh.p, NI, level_max.p, evo_classes.p,
+            evo_states.p, opt.event_keys ? evo_sigs.p : nullptr, evo_first_ev.p, evo_last_ev.p,
+            static_cast<uint32_t>(nevo), sync_pack.p);
+        check_launch();
+        HGX_CUDA_CHECK(cudaMemcpyAsync(hs, sync_pack.p, w1 * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        const uint32_t tot[6] = {uint32_t(hs[0]), uint32_t(hs[0] >> 32), uint32_t(hs[1]),
+                                 uint32_t(hs[1] >> 32), uint32_t(hs[2]), uint32_t(hs[2] >> 32)};
+        std::vector<uint32_t> h_first(nevo), h_last(nevo);
+        std::vector<unsigned long long> h_classes(hs + 3, hs + 3 + nevo),
+            h_states_ev(hs + 3 + nevo, hs + 3 + 2 * nevo), h_sigs(hs + 3 + 2 * nevo, hs + 3 + 3 * nevo);
+        for (size_t e = 0; e < nevo; ++e) {
+            h_first[e] = uint32_t(hs[3 + 3 * nevo + e]);
+            h_last[e] = uint32_t(hs[3 + 3 * nevo + e] >> 32);
+        }
         auto h_states_now = [&](uint32_t e) { return static_cast<uint64_t>(h_states_ev[e]); };
         const uint32_t n_ev = tot[0], n_cons_lv = tot[1], n_prod = tot[2], n_fresh = tot[3];
         const uint32_t fmax_ne = tot[4], fmax_nocc = tot[5];
@@ -1389,7 +1410,7 @@ struct Engine::Impl {
                 A.f_begin = 0;
                 A.f_end = n_work;
                 HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, 2 * sizeof(uint32_t), st));
-                tic();
+                tic(true);
                 if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_a, st));
                 if (cross && walk) k_expand_lanes2<true, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 else if (cross) k_expand_lanes2<false, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
@@ -1397,7 +1418,7 @@ struct Engine::Impl {
                 else k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 check_launch();
                 if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_b, st));
-                toc(times.expand);
+                toc(times.expand, true);
                 ++times.expand_launches;
                 if (walk) ++times.walk_launches;
                 tic();
@@ -1591,23 +1612,22 @@ struct Engine::Impl {
         // per-evolution ranges of this level (events kept, new states, branchial pairs)
         A.state_base = static_cast<uint32_t>(n_states);
         A.bbase = static_cast<uint32_t>(n_bpairs);
-        lvl_ranges.ensure(7 * nevo, 0, st);
+        lvl_ranges.ensure(7 * nevo + 4, 0, st);
         if (ne2 || F_eff) {
             A.n_frontier = F;   // boundaries over the whole frontier; event ranges clamp to ne2
             k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, lvl_ranges.p);
             check_launch();
             A.n_frontier = F_eff;
         }
-        std::vector<uint32_t> h_rng(7 * nevo);
-        HGX_CUDA_CHECK(cudaMemcpyAsync(h_rng.data(), lvl_ranges.p, 7 * nevo * 4, cudaMemcpyDeviceToHost, st));
-
-        // ---- sync 2: new states, next frontier, branchial pairs, errors
-        uint32_t s2[4];
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[0], flag_rep.p + ne2, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[1], flag_front.p + ne2, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[2], boff.p + ne2, 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(&s2[3], err.p, 4, cudaMemcpyDeviceToHost, st));
+        // ---- sync 2: new states, next frontier, branchial pairs, errors (behind the ranges)
+        k_sync2_pack<<<1, 32, 0, st>>>(flag_rep.p, flag_front.p, boff.p, ne2, err.p,
+                                       lvl_ranges.p + 7 * nevo);
+        check_launch();
+        uint32_t* hs2 = reinterpret_cast<uint32_t*>(sync_host((7 * nevo + 4 + 1) / 2));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(hs2, lvl_ranges.p, (7 * nevo + 4) * 4, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        const std::vector<uint32_t> h_rng(hs2, hs2 + 7 * nevo);
+        const uint32_t* s2 = hs2 + 7 * nevo;
         if (tune) {
             float ms = 0;
             HGX_CUDA_CHECK(cudaEventElapsedTime(&ms, ev_a, ev_b));
@@ -1764,7 +1784,7 @@ uint64_t Engine::estimate_bytes(const EvolutionSpec& spec) {
     return states * per_state + states * 8 * 96 + states * 64;
 }
 cudaStream_t Engine::stream() const { return impl_->st; }
-void Engine::set_timing(bool on) { impl_->timing = on; }
+void Engine::set_timing(int level) { impl_->timing = level; }
 const StageTimes& Engine::times() const { return impl_->times; }
 void Engine::sync() { HGX_CUDA_CHECK(cudaStreamSynchronize(impl_->st)); }
 

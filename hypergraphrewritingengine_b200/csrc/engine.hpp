@@ -147,7 +147,7 @@ public:
     static uint64_t estimate_bytes(const EvolutionSpec& spec);
 
     cudaStream_t stream() const;
-    void set_timing(bool on);
+    void set_timing(int level);   // 0 off, 1 every stage, 2 the expand kernel only
     const StageTimes& times() const;
     void sync();
 

@@ -1489,6 +1489,43 @@ __global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t
 // one contiguous range (the frontier is grouped by evolution and everything is numbered in
 // frontier order). out[evo * 7 + {0..6}] = event first/end, state first/end, pair first/end, and
 // the evolution's states in the next frontier.
+// A level's first read-back in one copy: out[0..2] = event / consumed, produced / fresh totals and
+// the frontier's largest edge / occurrence counts (low | high << 32), then per evolution its
+// classes, states, event signatures (sigs may be null) and first | last event << 32.
+__global__ void k_sync1_pack(const uint32_t* item_ev, const uint32_t* item_cons,
+                             const uint32_t* item_prod, const uint32_t* item_fresh, uint32_t ni,
+                             const uint32_t* level_max, const unsigned long long* classes,
+                             const unsigned long long* states, const unsigned long long* sigs,
+                             const uint32_t* first, const uint32_t* last, uint32_t nevo,
+                             unsigned long long* out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    using u64 = unsigned long long;
+    if (t == 0) {
+        out[0] = item_ev[ni] | (u64(item_cons[ni]) << 32);
+        out[1] = item_prod[ni] | (u64(item_fresh[ni]) << 32);
+        out[2] = level_max[2] | (u64(level_max[3]) << 32);
+    }
+    for (uint32_t e = t; e < nevo; e += gridDim.x * blockDim.x) {
+        out[3 + e] = classes[e];
+        out[3 + nevo + e] = states[e];
+        out[3 + 2ull * nevo + e] = sigs ? sigs[e] : 0ull;
+        out[3 + 3ull * nevo + e] = first[e] | (u64(last[e]) << 32);
+    }
+}
+
+// The level's second read-back rides behind the per-evolution ranges: new states, next-frontier
+// states, branchial pairs and the error flags.
+__global__ void k_sync2_pack(const uint32_t* flag_rep, const uint32_t* flag_front,
+                             const uint32_t* boff, uint32_t ne2, const uint32_t* err,
+                             uint32_t* out) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        out[0] = flag_rep[ne2];
+        out[1] = flag_front[ne2];
+        out[2] = boff[ne2];
+        out[3] = *err;
+    }
+}
+
 __global__ void k_evo_ranges(DevPtrs P, LevelArgs A, const uint32_t* evo_last, uint32_t* out) {
     for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
          f += gridDim.x * blockDim.x) {

@@ -65,7 +65,8 @@ typedef enum hgx_option {
     /* EvolveInput::edge_identity (gpu/include/hg_gpu/evolve.hpp:36): read back every state's
        edge record (ids, arities, vertices). */
     HGX_OPT_KEEP_STATE_EDGES = 5,
-    /* 1 = record per-stage device times (CUDA events on the engine stream). */
+    /* 1 = record per-stage device times (CUDA events on the engine stream); 2 = time the expand
+       kernel launches only (two events per launch; the other stages read 0). */
     HGX_OPT_TIMING = 6,
     /* 1 (default) = copy the result to host memory; 0 = keep it on the device and report the
        counts only (hgx_result_count works, hgx_result_copy returns empty arrays). */
