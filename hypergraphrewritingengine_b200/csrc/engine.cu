@@ -319,7 +319,7 @@ struct Engine::Impl {
     DVec<uint8_t> fmode, fin;
     DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e, frng, slice_off;
     DVec<unsigned long long> evo_new, ev_anc, ev_sig, evo_sigs;
-    DVec<uint32_t> ev_bkey;
+    DVec<unsigned long long> ev_bmask;
     DVec<uint64_t> fin_rng;
     DVec<uint32_t> fin_tab;   // many-evolution finalisation: bases, rule starts, boundary values
     DVec<uint64_t> fin_sec;   // many-evolution finalisation: section offsets
@@ -422,7 +422,7 @@ struct Engine::Impl {
         slice_off.release(st);
         evo_new.release(st);
         ev_anc.release(st);
-        ev_bkey.release(st);
+        ev_bmask.release(st);
         ev_sig.release(st);
         evo_sigs.release(st);
         lvl_ranges.release(st);
@@ -493,7 +493,7 @@ struct Engine::Impl {
         P.ev_cons = ev_cons.p;
         P.ev_cprod = ev_cprod.p;
         P.ev_anc = ev_anc.p;
-        P.ev_bkey = ev_bkey.p;
+        P.ev_bmask = ev_bmask.p;
         P.ev_sig = ev_sig.p;
         P.evo_sigs = evo_sigs.p;
         P.state_of_arrival = state_of_arrival.p;
@@ -1329,7 +1329,7 @@ struct Engine::Impl {
 
         // capacity
         grow_events(n_events + n_ev);
-        ev_bkey.ensure(n_events + n_ev, n_events, st);
+        ev_bmask.ensure(n_events + n_ev, n_events, st);
         ev_cons.ensure(n_cons + n_cons_lv, n_cons, st);
         ev_cprod.ensure(n_cons + n_cons_lv, n_cons, st);
         edge_creator.ensure(n_edges + n_prod, n_edges, st);

@@ -1145,14 +1145,14 @@ __global__ void k_item_sizes(DevPtrs P, LevelArgs A) {
     }
 }
 
-// An event's consumed parent positions packed for the branchial test (events of one input state
-// share the parent's positions, so equal positions are equal edges): (n << 24) | one byte per
-// position, or kNone when the rule consumes more than three edges or the parent has more than 256.
-__device__ __forceinline__ uint32_t branch_key(uint32_t n, uint32_t pne, const uint8_t* pos) {
-    if (n == 0 || n > 3 || pne > 256) return kNone;
-    uint32_t w = n << 24;
-    for (uint32_t k = 0; k < n; ++k) w |= uint32_t(pos[k]) << (8u * k);
-    return w;
+// An event's consumed parent positions as a bit mask for the branchial test (events of one input
+// state share the parent's positions, so equal positions are equal edges), or 0 when the parent
+// has more than 64 edges (the test then compares edge ids).
+__device__ __forceinline__ unsigned long long branch_mask(uint32_t n, uint32_t pne, const uint8_t* pos) {
+    if (pne > 64) return 0ull;
+    unsigned long long m = 0;
+    for (uint32_t k = 0; k < n; ++k) m |= 1ull << pos[k];
+    return m;
 }
 
 // Frontier position of work index w (identity unless the level runs over a list of ranges).
@@ -1261,7 +1261,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                 P.ev_fresh[e] = fresh0 + idx * R.n_fresh;
                 P.ev_hash[e] = h;
                 for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = peid[rpos[k]];
-                P.ev_bkey[e] = branch_key(R.n_lhs, pa.ne, rpos);
+                P.ev_bmask[e] = branch_mask(R.n_lhs, pa.ne, rpos);
                 for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
                 table_insert(P, ev, h, e);
                 const uint64_t k = R.n_lhs, rr = R.n_rhs;
@@ -1593,7 +1593,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
             P.ev_fresh[e] = ri.fresh0 + idx * R.n_fresh;
             P.ev_hash[e] = h;
             for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = peid[slot[k]];
-            P.ev_bkey[e] = branch_key(R.n_lhs, pa.ne, slot);
+            P.ev_bmask[e] = branch_mask(R.n_lhs, pa.ne, slot);
             for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
             slot_insert(P, ri.table_off, ri.table_mask, h, e);
             const uint64_t k = R.n_lhs, rr = R.n_rhs;
@@ -2045,7 +2045,7 @@ __global__ void k_void(DevPtrs P, LevelArgs A, uint32_t n) {
                 P.ev_hash[e] = 0;
                 P.ev_out[e] = kNone;
                 for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = 0;   // edge 0 exists
-                P.ev_bkey[e] = kNone;
+                P.ev_bmask[e] = 0ull;
                 for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
                 A.flag_new[lo + idx] = 0;
             }
@@ -2298,21 +2298,16 @@ __global__ void k_bpairs(DevPtrs P, LevelArgs A) {
         if (P.ev_kept[a]) {
             const uint32_t in = P.ev_in[a];
             const uint32_t na = P.rules[P.ev_rule[a]].n_lhs, ca0 = P.ev_coff[a];
-            const uint32_t ka = P.ev_bkey[a];
+            const unsigned long long ma = P.ev_bmask[a];
             uint32_t ca[kMaxPatternEdges];
             for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[ca0 + k];
             uint32_t out = kEmit ? A.boff[t] : 0u;
             for (uint32_t c = a + 1; c < end && P.ev_in[c] == in; ++c) {
                 if (!P.ev_kept[c]) continue;
-                const uint32_t kc = P.ev_bkey[c];
+                const unsigned long long mc = P.ev_bmask[c];
                 bool share = false;
-                if (ka != kNone && kc != kNone) {
-                    // packed parent positions: any byte of one equals any byte of the other
-                    const uint32_t nka = ka >> 24, nkc = kc >> 24;
-                    for (uint32_t i = 0; i < nkc && !share; ++i) {
-                        const uint32_t x = (kc >> (8u * i)) & 0xFFu;
-                        for (uint32_t m = 0; m < nka; ++m) share |= ((ka >> (8u * m)) & 0xFFu) == x;
-                    }
+                if (ma && mc) {
+                    share = (ma & mc) != 0ull;   // a consumed parent position in common
                 } else {
                     const uint32_t nc = P.rules[P.ev_rule[c]].n_lhs, cc0 = P.ev_coff[c];
                     for (uint32_t k = 0; k < nc && !share; ++k) {

@@ -63,9 +63,9 @@ struct DevPtrs {
     // transitive reduction: per event, bit d set = an event at level d is a proper causal
     // ancestor (levels < 64; an event's ancestors lie on its input state's history chain)
     unsigned long long* ev_anc;
-    // per event: the parent positions it consumed, packed for the branchial test -- (n << 24) |
-    // positions one byte each (n <= 3 LHS edges, positions < 256), or kNone (compare edge ids)
-    uint32_t* ev_bkey;
+    // per event: the parent positions it consumed as a bit mask for the branchial test, or 0 when
+    // the parent has more than 64 edges (compare edge ids)
+    unsigned long long* ev_bmask;
     // event canonicalisation: per event its signature; per evolution the distinct signatures
     unsigned long long* ev_sig;
     unsigned long long* evo_sigs;
