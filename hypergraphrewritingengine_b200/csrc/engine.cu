@@ -456,6 +456,7 @@ struct Engine::Impl {
         next_vertex = arena_words = tab_slots = 0;
         frontier_size = 0;
         ne_bound = nocc_bound = 1;
+        hist = LevelHist{};
         HGX_CUDA_CHECK(cudaMemsetAsync(arena_top.p, 0, sizeof(unsigned long long), st));
         HGX_CUDA_CHECK(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), st));
         times = StageTimes{};
@@ -1236,9 +1237,84 @@ struct Engine::Impl {
     }
 
     // ---- one level for every evolution in the frontier ---------------------------------------
+    //
+    // A single evolution under a state cap that the previous level's ratios (events per frontier
+    // state, events per new state) place well inside this level's frontier is processed as two
+    // frontier ranges in canonical order: a prefix sized to hold the cut, then the rest only if the
+    // cap was not reached. Events, states and pairs keep their canonical numbering (the second range
+    // follows the first), so the result is the one-pass result; the unexpanded tail is never counted.
+    struct LevelHist {
+        bool valid = false;
+        double ev_per_state = 0, ev_per_new = 0;
+    } hist;
+    uint32_t sub_nf = 0;                           // next-frontier states written by earlier ranges
+    uint64_t sub_ne = 0, sub_no = 0, sub_ev = 0, sub_new = 0;
+    std::vector<uint64_t> sub_front;               // per evolution: next-frontier states so far
+    std::vector<uint8_t> sub_part;                 // per evolution: in this level's frontier
+
     bool level(const RunOptions& opt) {
         const uint32_t F = frontier_size;
         if (F == 0) return false;
+        const size_t nevo = h_evos.size();
+        sub_nf = 0;
+        sub_ne = sub_no = sub_ev = sub_new = 0;
+        sub_front.assign(nevo, 0);
+        sub_part.assign(nevo, 0);
+        uint32_t P = F;
+        const bool one_capped = nevo == 1 && !evo_done[0] && h_evos[0].max_states;
+        if (one_capped && opt.level_split >= 2) {
+            if (F > opt.level_split) P = static_cast<uint32_t>(opt.level_split);
+        } else if (one_capped && opt.level_split == 0 && hist.valid && F >= 4096) {
+            unsigned long long have[2];
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&have[0], evo_classes.p, 8, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&have[1], evo_states.p, 8, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            const uint64_t h = h_evos[0].quotient ? have[0] : have[1];
+            const uint64_t remaining = h_evos[0].max_states > h ? h_evos[0].max_states - h : 0;
+            const double need = double(remaining) * (h_evos[0].quotient ? hist.ev_per_new : 1.0);
+            const double est = need / std::max(hist.ev_per_state, 1e-9) * 1.15 + 256;
+            if (est < 0.8 * double(F)) P = static_cast<uint32_t>(est);
+        }
+        level_range(opt, 0, P);
+        bool cut = false;
+        if (P < F) {
+            uint32_t stopped = 0;
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&stopped, evo_stopped.p, 4, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            if (!stopped) level_range(opt, P, F);
+            HGX_CUDA_CHECK(cudaMemcpyAsync(&stopped, evo_stopped.p, 4, cudaMemcpyDeviceToHost, st));
+            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            // a level with a cut sends none of the evolution's new states on (the cut range has
+            // sent none of its own; the earlier range's are dropped here)
+            cut = stopped != 0;
+            if (cut) {
+                sub_nf = 0;
+                sub_front[0] = 0;
+            }
+        }
+        // the next level's estimate, from a level expanded whole
+        if (P == F && sub_ev && sub_new) {
+            hist.valid = true;
+            hist.ev_per_state = double(sub_ev) / double(F);
+            hist.ev_per_new = double(sub_ev) / double(sub_new);
+        }
+        // which evolutions still have a frontier
+        for (size_t e = 0; e < nevo; ++e)
+            if (sub_part[e] && !evo_done[e] && sub_front[e] == 0) {
+                evo_done[e] = 1;
+                finished.push_back(static_cast<uint32_t>(e));
+            }
+        std::swap(frontier, next_frontier);
+        frontier_size = sub_nf;
+        ne_bound = static_cast<uint32_t>(sub_ne);
+        nocc_bound = static_cast<uint32_t>(sub_no);
+        return frontier_size > 0;
+    }
+
+    // Frontier range [f0, f1) of the current level.
+    void level_range(const RunOptions& opt, uint32_t f0, uint32_t f1) {
+        const uint32_t F = f1 - f0;
+        if (F == 0) return;
         const uint32_t R = rm.stride;
         const uint64_t items = uint64_t(F) * R;
         if (items + 1 > 0xFFFFFFFFull) throw std::runtime_error("hgx: frontier too large for one level");
@@ -1251,7 +1327,7 @@ struct Engine::Impl {
 
         LevelArgs A;
         std::memset(&A, 0, sizeof(A));
-        A.frontier = frontier.p;
+        A.frontier = frontier.p + f0;
         A.n_frontier = F;
         A.rules_stride = R;
         A.counts = counts.p;
@@ -1655,14 +1731,14 @@ struct Engine::Impl {
 
         grow_states(n_states + n_new);
         new_state_event.ensure(n_new, 0, st);
-        next_frontier.ensure(n_front, 0, st);
+        next_frontier.ensure(uint64_t(sub_nf) + n_front, sub_nf, st);
         const uint64_t max_ne = uint64_t(fmax_ne) + rm.grow_e, max_no = uint64_t(fmax_nocc) + rm.grow_o;
         const uint64_t rec_words = max_ne + (max_ne + 3) / 4 + max_no;
         arena.ensure(arena_words + uint64_t(n_new) * rec_words, arena_words, st);
         bpairs.ensure(2ull * (n_bpairs + n_b), 2ull * n_bpairs, st);
         A.state_base = static_cast<uint32_t>(n_states);
         A.new_state_event = new_state_event.p;
-        A.next_frontier = next_frontier.p;
+        A.next_frontier = next_frontier.p + sub_nf;
         A.bpairs = bpairs.p;
         A.bbase = static_cast<uint32_t>(n_bpairs);
         if (ne2) {
@@ -1694,11 +1770,11 @@ struct Engine::Impl {
             toc(times.branchial);
         }
 
-        // which evolutions still have a frontier (their next-frontier counts came with sync 2)
+        // the evolutions of this range and their next-frontier counts (from sync 2)
         for (size_t e = 0; e < nevo; ++e)
-            if (!evo_done[e] && h_first[e] != kNone && h_rng[7 * e + 6] == 0) {
-                evo_done[e] = 1;
-                finished.push_back(static_cast<uint32_t>(e));
+            if (!evo_done[e] && h_first[e] != kNone) {
+                sub_part[e] = 1;
+                sub_front[e] += h_rng[7 * e + 6];
             }
 
         // advance (id ranges of produced edges / fresh vertices / consumed lists were reserved for
@@ -1710,11 +1786,11 @@ struct Engine::Impl {
         n_states += n_new;
         n_bpairs += n_b;
         arena_words += uint64_t(n_new) * rec_words;   // host bound >= the device bump pointer
-        std::swap(frontier, next_frontier);
-        frontier_size = n_front;
-        ne_bound = static_cast<uint32_t>(max_ne);
-        nocc_bound = static_cast<uint32_t>(max_no);
-        return frontier_size > 0;
+        sub_nf += n_front;
+        sub_ne = std::max(sub_ne, max_ne);
+        sub_no = std::max(sub_no, max_no);
+        sub_ev += n_ev;
+        sub_new += n_new;
     }
 };
 

@@ -101,6 +101,8 @@ struct RunOptions {
     // Join of the lane (small-state) expand kernel: 0 = autotuned per bucket of children per
     // frontier state, 1 = warp join, 2 = lane-parallel walk. Results are identical.
     uint32_t lane_join = 0;
+    // Capped single evolution: 0 = split a level at the estimated cut, 1 = never, N >= 2 = at N.
+    uint64_t level_split = 0;
 };
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.

@@ -93,7 +93,13 @@ typedef enum hgx_option {
     /* Join of the small-state expand kernel: 0 (default) = chosen per level by the engine's
        autotuner (device time per child, per bucket of children per frontier state), 1 = warp join,
        2 = lane-parallel walk. No reference counterpart; results are identical. */
-    HGX_OPT_LANE_JOIN = 11
+    HGX_OPT_LANE_JOIN = 11,
+    /* A single evolution under a state cap: a level whose cut the previous level's ratios place
+       early in its frontier is counted and expanded as a frontier prefix first, the rest only if
+       the cap is not reached. 0 (default) = prefix sized by that estimate, 1 = never split,
+       N >= 2 = a prefix of N frontier states whenever the frontier is larger (for tests). No
+       reference counterpart; results are identical for every value. */
+    HGX_OPT_LEVEL_SPLIT = 12
 } hgx_option;
 
 /* One evolution of a batch or a served request. */

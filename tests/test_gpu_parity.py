@@ -185,6 +185,27 @@ def test_capped_rounds_match_oracle(engine, chunk_min):
         engine.set_option(api.OPT_CHUNK_MIN, 8192)
 
 
+@pytest.mark.parametrize("split", [2000, 9000, 1])
+def test_level_split_matches_oracle(engine, split):
+    """A capped single evolution whose levels are counted and expanded as a frontier prefix and
+    then the rest: prefixes that hold the cut, prefixes that end before it (the second range
+    runs, and a cut there drops the first range's next frontier), and no split at all."""
+    from hypergraphrewritingengine_b200 import api
+    engine.set_option(api.OPT_LEVEL_SPLIT, split)
+    try:
+        for cap in (26_700, 60_000, 100_000, 0):
+            res = engine.evolve([cases.C2_RULE], [cases.C2_INIT], 7, quotient=True, max_states=cap)
+            ref = pyoracle.evolve([cases.C2_RULE], [cases.C2_INIT], 7, quotient=True, max_states=cap)
+            assert res.truncated == ref["truncated"], cap
+            assert_same(norm_gpu(res), norm_oracle(ref), f"cap {cap} split {split}")
+        res = engine.evolve([cases.C1_RULE], [cases.C1_INIT], 6, quotient=False, max_states=50_000)
+        ref = pyoracle.evolve([cases.C1_RULE], [cases.C1_INIT], 6, quotient=False, max_states=50_000)
+        assert res.truncated == ref["truncated"]
+        assert_same(norm_gpu(res), norm_oracle(ref), f"full cap split {split}")
+    finally:
+        engine.set_option(api.OPT_LEVEL_SPLIT, 0)
+
+
 @pytest.mark.parametrize("join", [1, 2])
 def test_lane_join_variants_match_oracle(engine, join):
     """Both joins of the small-state expand kernel (the autotuner's choices) give the same result."""
