@@ -1593,7 +1593,9 @@ struct Engine::Impl {
                         uint64_t want = need;
                         if (h_evos[c.evo].quotient && c.ev_built) {
                             want = c.got ? need * c.ev_built / c.got : c.ev_built;
-                            want += want / 4 + 32;
+                            // margin: 1/20 for a lone capped evolution (a short round costs one more
+                            // round), 1/4 with many (another round runs while any one is short)
+                            want += want / (capped.size() == 1 ? 20 : 4) + 32;
                         }
                         if (round >= 12) want = UINT64_MAX;
                         const uint64_t goal = fev(c.built) + std::min<uint64_t>(want, UINT64_MAX / 2);
