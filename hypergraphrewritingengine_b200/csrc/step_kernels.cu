@@ -2186,12 +2186,23 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
          g += (gridDim.x * blockDim.x) >> 5) {
         const uint32_t jl = g * 32 + lane;
         uint32_t words = 0, gne = 0, gnocc = 0;
+        // lane k loads state k's event, parent and rule once; the serial loop below takes them
+        // by shuffle instead of repeating the chain of dependent loads per state
+        uint32_t e_l = 0, f_l = 0, r_l = 0, pne_l = 0, pnocc_l = 0, coff_l = 0, pid_l = 0, fid_l = 0;
+        unsigned long long poff_l = 0;
         if (jl < n_new) {
-            const uint32_t e = A.new_state_event[jl];
-            const uint32_t f = P.ev_in[e];
-            const DevRule& R = P.rules[P.ev_rule[e]];
-            gne = P.st_ne[f] - R.n_lhs + R.n_rhs;
-            gnocc = P.st_nocc[f] - R.lhs_total + R.rhs_total;
+            e_l = A.new_state_event[jl];
+            f_l = P.ev_in[e_l];
+            r_l = P.ev_rule[e_l];
+            coff_l = P.ev_coff[e_l];
+            pid_l = P.ev_prod[e_l];
+            fid_l = P.ev_fresh[e_l];
+            const DevRule& R = P.rules[r_l];
+            pne_l = P.st_ne[f_l];
+            pnocc_l = P.st_nocc[f_l];
+            poff_l = P.st_off[f_l];
+            gne = pne_l - R.n_lhs + R.n_rhs;
+            gnocc = pnocc_l - R.lhs_total + R.rhs_total;
             words = gne + ((gne + 3) >> 2) + gnocc;
         }
         const uint32_t inc = warp_incl_scan(words);
@@ -2214,12 +2225,12 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
         for (uint32_t k = 0; k < cnt; ++k) {
             const uint32_t j = g * 32 + k;
             const unsigned long long off = __shfl_sync(0xFFFFFFFFu, my_off, k);
-            const uint32_t e = A.new_state_event[j];
             const uint32_t sid = A.state_base + j;
-            const uint32_t f = P.ev_in[e];
-            const DevRule& R = P.rules[P.ev_rule[e]];
-            const uint32_t pne = P.st_ne[f], pnocc = P.st_nocc[f];
-            const uint32_t* prec = P.arena + P.st_off[f];
+            const DevRule& R = P.rules[__shfl_sync(0xFFFFFFFFu, r_l, k)];
+            const uint32_t pne = __shfl_sync(0xFFFFFFFFu, pne_l, k);
+            const uint32_t pnocc = __shfl_sync(0xFFFFFFFFu, pnocc_l, k);
+            const uint32_t coff = __shfl_sync(0xFFFFFFFFu, coff_l, k);
+            const uint32_t* prec = P.arena + __shfl_sync(0xFFFFFFFFu, poff_l, k);
             const uint32_t paw = (pne + 3) >> 2;
             const uint32_t ne = pne - R.n_lhs + R.n_rhs;
             const uint32_t nocc = pnocc - R.lhs_total + R.rhs_total;
@@ -2227,7 +2238,7 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
             uint32_t* rec = P.arena + off;
             uint8_t* rar = reinterpret_cast<uint8_t*>(rec + ne);
             uint32_t* rv = rec + ne + aw;
-            if (lane < R.n_lhs) cons[lane] = P.ev_cons[P.ev_coff[e] + lane];
+            if (lane < R.n_lhs) cons[lane] = P.ev_cons[coff + lane];
             for (uint32_t t = lane; t < aw; t += 32) rec[ne + t] = 0;   // arity padding bytes
             __syncwarp();
             // kept parent edges; a consumed edge binds its pattern edge's variables instead
@@ -2263,7 +2274,8 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
             }
             __syncwarp();
             // produced edges
-            const uint32_t pid = P.ev_prod[e], fid = P.ev_fresh[e];
+            const uint32_t pid = __shfl_sync(0xFFFFFFFFu, pid_l, k);
+            const uint32_t fid = __shfl_sync(0xFFFFFFFFu, fid_l, k);
             for (uint32_t k2 = lane; k2 < R.n_rhs; k2 += 32) {
                 rec[run_e + k2] = pid + k2;
                 rar[run_e + k2] = R.rhs_ar[k2];
