@@ -374,7 +374,9 @@ struct Engine::Impl {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
         // (the cross-parent lane kernel also has ~2 KB of static shared memory per block)
         for (const void* k : {(const void*)k_expand_lanes2<false, kLaneRegions>,
-                              (const void*)k_expand_lanes2<true, kLaneRegions>})
+                              (const void*)k_expand_lanes2<true, kLaneRegions>,
+                              (const void*)k_expand_lanes2<false, kLaneRegions, false>,
+                              (const void*)k_expand_lanes2<true, kLaneRegions, false>})
             HGX_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 static_cast<int>(kMaxDynSmem - 8192)));
         for (const void* k : {(const void*)k_count, (const void*)k_expand<true>,
@@ -1477,8 +1479,10 @@ struct Engine::Impl {
             Layout Ll2 = Ll;
             Ll2.bytes = kLaneRegions * Ll.bytes;
             const bool cross = rm.stride == 1 && Ll2.bytes <= (kMaxDynSmem - 8192) / 2;
-            LaunchShape sl = cross ? (walk ? warp_shape(k_expand_lanes2<true, kLaneRegions>, Ll2, F)
-                                           : warp_shape(k_expand_lanes2<false, kLaneRegions>, Ll2, F))
+            LaunchShape sl = cross ? (walk ? (fwd ? warp_shape(k_expand_lanes2<true, kLaneRegions>, Ll2, F)
+                                                  : warp_shape(k_expand_lanes2<true, kLaneRegions, false>, Ll2, F))
+                                           : (fwd ? warp_shape(k_expand_lanes2<false, kLaneRegions>, Ll2, F)
+                                                  : warp_shape(k_expand_lanes2<false, kLaneRegions, false>, Ll2, F)))
                                    : (walk ? warp_shape(k_expand<true, true>, Ll, F)
                                            : warp_shape(k_expand<true>, Ll, F));
             LaunchShape sw = warp_shape(k_expand<false>, Lw, n_ev);   // work units: slices
@@ -1488,8 +1492,11 @@ struct Engine::Impl {
                 HGX_CUDA_CHECK(cudaMemsetAsync(work.p + 1, 0, 2 * sizeof(uint32_t), st));
                 tic(true);
                 if (tune) HGX_CUDA_CHECK(cudaEventRecord(ev_a, st));
-                if (cross && walk) k_expand_lanes2<true, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
-                else if (cross) k_expand_lanes2<false, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                // levels without forwarding run the lane kernel compiled without its paths
+                if (cross && walk && fwd) k_expand_lanes2<true, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                else if (cross && walk) k_expand_lanes2<true, kLaneRegions, false><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                else if (cross && fwd) k_expand_lanes2<false, kLaneRegions><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
+                else if (cross) k_expand_lanes2<false, kLaneRegions, false><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 else if (walk) k_expand<true, true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 else k_expand<true><<<sl.grid, sl.block, sl.smem, st>>>(ptrs(), A, Ll);
                 check_launch();

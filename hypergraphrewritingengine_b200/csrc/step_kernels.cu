@@ -1558,7 +1558,8 @@ struct LaneRegion {
     uint64_t table_off, table_mask;
 };
 
-template <bool kWalk, int kReg = 2>
+// kFwd = false: a level without match forwarding, compiled without its paths (a smaller kernel).
+template <bool kWalk, int kReg = 2, bool kFwd = true>
 __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A, Layout L) {
     extern __shared__ __align__(16) char smem[];
     __shared__ LaneRegion rinfo_sm[8][kReg];
@@ -1655,7 +1656,9 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
             rinfo[cur] = ri;
         }
         __syncwarp();
-        const Fwd fwd = fwd_prepare(P, A, L, sm, R, ev, pa, sid, (fm & 2u) != 0);
+        Fwd fwd;
+        fwd.on = false;
+        if constexpr (kFwd) fwd = fwd_prepare(P, A, L, sm, R, ev, pa, sid, (fm & 2u) != 0);
         if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= kLaneJoinCap) {
             uint32_t* mlist = smp<uint32_t>(sm, L.o_mlist);
             const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
@@ -1709,7 +1712,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
             const uint16_t* match = smp<uint16_t>(sm, L.o_match);
             const uint16_t* bind = smp<uint16_t>(sm, L.o_bind);
             uint32_t idx = 0;
-            enumerate_matches(P, L, sm, R, pa, fwd, [&](uint32_t nm) {
+            auto on_match = [&](uint32_t nm) {
                 uint8_t* slot = batch + nb * L.SB;
                 if (lane < R.n_lhs) slot[lane] = static_cast<uint8_t>(match[lane]);
                 for (uint32_t t = lane; t < R.rhs_total; t += 32) {
@@ -1723,7 +1726,9 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
                 ++nb;
                 held |= 1u << cur;
                 if (nb == 32) flush();
-            });
+            };
+            if constexpr (kFwd) enumerate_matches(P, L, sm, R, pa, fwd, on_match);
+            else warp_join(L, sm, R, pa, R.sched, -1, on_match);
         }
         cur = cur + 1 == kReg ? 0u : cur + 1;
     }
