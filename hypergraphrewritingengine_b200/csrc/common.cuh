@@ -9,8 +9,10 @@
 
 #ifdef __CUDACC__
 #define HGX_HD __host__ __device__ __forceinline__
+#define HGX_NOINLINE __host__ __device__ __noinline__
 #else
 #define HGX_HD inline
+#define HGX_NOINLINE inline
 #endif
 
 namespace hgx {

@@ -82,6 +82,73 @@ HGX_HD uint32_t lane_distinct(const uint64_t* cur, const uint16_t* deg, uint32_t
     return d;
 }
 
+// Component term of a connected child.
+HGX_HD uint64_t lane_one_component(uint32_t ne, uint32_t nv, uint64_t vs) {
+    return smix(fnv(fnv(kFnvOffset, (static_cast<uint64_t>(ne) << 32) | nv), vs));
+}
+
+// Component term of a child whose connectivity is not known from its parent: union-find over its
+// edges, then per component smix(fnv(fnv(offset, edges << 32 | vertices), sum of vertex terms)).
+// Kept out of line: the expand kernel's hot path (connected children) stays small.
+template <int VM>
+HGX_NOINLINE uint64_t lane_component_term(const uint8_t* pear, const uint16_t* pevo,
+                                          const uint16_t* vloc, uint32_t pne, const DevRule& R,
+                                          const uint8_t* prodv, uint64_t rmask,
+                                          const uint16_t* deg, const uint64_t* vterm, uint32_t V,
+                                          uint32_t ne, uint32_t nv, uint64_t vs) {
+    uint8_t comp[VM];
+        #pragma unroll 1
+    for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(v);
+    auto find = [&](uint32_t x) -> uint32_t {
+        while (comp[x] != x) { comp[x] = comp[comp[x]]; x = comp[x]; }
+        return x;
+    };
+        #pragma unroll 1
+    for (uint32_t e = 0; e < pne; ++e) {
+        if ((rmask >> e) & 1ull) continue;
+        const uint32_t a = pear[e], vo = pevo[e];
+        const uint32_t r = find(vloc[vo]);
+                #pragma unroll 1
+        for (uint32_t q = 1; q < a; ++q) {
+            const uint32_t x = find(vloc[vo + q]);
+            if (x != r) comp[x] = static_cast<uint8_t>(r);
+        }
+    }
+        #pragma unroll 1
+    for (uint32_t k = 0; k < R.n_rhs; ++k) {
+        const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+        const uint32_t r = find(prodv[o]);
+                #pragma unroll 1
+        for (uint32_t q = 1; q < a; ++q) {
+            const uint32_t x = find(prodv[o + q]);
+            if (x != r) comp[x] = static_cast<uint8_t>(r);
+        }
+    }
+        #pragma unroll 1
+    for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(find(v));
+    uint32_t roots = 0;
+        #pragma unroll 1
+    for (uint32_t v = 0; v < V; ++v) roots += (deg[v] && comp[v] == v) ? 1u : 0u;
+    if (roots == 1) return lane_one_component(ne, nv, vs);
+    uint64_t cs = 0;
+        #pragma unroll 1
+    for (uint32_t r = 0; r < V; ++r) {
+        if (!deg[r] || comp[r] != r) continue;
+        uint64_t col = 0, vc = 0, ec = 0;
+                #pragma unroll 1
+        for (uint32_t v = 0; v < V; ++v)
+            if (deg[v] && comp[v] == r) { col += vterm[v]; ++vc; }
+                #pragma unroll 1
+        for (uint32_t e = 0; e < pne; ++e)
+            if (!((rmask >> e) & 1ull) && comp[vloc[pevo[e]]] == r) ++ec;
+                #pragma unroll 1
+        for (uint32_t k = 0; k < R.n_rhs; ++k)
+            if (comp[prodv[R.rhs_off[k]]] == r) ++ec;
+        cs += smix(fnv(fnv(kFnvOffset, (ec << 32) | vc), col));
+    }
+    return cs;
+}
+
 template <int VM, int NM>
 HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const uint16_t* vloc,
                              const uint16_t* poff, const uint16_t* pocc, const uint16_t* pdeg,
@@ -212,40 +279,9 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         prev = d;
     }
 
-    // components (partition), then the commutative folds. A connected parent and a rule whose RHS
-    // joins every LHS vertex give a connected child: no partition needed.
-    const bool one = pconn && (R.flags & kRuleRhsJoinsLhs);
-    uint8_t comp[VM];
-        #pragma unroll 1
-    for (uint32_t v = 0; v < V && !one; ++v) comp[v] = static_cast<uint8_t>(v);
-    auto find = [&](uint32_t x) -> uint32_t {
-        while (comp[x] != x) { comp[x] = comp[comp[x]]; x = comp[x]; }
-        return x;
-    };
-        #pragma unroll 1
-    for (uint32_t e = 0; e < pne && !one; ++e) {
-        if ((rmask >> e) & 1ull) continue;
-        const uint32_t a = pear[e], vo = pevo[e];
-        const uint32_t r = find(vloc[vo]);
-                #pragma unroll 1
-        for (uint32_t q = 1; q < a; ++q) {
-            const uint32_t x = find(vloc[vo + q]);
-            if (x != r) comp[x] = static_cast<uint8_t>(r);
-        }
-    }
-        #pragma unroll 1
-    for (uint32_t k = 0; k < R.n_rhs && !one; ++k) {
-        const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
-        const uint32_t r = find(prodv[o]);
-                #pragma unroll 1
-        for (uint32_t q = 1; q < a; ++q) {
-            const uint32_t x = find(prodv[o + q]);
-            if (x != r) comp[x] = static_cast<uint8_t>(r);
-        }
-    }
-        #pragma unroll 1
-    for (uint32_t v = 0; v < V && !one; ++v) comp[v] = static_cast<uint8_t>(find(v));
-    uint64_t vs = 0, es = 0, cs = 0;
+    // the commutative folds, then the component term: a connected parent and a rule whose RHS
+    // joins every LHS vertex give a connected child (one component, no partition needed)
+    uint64_t vs = 0, es = 0;
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         nxt[v] = deg[v] ? smix(cur[v]) : 0;
@@ -268,27 +304,10 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         for (uint32_t q = 0; q < a; ++q) h = fnv(h, cur[prodv[o + q]]);
         es += smix(h);
     }
-    // one component (the usual case): its term folds every vertex and edge, no per-root scans
-    uint32_t roots = one ? 1u : 0u;
-        #pragma unroll 1
-    for (uint32_t v = 0; v < V && !one; ++v) roots += (deg[v] && comp[v] == v) ? 1u : 0u;
-    if (roots == 1)
-        cs = smix(fnv(fnv(kFnvOffset, (static_cast<uint64_t>(ne) << 32) | nv), vs));
-        #pragma unroll 1
-    for (uint32_t r = 0; r < V && roots != 1; ++r) {
-        if (!deg[r] || comp[r] != r) continue;
-        uint64_t col = 0, vc = 0, ec = 0;
-                #pragma unroll 1
-        for (uint32_t v = 0; v < V; ++v)
-            if (deg[v] && comp[v] == r) { col += nxt[v]; ++vc; }
-                #pragma unroll 1
-        for (uint32_t e = 0; e < pne; ++e)
-            if (!((rmask >> e) & 1ull) && comp[vloc[pevo[e]]] == r) ++ec;
-                #pragma unroll 1
-        for (uint32_t k = 0; k < R.n_rhs; ++k)
-            if (comp[prodv[R.rhs_off[k]]] == r) ++ec;
-        cs += smix(fnv(fnv(kFnvOffset, (ec << 32) | vc), col));
-    }
+    const bool one = pconn && (R.flags & kRuleRhsJoinsLhs);
+    const uint64_t cs = one ? lane_one_component(ne, nv, vs)
+                            : lane_component_term<VM>(pear, pevo, vloc, pne, R, prodv, rmask, deg,
+                                                      nxt, V, ne, nv, vs);
     uint64_t h = kFnvOffset;
     h = fnv(h, nv);
     h = fnv(h, ne);
