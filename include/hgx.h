@@ -62,8 +62,10 @@ typedef enum hgx_option {
     /* RecordSet::causal / ::branchial (common/include/hgcommon/core.hpp:128-155). */
     HGX_OPT_RECORD_CAUSAL = 3,
     HGX_OPT_RECORD_BRANCHIAL = 4,
-    /* EvolveInput::edge_identity (gpu/include/hg_gpu/evolve.hpp:36): read back every state's
-       edge record (ids, arities, vertices). */
+    /* Read back every state's edge record (ids, arities, vertices); default 1. The reference
+       returns state edge contents in every mode and adds the edge ids under
+       EvolveInput::edge_identity (gpu/include/hg_gpu/evolve.hpp:36); the hg_gpu shim in
+       hgx/compat.hpp keeps this on and selects the ids by edge_identity. */
     HGX_OPT_KEEP_STATE_EDGES = 5,
     /* 1 = record per-stage device times (CUDA events on the engine stream); 2 = time the expand
        kernel launches only (two events per launch; the other stages read 0). */

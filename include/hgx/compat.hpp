@@ -276,7 +276,11 @@ struct EvolveInput {
     // None / Full (input and output WL hashes); Automatic needs edge ranks and is rejected
     EventCanonicalizationMode event_canonicalization = EventCanonicalizationMode::None;
     bool explore_from_canonical_states_only = true;
-    bool edge_identity = true;                  // keep the state edge records
+    // As the reference (evolve.hpp:36): states always carry their edge contents; true also
+    // carries each state's global edge ids (EvolveResult::state_edge_ids). The reference's
+    // edge id -> vertices table (global_edges) is not provided: edges produced by events whose
+    // child was a duplicate are never materialised on this path.
+    bool edge_identity = false;
     uint64_t max_states = 0;
 };
 
@@ -304,6 +308,7 @@ struct BranchialEdge {
 
 struct EvolveResult {
     std::vector<CanonicalState> states;
+    std::vector<std::vector<EdgeId>> state_edge_ids;   // per state, when edge_identity is set
     std::vector<Event> events;
     std::vector<CausalEdge> causal_edges;       // one per (producer, consumer, edge) triple
     std::vector<BranchialEdge> branchial_edges;
@@ -321,7 +326,7 @@ inline EvolveResult evolve(const EvolveInput& in, int device = 0) {
     }
     detail::check(hgx_engine_set_option(e, HGX_OPT_TRANSITIVE_REDUCTION, in.transitive_reduction));
     detail::check(hgx_engine_set_option(e, HGX_OPT_QUOTIENT, in.explore_from_canonical_states_only));
-    detail::check(hgx_engine_set_option(e, HGX_OPT_KEEP_STATE_EDGES, in.edge_identity));
+    detail::check(hgx_engine_set_option(e, HGX_OPT_KEEP_STATE_EDGES, 1));
     detail::check(hgx_engine_set_option(e, HGX_OPT_MAX_STATES, in.max_states));
     if (in.event_canonicalization == EventCanonicalizationMode::Automatic)
         throw std::invalid_argument("event canonicalization Automatic needs edge ranks (not provided)");
@@ -336,19 +341,24 @@ inline EvolveResult evolve(const EvolveInput& in, int device = 0) {
     EvolveResult out;
     auto hash = detail::copy_array<uint64_t>(rr, HGX_ARR_STATE_HASH);
     auto eoff = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_EDGE_OFF);
+    auto eids = in.edge_identity ? detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_EDGE_IDS)
+                                 : std::vector<uint32_t>{};
     auto ar = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_ARITY);
     auto voff = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_VERT_OFF);
     auto verts = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_VERTS);
     out.states.resize(hash.size());
+    if (in.edge_identity) out.state_edge_ids.resize(hash.size());
     for (size_t s = 0; s < hash.size(); ++s) {
         out.states[s].id = static_cast<StateId>(s);
         out.states[s].canonical_hash = hash[s];
-        if (in.edge_identity && eoff.size() > s + 1) {
+        if (eoff.size() > s + 1) {
             uint32_t v = voff[s];
             for (uint32_t k = eoff[s]; k < eoff[s + 1]; ++k) {
                 out.states[s].edges.emplace_back(verts.begin() + v, verts.begin() + v + ar[k]);
                 v += ar[k];
             }
+            if (in.edge_identity)
+                out.state_edge_ids[s].assign(eids.begin() + eoff[s], eids.begin() + eoff[s + 1]);
         }
     }
     auto ev = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENTS);

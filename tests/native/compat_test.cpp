@@ -37,6 +37,16 @@ int main() {
     std::printf("c2: states %zu events %zu classes %llu\n", r.states.size(), r.events.size(),
                 (unsigned long long)r.num_classes);
     ok = ok && r.states.size() == 1952 && r.events.size() == 5056 && r.num_classes == 1952;
+    // edge contents always; edge ids only under edge_identity (the reference's defaults)
+    ok = ok && r.state_edge_ids.empty() && r.states[1951].edges.size() == 12;
+    in.edge_identity = true;
+    const auto r2 = hgx::compat::gpu::evolve(in);
+    bool ids_ok = r2.state_edge_ids.size() == r2.states.size();
+    for (size_t s = 0; ids_ok && s < r2.states.size(); ++s)
+        ids_ok = r2.state_edge_ids[s].size() == r2.states[s].edges.size() &&
+                 r2.states[s].edges == r.states[s].edges;
+    std::printf("c2 edge identity: %s\n", ids_ok ? "ids match contents" : "MISMATCH");
+    ok = ok && ids_ok;
     bool threw = false;
     try {
         make_rule(0).lhs({0, 40});
