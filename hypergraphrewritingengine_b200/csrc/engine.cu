@@ -143,7 +143,8 @@ enum class LayoutKind { Count, Lane, Warp };
 
 // Shared-memory carve-up per warp. Count: the parent and the join. Lane: plus the parent's
 // per-vertex occurrence lists and a 32-match batch. Warp: plus the warp-per-child WL arrays.
-Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kind, bool fwd = false) {
+Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kind, bool fwd = false,
+                   uint32_t mcap = kLaneJoinCap) {
     const bool wl = kind == LayoutKind::Warp;
     const bool lane = kind == LayoutKind::Lane;
     Layout L;
@@ -223,7 +224,8 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.o_pconn = take(4, 4);
         L.o_pdeg = take(2 * kLaneVMax, 2);
         L.o_batch = take(32 * L.SB, 1);
-        L.o_mlist = take(4 * kLaneJoinCap, 4);
+        L.MCAP = std::max<uint32_t>(1, std::min<uint32_t>(mcap, kLaneJoinCap));
+        L.o_mlist = take(4 * L.MCAP, 4);
     }
     L.bytes = align_up(off, 16);
     return L;
@@ -387,7 +389,7 @@ struct Engine::Impl {
         arena_top.ensure(1, 0, st);
         err.ensure(1, 0, st);
         work.ensure(8, 0, st);
-        level_max.ensure(4, 0, st);
+        level_max.ensure(8, 0, st);
         sync_buf.ensure(16, 0, st);
         stats.ensure(8, 0, st);
         reset();
@@ -1345,7 +1347,7 @@ struct Engine::Impl {
         A.fresh_base = static_cast<uint32_t>(next_vertex);
 
         HGX_CUDA_CHECK(cudaMemsetAsync(work.p, 0, 8 * sizeof(uint32_t), st));
-        HGX_CUDA_CHECK(cudaMemsetAsync(level_max.p, 0, 4 * sizeof(uint32_t), st));
+        HGX_CUDA_CHECK(cudaMemsetAsync(level_max.p, 0, 8 * sizeof(uint32_t), st));
 
         // ---- count
         const bool fwd = opt.forwarding != 0;
@@ -1378,7 +1380,7 @@ struct Engine::Impl {
 
         // ---- sync 1: level totals, per-evolution event ranges, exact frontier maxima
         const size_t nevo = h_evos.size();
-        const size_t w1 = 3 + 4 * nevo;
+        const size_t w1 = 4 + 4 * nevo;
         sync_pack.ensure(w1, 0, st);
         unsigned long long* hs = sync_host(std::max<size_t>(w1, (7 * nevo + 4 + 1) / 2));
         k_sync1_pack<<<grid_for(std::max<size_t>(nevo, 1), 256), 256, 0, st>>>(
@@ -1390,12 +1392,13 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         const uint32_t tot[6] = {uint32_t(hs[0]), uint32_t(hs[0] >> 32), uint32_t(hs[1]),
                                  uint32_t(hs[1] >> 32), uint32_t(hs[2]), uint32_t(hs[2] >> 32)};
+        const uint32_t fmax_cnt = uint32_t(hs[3]);
         std::vector<uint32_t> h_first(nevo), h_last(nevo);
-        std::vector<unsigned long long> h_classes(hs + 3, hs + 3 + nevo),
-            h_states_ev(hs + 3 + nevo, hs + 3 + 2 * nevo), h_sigs(hs + 3 + 2 * nevo, hs + 3 + 3 * nevo);
+        std::vector<unsigned long long> h_classes(hs + 4, hs + 4 + nevo),
+            h_states_ev(hs + 4 + nevo, hs + 4 + 2 * nevo), h_sigs(hs + 4 + 2 * nevo, hs + 4 + 3 * nevo);
         for (size_t e = 0; e < nevo; ++e) {
-            h_first[e] = uint32_t(hs[3 + 3 * nevo + e]);
-            h_last[e] = uint32_t(hs[3 + 3 * nevo + e] >> 32);
+            h_first[e] = uint32_t(hs[4 + 3 * nevo + e]);
+            h_last[e] = uint32_t(hs[4 + 3 * nevo + e] >> 32);
         }
         auto h_states_now = [&](uint32_t e) { return static_cast<uint64_t>(h_states_ev[e]); };
         const uint32_t n_ev = tot[0], n_cons_lv = tot[1], n_prod = tot[2], n_fresh = tot[3];
@@ -1460,7 +1463,8 @@ struct Engine::Impl {
         uint32_t bucket = 0;
         if (n_ev) {
             const uint32_t mne = std::max<uint32_t>(fmax_ne, 1), mno = std::max<uint32_t>(fmax_nocc, 1);
-            const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane, fwd);
+            const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane, fwd,
+                                          fmax_cnt);
             const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp, fwd);
             // lane kernel join: autotuned per bucket of children per frontier state (the walk
             // amortises its count-and-emit passes over many children per state)

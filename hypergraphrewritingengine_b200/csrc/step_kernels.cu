@@ -1081,6 +1081,7 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
     char* sm = smem + (threadIdx.x >> 5) * L.bytes;
     const uint32_t lane = lane_id();
     const DevRule& R = *smp<DevRule>(sm, L.o_rule);
+    uint32_t max_cnt = 0;   // largest match count of a (state, rule) this warp counted
     WarpWork q;
     while (true) {
         const uint32_t f = q.next(&A.work[0]);
@@ -1117,10 +1118,12 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
                 else warp_join(L, sm, R, pa, R.sched, -1, [&](uint32_t) { ++cnt; });
             }
             if (lane == 0) A.counts[f * A.rules_stride + r] = cnt;
+            max_cnt = max(max_cnt, cnt);
             __syncwarp();
         }
         if (lane == 0) A.fmode[f] = (lane_ok ? 1 : 0) | (fwd_on ? 2 : 0);
     }
+    if (lane == 0 && max_cnt) atomicMax(&A.level_max[4], max_cnt);   // sizes the staged match list
 }
 
 // Per-item counts scaled by the rule's consumed / produced / fresh sizes, for the scans.
@@ -1277,7 +1280,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                 n_rounds += info.rounds;
             };
             if constexpr (kLane) {
-              if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= kLaneJoinCap) {
+              if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= L.MCAP) {
                 // stage the rule's matches in canonical order (lane walks: count, scan, emit),
                 // then hash them 32 at a time, one child per lane
                 uint32_t* mlist = smp<uint32_t>(sm, L.o_mlist);
@@ -1290,7 +1293,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                     const uint32_t inc = warp_incl_scan(c);
                     uint32_t w = total + inc - c;
                     if (c) lane_walk(L, sm, R, pa, e0, [&](uint32_t pk) {
-                        if (w < kLaneJoinCap) mlist[w] = pk;
+                        if (w < L.MCAP) mlist[w] = pk;
                         ++w;
                     });
                     total += __shfl_sync(0xFFFFFFFFu, inc, 31);
@@ -1490,7 +1493,8 @@ __global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t
 // frontier order). out[evo * 7 + {0..6}] = event first/end, state first/end, pair first/end, and
 // the evolution's states in the next frontier.
 // A level's first read-back in one copy: out[0..2] = event / consumed, produced / fresh totals and
-// the frontier's largest edge / occurrence counts (low | high << 32), then per evolution its
+// the frontier's largest edge / occurrence counts (low | high << 32), out[3] the largest match
+// count of a (state, rule), then per evolution its
 // classes, states, event signatures (sigs may be null) and first | last event << 32.
 __global__ void k_sync1_pack(const uint32_t* item_ev, const uint32_t* item_cons,
                              const uint32_t* item_prod, const uint32_t* item_fresh, uint32_t ni,
@@ -1504,12 +1508,13 @@ __global__ void k_sync1_pack(const uint32_t* item_ev, const uint32_t* item_cons,
         out[0] = item_ev[ni] | (u64(item_cons[ni]) << 32);
         out[1] = item_prod[ni] | (u64(item_fresh[ni]) << 32);
         out[2] = level_max[2] | (u64(level_max[3]) << 32);
+        out[3] = level_max[4];
     }
     for (uint32_t e = t; e < nevo; e += gridDim.x * blockDim.x) {
-        out[3 + e] = classes[e];
-        out[3 + nevo + e] = states[e];
-        out[3 + 2ull * nevo + e] = sigs ? sigs[e] : 0ull;
-        out[3 + 3ull * nevo + e] = first[e] | (u64(last[e]) << 32);
+        out[4 + e] = classes[e];
+        out[4 + nevo + e] = states[e];
+        out[4 + 2ull * nevo + e] = sigs ? sigs[e] : 0ull;
+        out[4 + 3ull * nevo + e] = first[e] | (u64(last[e]) << 32);
     }
 }
 
@@ -1659,7 +1664,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
         Fwd fwd;
         fwd.on = false;
         if constexpr (kFwd) fwd = fwd_prepare(P, A, L, sm, R, ev, pa, sid, (fm & 2u) != 0);
-        if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= kLaneJoinCap) {
+        if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= L.MCAP) {
             uint32_t* mlist = smp<uint32_t>(sm, L.o_mlist);
             const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
             const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
@@ -1670,7 +1675,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
                 const uint32_t inc = warp_incl_scan(c);
                 uint32_t wpos = total + inc - c;
                 if (c) lane_walk(L, sm, R, pa, e0, [&](uint32_t pk) {
-                    if (wpos < kLaneJoinCap) mlist[wpos] = pk;
+                    if (wpos < L.MCAP) mlist[wpos] = pk;
                     ++wpos;
                 });
                 total += __shfl_sync(0xFFFFFFFFu, inc, 31);

@@ -110,7 +110,8 @@ struct LevelArgs {
     uint32_t state_base;
     uint32_t* new_state_event;  // [n_new] event of each new state
     uint32_t* next_frontier;
-    uint32_t* level_max;        // [2] max ne, max nocc over new states
+    uint32_t* level_max;        // [0..1] max ne, nocc of new states; [2..3] of the frontier;
+                                // [4] largest match count of a (state, rule)
     // branchial
     uint32_t* bcount;           // [n_events] pairs (a, later b) per event a
     uint32_t* boff;             // [n_events+1] exclusive scan of bcount
@@ -131,6 +132,7 @@ struct Layout {
     // neighbour counts, and a batch of up to 32 matches (removed positions + produced local
     // vertices)
     uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_pnoff, o_pnbr, o_batch, o_mlist;
+    uint32_t MCAP;      // matches the lane walk stages per (state, rule) (<= kLaneJoinCap)
     uint32_t o_pconn;   // u32: 1 when the parent is connected
     // match forwarding: seeded schedule, creating event's consumed edges, delta matches (and a
     // sorted copy), a 32-match chunk of forwarded matches
