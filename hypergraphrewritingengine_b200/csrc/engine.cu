@@ -223,8 +223,9 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.o_pnn = take(2 * kLaneVMax, 2);
         L.o_pconn = take(4, 4);
         L.o_pdeg = take(2 * kLaneVMax, 2);
-        L.o_batch = take(32 * L.SB, 1);
         L.MCAP = std::max<uint32_t>(1, std::min<uint32_t>(mcap, kLaneJoinCap));
+        L.region_bytes = align_up(off, 16);   // batch and match list last: regions >= 1 stop here
+        L.o_batch = take(32 * L.SB, 1);
         L.o_mlist = take(4 * L.MCAP, 4);
     }
     L.bytes = align_up(off, 16);
@@ -1481,7 +1482,7 @@ struct Engine::Impl {
             }
             // single-rule evolutions: batches of children cross parents (two parent regions per warp)
             Layout Ll2 = Ll;
-            Ll2.bytes = kLaneRegions * Ll.bytes;
+            Ll2.bytes = Ll.bytes + (kLaneRegions - 1) * Ll.region_bytes;   // one batch per warp
             const bool cross = rm.stride == 1 && Ll2.bytes <= (kMaxDynSmem - 8192) / 2;
             LaunchShape sl = cross ? (walk ? (fwd ? warp_shape(k_expand_lanes2<true, kLaneRegions>, Ll2, F)
                                                   : warp_shape(k_expand_lanes2<true, kLaneRegions, false>, Ll2, F))

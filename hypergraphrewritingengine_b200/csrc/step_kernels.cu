@@ -1571,8 +1571,9 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
     __shared__ uint32_t meta_sm[8][32];
     const uint32_t w = threadIdx.x >> 5;
     const uint32_t lane = lane_id();
-    char* const wbase = smem + w * kReg * L.bytes;
-    auto rg = [&](uint32_t r) { return wbase + r * L.bytes; };
+    // region 0 carries the warp's batch and match list at its end; regions >= 1 stop before them
+    char* const wbase = smem + w * (L.bytes + (kReg - 1) * L.region_bytes);
+    auto rg = [&](uint32_t r) { return r == 0 ? wbase : wbase + L.bytes + (r - 1) * L.region_bytes; };
     LaneRegion* rinfo = rinfo_sm[w];
     uint32_t* meta = meta_sm[w];            // slot -> (region << 29) | child index in its parent
     uint8_t* batch = smp<uint8_t>(rg(0), L.o_batch);
@@ -1665,7 +1666,7 @@ __global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A
         fwd.on = false;
         if constexpr (kFwd) fwd = fwd_prepare(P, A, L, sm, R, ev, pa, sid, (fm & 2u) != 0);
         if (kWalk && !fwd.on && pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs && rn <= L.MCAP) {
-            uint32_t* mlist = smp<uint32_t>(sm, L.o_mlist);
+            uint32_t* mlist = smp<uint32_t>(rg(0), L.o_mlist);   // the warp's one match list
             const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
             const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
             uint32_t total = 0;

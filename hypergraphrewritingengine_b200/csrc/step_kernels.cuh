@@ -133,6 +133,8 @@ struct Layout {
     // vertices)
     uint32_t o_poff, o_pocc, o_pdeg, o_pnn, o_pnoff, o_pnbr, o_batch, o_mlist;
     uint32_t MCAP;      // matches the lane walk stages per (state, rule) (<= kLaneJoinCap)
+    uint32_t region_bytes;   // lane layout without the trailing batch and match list (a warp's
+                             // further parent regions need no batch or match list of their own)
     uint32_t o_pconn;   // u32: 1 when the parent is connected
     // match forwarding: seeded schedule, creating event's consumed edges, delta matches (and a
     // sorted copy), a 32-match chunk of forwarded matches
