@@ -68,15 +68,15 @@ HGX_HD void lane_isort64(uint64_t* a, uint32_t n) {
 }
 
 template <int VM>
-HGX_HD uint32_t lane_distinct(const uint64_t* cur, const uint16_t* deg, uint32_t V) {
+HGX_HD uint32_t lane_distinct(const uint64_t* cur, uint32_t alive, uint32_t V) {
     uint32_t d = 0;
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
-        if (!deg[v]) continue;
+        if (!((alive >> v) & 1u)) continue;
         bool first = true;
                 #pragma unroll 1
         for (uint32_t u = 0; u < v && first; ++u)
-            if (deg[u] && cur[u] == cur[v]) first = false;
+            if (((alive >> u) & 1u) && cur[u] == cur[v]) first = false;
         d += first ? 1u : 0u;
     }
     return d;
@@ -94,7 +94,7 @@ template <int VM>
 HGX_NOINLINE uint64_t lane_component_term(const uint8_t* pear, const uint16_t* pevo,
                                           const uint16_t* vloc, uint32_t pne, const DevRule& R,
                                           const uint8_t* prodv, uint64_t rmask,
-                                          const uint16_t* deg, const uint64_t* vterm, uint32_t V,
+                                          uint32_t alive, const uint64_t* vterm, uint32_t V,
                                           uint32_t ne, uint32_t nv, uint64_t vs) {
     uint8_t comp[VM];
         #pragma unroll 1
@@ -128,16 +128,16 @@ HGX_NOINLINE uint64_t lane_component_term(const uint8_t* pear, const uint16_t* p
     for (uint32_t v = 0; v < V; ++v) comp[v] = static_cast<uint8_t>(find(v));
     uint32_t roots = 0;
         #pragma unroll 1
-    for (uint32_t v = 0; v < V; ++v) roots += (deg[v] && comp[v] == v) ? 1u : 0u;
+    for (uint32_t v = 0; v < V; ++v) roots += (((alive >> v) & 1u) && comp[v] == v) ? 1u : 0u;
     if (roots == 1) return lane_one_component(ne, nv, vs);
     uint64_t cs = 0;
         #pragma unroll 1
     for (uint32_t r = 0; r < V; ++r) {
-        if (!deg[r] || comp[r] != r) continue;
+        if (!((alive >> r) & 1u) || comp[r] != r) continue;
         uint64_t col = 0, vc = 0, ec = 0;
                 #pragma unroll 1
         for (uint32_t v = 0; v < V; ++v)
-            if (deg[v] && comp[v] == r) { col += vterm[v]; ++vc; }
+            if (((alive >> v) & 1u) && comp[v] == r) { col += vterm[v]; ++vc; }
                 #pragma unroll 1
         for (uint32_t e = 0; e < pne; ++e)
             if (!((rmask >> e) & 1ull) && comp[vloc[pevo[e]]] == r) ++ec;
@@ -191,10 +191,11 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
             nn[v] += static_cast<uint16_t>(a - 1);
         }
     }
-    uint32_t nv = 0, cap = 1, nocc = 0, nbr = 0;
+    uint32_t nv = 0, cap = 1, nocc = 0, nbr = 0, alive = 0;   // alive: vertices of degree > 0
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         nv += deg[v] ? 1u : 0u;
+        alive |= (deg[v] ? 1u : 0u) << v;
         cap = nn[v] > cap ? nn[v] : cap;
         nocc += deg[v];
         nbr += nn[v];
@@ -241,12 +242,12 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         }
         cur[v] = h;
     }
-    uint32_t prev = lane_distinct<VM>(cur, deg, V);
+    uint32_t prev = lane_distinct<VM>(cur, alive, V);
         #pragma unroll 1
     for (uint32_t it = 0; it < kWlMaxRounds; ++it) {
                 #pragma unroll 1
         for (uint32_t v = 0; v < V; ++v) {
-            if (!deg[v]) { nxt[v] = 0; continue; }
+            if (!((alive >> v) & 1u)) { nxt[v] = 0; continue; }
             // the neighbour multiset; nn[v] <= cap entries, so the reference's cap never cuts here
             uint32_t n = 0;
             const uint32_t j0 = v < nvp ? pnoff[v] : 0u, j1 = v < nvp ? pnoff[v + 1] : 0u;
@@ -273,7 +274,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         uint64_t* t = cur;
         cur = nxt;
         nxt = t;
-        const uint32_t d = lane_distinct<VM>(cur, deg, V);
+        const uint32_t d = lane_distinct<VM>(cur, alive, V);
         ++info.rounds;
         if (d == prev) break;
         prev = d;
@@ -284,7 +285,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
     uint64_t vs = 0, es = 0;
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
-        nxt[v] = deg[v] ? smix(cur[v]) : 0;
+        nxt[v] = ((alive >> v) & 1u) ? smix(cur[v]) : 0;
         vs += nxt[v];
     }
         #pragma unroll 1
@@ -306,7 +307,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
     }
     const bool one = pconn && (R.flags & kRuleRhsJoinsLhs);
     const uint64_t cs = one ? lane_one_component(ne, nv, vs)
-                            : lane_component_term<VM>(pear, pevo, vloc, pne, R, prodv, rmask, deg,
+                            : lane_component_term<VM>(pear, pevo, vloc, pne, R, prodv, rmask, alive,
                                                       nxt, V, ne, nv, vs);
     uint64_t h = kFnvOffset;
     h = fnv(h, nv);
