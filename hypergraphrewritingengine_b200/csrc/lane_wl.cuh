@@ -165,20 +165,16 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
     uint64_t rmask = 0;
         #pragma unroll 1
     for (uint32_t k = 0; k < R.n_lhs; ++k) rmask |= 1ull << rpos[k];
-    uint16_t deg[VM], nn[VM];
+    uint32_t dn[VM];   // degree | neighbour count << 16
         #pragma unroll 1
-    for (uint32_t v = 0; v < V; ++v) {
-        deg[v] = v < nvp ? pdeg[v] : 0;
-        nn[v] = v < nvp ? pnn[v] : 0;
-    }
+    for (uint32_t v = 0; v < V; ++v) dn[v] = v < nvp ? (pdeg[v] | (uint32_t(pnn[v]) << 16)) : 0u;
         #pragma unroll 1
     for (uint32_t k = 0; k < R.n_lhs; ++k) {
         const uint32_t e = rpos[k], a = pear[e], vo = pevo[e];
                 #pragma unroll 1
         for (uint32_t q = 0; q < a; ++q) {
             const uint32_t v = vloc[vo + q];
-            deg[v] -= 1;
-            nn[v] -= static_cast<uint16_t>(a - 1);
+            dn[v] -= 1u + ((a - 1u) << 16);
         }
     }
         #pragma unroll 1
@@ -187,18 +183,18 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
                 #pragma unroll 1
         for (uint32_t q = 0; q < a; ++q) {
             const uint32_t v = prodv[o + q];
-            deg[v] += 1;
-            nn[v] += static_cast<uint16_t>(a - 1);
+            dn[v] += 1u + ((a - 1u) << 16);
         }
     }
     uint32_t nv = 0, cap = 1, nocc = 0, nbr = 0, alive = 0;   // alive: vertices of degree > 0
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
-        nv += deg[v] ? 1u : 0u;
-        alive |= (deg[v] ? 1u : 0u) << v;
-        cap = nn[v] > cap ? nn[v] : cap;
-        nocc += deg[v];
-        nbr += nn[v];
+        const uint32_t d = dn[v] & 0xFFFFu, m = dn[v] >> 16;
+        nv += d ? 1u : 0u;
+        alive |= (d ? 1u : 0u) << v;
+        cap = m > cap ? m : cap;
+        nocc += d;
+        nbr += m;
     }
     info.nv = nv;
     info.nocc = nocc;
@@ -219,7 +215,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
         cur[v] = 0;
-        if (!deg[v]) continue;
+        if (!((alive >> v) & 1u)) continue;
         uint32_t n = 0;
         const uint32_t j0 = v < nvp ? poff[v] : 0u, j1 = v < nvp ? poff[v + 1] : 0u;
                 #pragma unroll 1
@@ -234,7 +230,7 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
             buf[n++] = (static_cast<uint64_t>(R.rhs_ar[k]) << 8) | (p - R.rhs_off[k]);
         }
         lane_isort64(buf, n);
-        uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(deg[v]));
+        uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(dn[v] & 0xFFFFu));
                 #pragma unroll 1
         for (uint32_t j = 0; j < n; ++j) {
             h = fnv(h, buf[j] >> 8);
