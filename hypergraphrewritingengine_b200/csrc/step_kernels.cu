@@ -1564,8 +1564,10 @@ struct LaneRegion {
 };
 
 // kFwd = false: a level without match forwarding, compiled without its paths (a smaller kernel).
+// The walk instantiation is held to 4 blocks per SM (64 registers; measured faster on small-state
+// levels), the warp-join one to 3.
 template <bool kWalk, int kReg = 2, bool kFwd = true>
-__global__ void __launch_bounds__(256, 3) k_expand_lanes2(DevPtrs P, LevelArgs A, Layout L) {
+__global__ void __launch_bounds__(256, kWalk ? 4 : 3) k_expand_lanes2(DevPtrs P, LevelArgs A, Layout L) {
     extern __shared__ __align__(16) char smem[];
     __shared__ LaneRegion rinfo_sm[8][kReg];
     __shared__ uint32_t meta_sm[8][32];
