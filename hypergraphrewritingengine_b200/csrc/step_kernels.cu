@@ -1579,9 +1579,15 @@ __global__ void __launch_bounds__(256, kWalk ? 4 : 3) k_expand_lanes2(DevPtrs P,
     LaneRegion* rinfo = rinfo_sm[w];
     uint32_t* meta = meta_sm[w];            // slot -> (region << 29) | child index in its parent
     uint8_t* batch = smp<uint8_t>(rg(0), L.o_batch);
-    uint64_t b_stage = 0, b_hbm = 0, n_child = 0, n_rounds = 0;   // per-lane accumulators
+    // byte / child / round counters: per warp in shared memory (kept out of the registers the
+    // parent loop holds); each flush adds its batch's warp sums
+    __shared__ unsigned long long stats_sm[8][4];
+    unsigned long long* wstats = stats_sm[w];
+    if (lane < 4) wstats[lane] = 0;
+    __syncwarp();
     uint32_t nb = 0, held = 0, cur = 0;     // children in the batch, regions they come from
     auto flush = [&]() {
+        uint64_t b_stage = 0, b_hbm = 0, n_rounds = 0;
         if (lane < nb) {
             const uint32_t m = meta[lane], r = m >> 29, idx = m & 0x1FFFFFFFu;
             const LaneRegion ri = rinfo[r];
@@ -1614,8 +1620,16 @@ __global__ void __launch_bounds__(256, kWalk ? 4 : 3) k_expand_lanes2(DevPtrs P,
                        8ull * info.nv + 8ull * info.nocc;
             b_stage += 16;
             b_hbm += 20 + 8 + 8 * k + 4 * rr + 16;
-            n_child += 1;
             n_rounds += info.rounds;
+        }
+        b_stage = warp_sum64(b_stage);
+        b_hbm = warp_sum64(b_hbm);
+        n_rounds = warp_sum64(n_rounds);
+        if (lane == 0) {
+            wstats[0] += b_stage;
+            wstats[1] += b_hbm;
+            wstats[2] += nb;
+            wstats[3] += n_rounds;
         }
         __syncwarp();
         nb = 0;
@@ -1635,8 +1649,8 @@ __global__ void __launch_bounds__(256, kWalk ? 4 : 3) k_expand_lanes2(DevPtrs P,
         if (rn == 0 || ev.rule_count == 0) {   // nothing to build: count what the join reads
             if (lane == 0) {
                 const uint64_t ne = P.st_ne[sid], nocc = P.st_nocc[sid];
-                b_hbm += 4 * (ne + (ne + 3) / 4 + nocc) + 20;
-                b_stage += 4 * ne + 4 * nocc;
+                wstats[1] += 4 * (ne + (ne + 3) / 4 + nocc) + 20;
+                wstats[0] += 4 * ne + 4 * nocc;
             }
             continue;
         }
@@ -1647,8 +1661,8 @@ __global__ void __launch_bounds__(256, kWalk ? 4 : 3) k_expand_lanes2(DevPtrs P,
         load_rule(sm, L, &P.rules[ev.rule_begin]);
         const DevRule& R = *smp<DevRule>(sm, L.o_rule);
         if (lane == 0) {
-            b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
-            b_stage += 4ull * pa.ne + 4ull * pa.nocc;
+            wstats[1] += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
+            wstats[0] += 4ull * pa.ne + 4ull * pa.nocc;
             LaneRegion ri;
             ri.sid = sid;
             ri.ev0 = A.ev_base + A.item_ev[f];
@@ -1741,15 +1755,12 @@ __global__ void __launch_bounds__(256, kWalk ? 4 : 3) k_expand_lanes2(DevPtrs P,
         cur = cur + 1 == kReg ? 0u : cur + 1;
     }
     if (nb) flush();
-    b_stage = warp_sum64(b_stage);
-    b_hbm = warp_sum64(b_hbm);
-    n_child = warp_sum64(n_child);
-    n_rounds = warp_sum64(n_rounds);
-    if (lane == 0 && b_hbm) {
-        atomicAdd(&P.stats[0], static_cast<unsigned long long>(b_stage));
-        atomicAdd(&P.stats[1], static_cast<unsigned long long>(b_hbm));
-        atomicAdd(&P.stats[2], static_cast<unsigned long long>(n_child));
-        atomicAdd(&P.stats[3], static_cast<unsigned long long>(n_rounds));
+    __syncwarp();
+    if (lane == 0 && wstats[1]) {
+        atomicAdd(&P.stats[0], wstats[0]);
+        atomicAdd(&P.stats[1], wstats[1]);
+        atomicAdd(&P.stats[2], wstats[2]);
+        atomicAdd(&P.stats[3], wstats[3]);
     }
 }
 
