@@ -1150,9 +1150,12 @@ __global__ void k_item_sizes(DevPtrs P, LevelArgs A) {
 
 // An event's consumed parent positions as a bit mask for the branchial test (events of one input
 // state share the parent's positions, so equal positions are equal edges), or 0 when the parent
-// has more than 64 edges (the test then compares edge ids).
+// has more than 63 edges (the test then compares edge ids). Bit 63 is never a position: an event
+// that is not kept carries kMaskDropped, which shares no position with any other mask.
+constexpr unsigned long long kMaskDropped = 1ull << 63;
+
 __device__ __forceinline__ unsigned long long branch_mask(uint32_t n, uint32_t pne, const uint8_t* pos) {
-    if (pne > 64) return 0ull;
+    if (pne > 63) return 0ull;
     unsigned long long m = 0;
     for (uint32_t k = 0; k < n; ++k) m |= 1ull << pos[k];
     return m;
@@ -2069,7 +2072,7 @@ __global__ void k_void(DevPtrs P, LevelArgs A, uint32_t n) {
                 P.ev_hash[e] = 0;
                 P.ev_out[e] = kNone;
                 for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = 0;   // edge 0 exists
-                P.ev_bmask[e] = 0ull;
+                P.ev_bmask[e] = kMaskDropped;   // never kept
                 for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
                 A.flag_new[lo + idx] = 0;
             }
@@ -2117,6 +2120,7 @@ __global__ void k_rep(DevPtrs P, LevelArgs A) {
             rep = kept && (ev.quotient ? fresh : true);
             const bool front = rep && (P.st_depth[sid] + 1 < ev.steps) && cut == kNone;
             P.ev_kept[e] = kept ? 1 : 0;
+            if (!kept && P.ev_bmask[e]) P.ev_bmask[e] = kMaskDropped;
             A.flag_rep[t] = rep ? 1u : 0u;
             A.flag_front[t] = front ? 1u : 0u;
             if (e == cut) P.evo_stopped[evo] = 1;
@@ -2335,16 +2339,20 @@ __global__ void k_bpairs(DevPtrs P, LevelArgs A) {
             const uint32_t in = P.ev_in[a];
             const uint32_t na = P.rules[P.ev_rule[a]].n_lhs, ca0 = P.ev_coff[a];
             const unsigned long long ma = P.ev_bmask[a];
-            uint32_t ca[kMaxPatternEdges];
-            for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[ca0 + k];
+            uint32_t ca[kMaxPatternEdges];   // edge ids, for parents past the mask's 63 positions
+            bool have_ca = false;
             uint32_t out = kEmit ? A.boff[t] : 0u;
             for (uint32_t c = a + 1; c < end && P.ev_in[c] == in; ++c) {
-                if (!P.ev_kept[c]) continue;
                 const unsigned long long mc = P.ev_bmask[c];
                 bool share = false;
                 if (ma && mc) {
-                    share = (ma & mc) != 0ull;   // a consumed parent position in common
-                } else {
+                    // a consumed parent position in common (never with a dropped event's mask)
+                    share = (ma & mc) != 0ull;
+                } else if (P.ev_kept[c]) {
+                    if (!have_ca) {
+                        for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[ca0 + k];
+                        have_ca = true;
+                    }
                     const uint32_t nc = P.rules[P.ev_rule[c]].n_lhs, cc0 = P.ev_coff[c];
                     for (uint32_t k = 0; k < nc && !share; ++k) {
                         const uint32_t x = P.ev_cons[cc0 + k];
