@@ -64,7 +64,7 @@ struct DevPtrs {
     // ancestor (levels < 64; an event's ancestors lie on its input state's history chain)
     unsigned long long* ev_anc;
     // per event: the parent positions it consumed as a bit mask for the branchial test, or 0 when
-    // the parent has more than 64 edges (compare edge ids)
+    // the parent has more than 63 edges (compare edge ids); bit 63 alone: the event is not kept
     unsigned long long* ev_bmask;
     // event canonicalisation: per event its signature; per evolution the distinct signatures
     unsigned long long* ev_sig;
