@@ -1361,8 +1361,6 @@ struct Engine::Impl {
         tic();
         k_count<<<sc.grid, sc.block, sc.smem, st>>>(ptrs(), A, Lc);
         check_launch();
-        k_frontier_max<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A);
-        check_launch();
         toc(times.count);
 
         // ---- scans of the per-item sizes
@@ -1371,11 +1369,9 @@ struct Engine::Impl {
         check_launch();
         scan_multi({{item_ev.p, item_ev.p}, {item_cons.p, item_cons.p}, {item_prod.p, item_prod.p},
                     {item_fresh.p, item_fresh.p}}, NI);
-        k_fwd_record<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A);
-        check_launch();
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_first_ev.p, 0xFF, h_evos.size() * 4, st));
         evo_frange.ensure(2 * h_evos.size(), 0, st);
-        k_evo_first<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, evo_frange.p);
+        k_frontier_events<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, evo_frange.p);
         check_launch();
         toc(times.scan);
 
@@ -1394,6 +1390,7 @@ struct Engine::Impl {
         const uint32_t tot[6] = {uint32_t(hs[0]), uint32_t(hs[0] >> 32), uint32_t(hs[1]),
                                  uint32_t(hs[1] >> 32), uint32_t(hs[2]), uint32_t(hs[2] >> 32)};
         const uint32_t fmax_cnt = uint32_t(hs[3]);
+        const uint32_t n_warp_states = uint32_t(hs[3] >> 32);   // 0: no warp-path launches
         std::vector<uint32_t> h_first(nevo), h_last(nevo);
         std::vector<unsigned long long> h_classes(hs + 4, hs + 4 + nevo),
             h_states_ev(hs + 4 + nevo, hs + 4 + 2 * nevo), h_sigs(hs + 4 + 2 * nevo, hs + 4 + 3 * nevo);
@@ -1509,6 +1506,7 @@ struct Engine::Impl {
                 toc(times.expand, true);
                 ++times.expand_launches;
                 if (walk) ++times.walk_launches;
+                if (!n_warp_states) return;   // every state of the level is on the lane path
                 tic();
                 slice_off.ensure(uint64_t(n_work) + 1, 0, st);
                 k_slice_counts<<<grid_for(n_work, 256), 256, 0, st>>>(A, n_work, slice_off.p);

@@ -1473,12 +1473,25 @@ __global__ void k_evo_causal(DevPtrs P, uint32_t n_events, unsigned long long* o
 
 
 
-// First / one-past-last event of every evolution in this level (the frontier is grouped by
-// evolution, so each evolution's items are contiguous); resets the evolution's cap cut.
-__global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t* evo_frange) {
+// Per frontier state: its first event and first-rule event count (the record match forwarding
+// reads at the next level). Per evolution: first / one-past-last event of this level (the
+// frontier is grouped by evolution, so each evolution's items are contiguous), and its cap cut
+// reset. For the level: the frontier's largest edge and occurrence counts (level_max[2..3], they
+// size the expand layouts) and how many states with children are off the lane path
+// (level_max[5]; none: the warp-path launches are skipped).
+__global__ void k_frontier_events(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t* evo_frange) {
+    uint32_t mne = 0, mno = 0, n_warp = 0;
     for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
          f += gridDim.x * blockDim.x) {
-        const uint32_t evo = P.st_evo[A.frontier[f]];
+        const uint32_t sid = A.frontier[f];
+        const uint32_t t = f * A.rules_stride;
+        P.st_ev0[sid] = A.ev_base + A.item_ev[t];
+        P.st_evn[sid] = A.item_ev[t + 1] - A.item_ev[t];
+        mne = max(mne, P.st_ne[sid]);
+        mno = max(mno, P.st_nocc[sid]);
+        const bool children = A.item_ev[t + A.rules_stride] != A.item_ev[t];
+        n_warp += (!(A.fmode[f] & 1u) && children) ? 1u : 0u;
+        const uint32_t evo = P.st_evo[sid];
         if (f == 0 || P.st_evo[A.frontier[f - 1]] != evo) {
             P.evo_first_ev[evo] = A.ev_base + A.item_ev[f * A.rules_stride];
             P.evo_cut[evo] = kNone;
@@ -1489,6 +1502,14 @@ __global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t
             evo_frange[2 * evo + 1] = f + 1;
         }
     }
+    mne = warp_max32(mne);
+    mno = warp_max32(mno);
+    n_warp = warp_sum32(n_warp);
+    if (lane_id() == 0) {
+        atomicMax(&A.level_max[2], mne);
+        atomicMax(&A.level_max[3], mno);
+        if (n_warp) atomicAdd(&A.level_max[5], n_warp);
+    }
 }
 
 // Per evolution of the level: its kept events, its new states and its branchial pairs are each
@@ -1497,7 +1518,7 @@ __global__ void k_evo_first(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t
 // the evolution's states in the next frontier.
 // A level's first read-back in one copy: out[0..2] = event / consumed, produced / fresh totals and
 // the frontier's largest edge / occurrence counts (low | high << 32), out[3] the largest match
-// count of a (state, rule), then per evolution its
+// count of a (state, rule) | frontier states for the warp path << 32, then per evolution its
 // classes, states, event signatures (sigs may be null) and first | last event << 32.
 __global__ void k_sync1_pack(const uint32_t* item_ev, const uint32_t* item_cons,
                              const uint32_t* item_prod, const uint32_t* item_fresh, uint32_t ni,
@@ -1511,7 +1532,7 @@ __global__ void k_sync1_pack(const uint32_t* item_ev, const uint32_t* item_cons,
         out[0] = item_ev[ni] | (u64(item_cons[ni]) << 32);
         out[1] = item_prod[ni] | (u64(item_fresh[ni]) << 32);
         out[2] = level_max[2] | (u64(level_max[3]) << 32);
-        out[3] = level_max[4];
+        out[3] = level_max[4] | (u64(level_max[5]) << 32);
     }
     for (uint32_t e = t; e < nevo; e += gridDim.x * blockDim.x) {
         out[4 + e] = classes[e];
@@ -1943,32 +1964,6 @@ __global__ void k_fin_bounds(const uint32_t* scan, const uint32_t* bases, uint32
 
 // Each frontier state's event range (its matches, in canonical order), for its children's
 // match forwarding. Single-rule evolutions only (item f * R of the state).
-__global__ void k_fwd_record(DevPtrs P, LevelArgs A) {
-    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
-         f += gridDim.x * blockDim.x) {
-        const uint32_t sid = A.frontier[f];
-        const uint32_t t = f * A.rules_stride;
-        P.st_ev0[sid] = A.ev_base + A.item_ev[t];
-        P.st_evn[sid] = A.item_ev[t + 1] - A.item_ev[t];
-    }
-}
-
-// Largest edge count / occurrence count in the frontier (sizes the expand kernel's layout).
-__global__ void k_frontier_max(DevPtrs P, LevelArgs A) {
-    uint32_t mne = 0, mno = 0;
-    for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
-         f += gridDim.x * blockDim.x) {
-        const uint32_t sid = A.frontier[f];
-        mne = max(mne, P.st_ne[sid]);
-        mno = max(mno, P.st_nocc[sid]);
-    }
-    mne = warp_max32(mne);
-    mno = warp_max32(mno);
-    if (lane_id() == 0) {
-        atomicMax(&A.level_max[2], mne);
-        atomicMax(&A.level_max[3], mno);
-    }
-}
 
 // Roots: count WL classes (first arrival of each hash) and states per evolution.
 __global__ void k_root_counts(DevPtrs P, const uint32_t* sids, uint32_t n) {

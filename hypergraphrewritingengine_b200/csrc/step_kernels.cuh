@@ -111,7 +111,8 @@ struct LevelArgs {
     uint32_t* new_state_event;  // [n_new] event of each new state
     uint32_t* next_frontier;
     uint32_t* level_max;        // [0..1] max ne, nocc of new states; [2..3] of the frontier;
-                                // [4] largest match count of a (state, rule)
+                                // [4] largest match count of a (state, rule); [5] frontier
+                                // states for the warp path
     // branchial
     uint32_t* bcount;           // [n_events] pairs (a, later b) per event a
     uint32_t* boff;             // [n_events+1] exclusive scan of bcount
