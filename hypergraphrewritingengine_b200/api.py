@@ -44,6 +44,9 @@ HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_
 EVENT_KEY_INPUT, EVENT_KEY_OUTPUT, EVENT_KEY_STEP, EVENT_KEY_RULE = 1, 2, 4, 8
 EVENT_SIG_NONE, EVENT_SIG_FULL = 0, 3
 
+_FNV_OFFSET = np.uint64(0xCBF29CE484222325)
+_FNV_PRIME = np.uint64(0x100000001B3)
+
 # Every symbol include/hgx.h declares (the library must export all of them).
 EXPORTS = (
     "hgx_last_error", "hgx_version", "hgx_engine_create", "hgx_engine_destroy",
@@ -214,6 +217,35 @@ class EvolveResult:
             out.append(self.state_verts[v:v + a].tolist())
             v += a
         return out
+
+    def keys(self) -> dict:
+        """The result as schedule-independent sorted key arrays: the distinct WL class hashes,
+        the event keys fnv(WL(in), WL(out), rule, step), the causal keys fnv(key(producer),
+        key(consumer)) and the branchial keys fnv(min, max) -- the reference's own cross-engine
+        normalisation (gpu/tests/test_gpu_vs_cpu_differential.cpp:119-157). Two results are the
+        same evolution exactly when these arrays are equal."""
+        sh = np.asarray(self.state_hash, dtype=np.uint64)
+        ev = np.asarray(self.events, dtype=np.uint32).reshape(-1, 4)
+        with np.errstate(over="ignore"):
+            def fold(h, x):
+                return np.bitwise_xor(h, np.asarray(x, dtype=np.uint64)) * _FNV_PRIME
+
+            ek = np.full(len(ev), _FNV_OFFSET, dtype=np.uint64)
+            for col in (sh[ev[:, 0]], sh[ev[:, 1]], ev[:, 2], ev[:, 3]):
+                ek = fold(ek, col)
+            ca = np.asarray(self.causal, dtype=np.uint32).reshape(-1, 3)
+            ck = fold(fold(np.full(len(ca), _FNV_OFFSET, dtype=np.uint64), ek[ca[:, 0]]), ek[ca[:, 1]])
+            br = np.asarray(self.branchial, dtype=np.uint32).reshape(-1, 2)
+            a, b = ek[br[:, 0]], ek[br[:, 1]]
+            bk = fold(fold(np.full(len(br), _FNV_OFFSET, dtype=np.uint64), np.minimum(a, b)),
+                      np.maximum(a, b))
+        return {"state_hashes": np.unique(sh), "event_keys": np.sort(ek),
+                "causal_keys": np.sort(ck), "branchial_keys": np.sort(bk)}
+
+    def same_as(self, other: "EvolveResult") -> bool:
+        """Exact equality of the two results' key multisets (see keys())."""
+        a, b = self.keys(), other.keys()
+        return all(np.array_equal(a[k], b[k]) for k in a)
 
     def bytes(self) -> int:
         return sum(getattr(self, f).nbytes for f in (

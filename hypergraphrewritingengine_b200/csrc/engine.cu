@@ -2026,7 +2026,9 @@ extern "C" HGX_API hgx_status hgx_hash_states_noalloc(
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         if (err)
             return noalloc_fail(HGX_ERR_CAPACITY, "hgx_hash_states_noalloc: a state exceeds max_edges / "
-                                                  "max_occ, or the table overflowed (flags " +
+                                                  "max_occ or its record is inconsistent (an arity "
+                                                  "outside 1..16, or arities not adding up to its "
+                                                  "occurrence count), or the table overflowed (flags " +
                                                   std::to_string(err) + ")");
         return HGX_OK;
     } catch (const std::exception& e) {

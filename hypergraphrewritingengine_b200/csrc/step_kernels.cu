@@ -184,12 +184,24 @@ __device__ Parent load_parent(const DevPtrs& P, const Layout& L, char* sm, uint3
     for (uint32_t j = lane; j < pa.nocc; j += 32) glob[j] = rec[pa.ne + aw + j];
     __syncwarp();
     uint32_t run = 0;
+    bool bad = false;
     for (uint32_t b = 0; b < pa.ne; b += 32) {
         const uint32_t i = b + lane;
         const uint32_t a = i < pa.ne ? pear[i] : 0u;
+        bad |= __any_sync(0xFFFFFFFFu, i < pa.ne && (a == 0u || a > static_cast<uint32_t>(kMaxArity)));
         const uint32_t inc = warp_incl_scan(a);
         if (i < pa.ne) pevo[i] = static_cast<uint16_t>(run + inc - a);
         run += __shfl_sync(0xFFFFFFFFu, inc, 31);
+    }
+    // A record whose arities are out of range or do not add up to its occurrence count (possible
+    // only for records a caller supplies; the engine writes consistent ones) would send the vertex
+    // offsets past the staged occurrences: flag it and treat the state as empty.
+    if (bad || run != pa.nocc) {
+        if (lane == 0) atomicOr(P.err, kErrStateTooLarge);
+        __syncwarp();
+        pa.ne = 0;
+        pa.nocc = 0;
+        return pa;
     }
     if (pa.nocc > kHashOccMin && L.VT) {
         // Large state: vertex -> local id through a shared-memory hash table, O(occurrences).

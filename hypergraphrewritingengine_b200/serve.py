@@ -59,6 +59,9 @@ class Server:
         """Serve a stream. arrivals: list of (arrival_time_s, workloads.Evolution), sorted by
         time. realtime=False admits `admit_per_step` requests before every step instead of
         following the clock (deterministic staggering, used by the tests)."""
+        if admit_per_step is not None and admit_per_step < 1:
+            raise ValueError(f"admit_per_step must be >= 1 (got {admit_per_step}): "
+                             "nothing would ever be admitted")
         eng = self.eng
         eng.serve_reset()
         recs = [Record(i, t) for i, (t, _) in enumerate(arrivals)]

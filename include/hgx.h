@@ -254,7 +254,10 @@ HGX_API hgx_status hgx_engine_stream(hgx_engine* engine, void** stream);
    capture. Every call clears and reuses the same array, so calls that overlap on the GPU (from
    two streams or two threads) race: serialise them. The call runs on `stream` (a cudaStream_t,
    NULL = legacy default stream) and synchronises it before returning, to report device-side
-   errors (a state larger than the declared bounds). */
+   errors as HGX_ERR_CAPACITY: a state larger than the declared bounds, or a record whose arities
+   are outside 1..16 or do not add up to its d_num_occ entry (such a state is not hashed). The
+   resolved address is kept for the life of the process: resetting the device (cudaDeviceReset)
+   after the first call is not supported. */
 HGX_API hgx_status hgx_hash_states_noalloc(const uint32_t* d_records, const uint64_t* d_offsets,
                                            const uint32_t* d_num_edges, const uint32_t* d_num_occ,
                                            uint32_t n_states, uint32_t max_edges, uint32_t max_occ,

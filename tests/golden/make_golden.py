@@ -35,7 +35,8 @@ sys.path.insert(0, HERE)
 from oracle import pyoracle  # noqa: E402
 import cases  # noqa: E402
 
-REF_MATRIX = "/root/reference/reference/golden_matrix.txt"
+REF_MATRIX = os.path.join(os.environ.get("HGX_REFERENCE", "/root/reference"),
+                          "reference", "golden_matrix.txt")
 
 
 def tr_section():

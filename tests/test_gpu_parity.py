@@ -122,10 +122,38 @@ def test_chunked_cap_matches_oracle(engine, quotient, rule, init, steps, cap):
 def test_full_size_workloads_match_oracle(engine, ev):
     """The benchmarked sizes themselves (C2: 8 levels, 2M-state cap; C3: 6 levels)."""
     res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
-    ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+    ref = _oracle_once(ev)
     assert res.truncated == ref["truncated"]
     assert res.num_classes == ref["classes"]
     assert_same(norm_gpu(res), norm_oracle(ref), ev.name)
+
+
+_ORACLE_CACHE = {}
+
+
+def _oracle_once(ev):
+    key = ev.name
+    if key not in _ORACLE_CACHE:
+        _ORACLE_CACHE[key] = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient,
+                                             max_states=ev.max_states)
+    return _ORACLE_CACHE[key]
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_c3_full_size_with_forwarding_matches_oracle(engine, mode):
+    """C3 as benchmarked -- ternary rule, 6 levels, WL quotient -- with incremental match
+    forwarding on (1: every eligible state; 2: states of at least 48 edges)."""
+    from hypergraphrewritingengine_b200 import api
+    ev = W.config3(6)
+    ref = _oracle_once(ev)
+    engine.set_option(api.OPT_FORWARDING, mode)
+    try:
+        res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+    finally:
+        engine.set_option(api.OPT_FORWARDING, 0)
+    assert res.truncated == ref["truncated"]
+    assert res.num_classes == ref["classes"]
+    assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} forwarding={mode}")
 
 
 def _forwarding_cases():

@@ -124,3 +124,10 @@ def test_plain_path_serves_in_order():
     recs = serve.serve_plain(FakeEngine(), _stream([2, 0, 1]), realtime=False)
     assert [r.result.num_events for r in recs] == [2, 0, 1]
     assert all(recs[i].finished <= recs[i + 1].admitted for i in range(2))
+
+
+def test_admissions_per_step_below_one_are_rejected():
+    import pytest
+    for bad in (0, -1):
+        with pytest.raises(ValueError):
+            serve.Server(FakeEngine()).run(_stream([1]), realtime=False, admit_per_step=bad)

@@ -53,9 +53,11 @@ def _random_states(seed, n):
     return out
 
 
-def _noalloc(L, states):
+def _noalloc(L, states, nocc_fix=None, expect=0):
     import torch
     words, offs, ne, nocc = _records(states)
+    if nocc_fix is not None:
+        nocc_fix(words, offs, ne, nocc)
     dev = torch.device("cuda", 0)
     d_words = torch.from_numpy(words.view(np.int32)).to(dev)
     d_offs = torch.from_numpy(offs.view(np.int64)).to(dev)
@@ -69,7 +71,9 @@ def _noalloc(L, states):
         ctypes.c_void_p(d_ne.data_ptr()), ctypes.c_void_p(d_nocc.data_ptr()), len(states),
         int(ne.max()), int(nocc.max()), ctypes.c_void_p(d_hash.data_ptr()),
         ctypes.c_void_p(d_cls.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
-    assert st == 0, L.hgx_last_error()
+    assert st == expect, L.hgx_last_error()
+    if expect:
+        return None
     return d_hash.cpu().numpy().view(np.uint64), d_cls.cpu().numpy().view(np.uint32)
 
 
@@ -103,3 +107,25 @@ def test_noalloc_rejects_oversize_batch():
     st = L.hgx_hash_states_noalloc(None, None, None, None, (1 << 19) + 1, 4, 8, None, None, None)
     assert st == 3   # HGX_ERR_CAPACITY
     assert b"exceed the maximum" in L.hgx_last_error()
+
+
+def test_noalloc_rejects_inconsistent_record():
+    """A caller-supplied record whose arities do not add up to its occurrence count is reported
+    as a typed error (HGX_ERR_CAPACITY) instead of being hashed; the next call works."""
+    from hypergraphrewritingengine_b200 import load_library
+    L = load_library()
+    states = _random_states(3, 40)
+    bad = 7
+
+    def overstate(words, offs, ne, nocc):
+        # one extra vertex word in the declared count: the arities sum to one less than num_occ
+        # (the staged occurrences still hold every offset the arities give, so the record is
+        # read in bounds whether or not it is checked)
+        nocc[bad] += 1
+
+    _noalloc(L, states, nocc_fix=overstate, expect=3)
+    assert b"inconsistent" in L.hgx_last_error()
+    want_hash, want_cls, _ = _allocating(states)
+    got_hash, got_cls = _noalloc(L, states)
+    assert np.array_equal(got_hash, want_hash)
+    assert np.array_equal(got_cls, want_cls)
