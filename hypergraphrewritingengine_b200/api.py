@@ -33,7 +33,7 @@ LIB_PATH = os.path.join(HERE, "libhgx.so")
 HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_ERR_INTERNAL = range(6)
 (OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
  OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING, OPT_CHUNK_MIN,
- OPT_EVENT_SIGNATURE_KEYS, OPT_LANE_JOIN, OPT_LEVEL_SPLIT) = range(13)
+ OPT_EVENT_SIGNATURE_KEYS, OPT_LANE_JOIN, OPT_LEVEL_SPLIT, OPT_MAX_DEVICE_BYTES) = range(14)
 (COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
  COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES,
  COUNT_CANONICAL_EVENTS) = range(11)
@@ -56,6 +56,7 @@ EXPORTS = (
     "hgx_result_count",
     "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
     "hgx_engine_stream", "hgx_hash_states_noalloc", "hgx_result_view",
+    "hgx_estimate_device_bytes", "hgx_device_memory",
 )
 
 
@@ -112,6 +113,8 @@ def load_library(path: str = LIB_PATH):
         "hgx_engine_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
         "hgx_hash_states_noalloc": ([vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_uint32, vp, vp, vp], ctypes.c_int),
+        "hgx_estimate_device_bytes": ([ctypes.POINTER(Job), u64p], ctypes.c_int),
+        "hgx_device_memory": ([ctypes.c_int, u64p, u64p], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -301,6 +304,15 @@ def _read_result(handle) -> EvolveResult:
         state_vert_off=arrays[ARR_STATE_VERT_OFF], state_verts=arrays[ARR_STATE_VERTS],
         num_classes=cnt(COUNT_CLASSES), truncated=bool(cnt(COUNT_TRUNCATED)),
         event_signature=arrays[ARR_EVENT_SIG], num_canonical_events=cnt(COUNT_CANONICAL_EVENTS))
+
+
+def estimate_device_bytes(evolution) -> int:
+    """Estimated device bytes of one evolution (rules, roots, steps, cap) -- the engine's own
+    estimate through the C-ABI (hgx_estimate_device_bytes); needs no device."""
+    jobs, _keep = Engine.make_jobs([evolution])
+    b = ctypes.c_uint64()
+    _check(load_library().hgx_estimate_device_bytes(ctypes.byref(jobs[0]), ctypes.byref(b)))
+    return int(b.value)
 
 
 class Engine:

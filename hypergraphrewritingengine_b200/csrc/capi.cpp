@@ -232,6 +232,7 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
             return HGX_OK;
         case HGX_OPT_CHUNK_MIN: e->opt.chunk_min = value; return HGX_OK;
         case HGX_OPT_LEVEL_SPLIT: e->opt.level_split = value; return HGX_OK;
+        case HGX_OPT_MAX_DEVICE_BYTES: e->engine.set_device_limit(value); return HGX_OK;
         case HGX_OPT_LANE_JOIN:
             if (value > 2) return fail(HGX_ERR_INVALID, "lane join must be 0 (autotuned), 1 or 2");
             e->opt.lane_join = static_cast<uint32_t>(value);
@@ -345,6 +346,36 @@ hgx_status hgx_serve_device_bytes(hgx_engine* e, uint64_t* bytes) {
     if (!e || !bytes) return fail(HGX_ERR_INVALID, "null argument");
     *bytes = e->engine.device_bytes_in_use();
     return HGX_OK;
+}
+
+hgx_status hgx_estimate_device_bytes(const hgx_job* job, uint64_t* bytes) {
+    if (!job || !bytes) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        *bytes = hgx::Engine::estimate_bytes(spec_of(*job));
+        return HGX_OK;
+    });
+}
+
+hgx_status hgx_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes) {
+    if (!free_bytes || !total_bytes) return fail(HGX_ERR_INVALID, "null argument");
+    return guarded([&] {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+            throw std::runtime_error("no CUDA device");
+        if (device < 0 || device >= n) throw std::invalid_argument("device index out of range");
+        int prev = 0;
+        cudaError_t err = cudaGetDevice(&prev);
+        if (err != cudaSuccess) throw hgx::CudaError(err, "cudaGetDevice", __FILE__, __LINE__);
+        err = cudaSetDevice(device);
+        if (err != cudaSuccess) throw hgx::CudaError(err, "cudaSetDevice", __FILE__, __LINE__);
+        size_t f = 0, t = 0;
+        err = cudaMemGetInfo(&f, &t);
+        cudaSetDevice(prev);
+        if (err != cudaSuccess) throw hgx::CudaError(err, "cudaMemGetInfo", __FILE__, __LINE__);
+        *free_bytes = f;
+        *total_bytes = t;
+        return HGX_OK;
+    });
 }
 
 uint64_t hgx_result_count(const hgx_result* res, hgx_count what) {

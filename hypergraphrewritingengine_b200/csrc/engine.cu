@@ -27,6 +27,20 @@ uint64_t next_pow2(uint64_t x) {
     return p;
 }
 
+// Device-memory ceiling of the engine the calling host thread is driving (HGX_OPT_MAX_DEVICE_BYTES;
+// limit 0 = none): the bytes its growable arrays hold, and a growth that would pass the limit
+// throws a capacity error before allocating. Set for the duration of every engine call.
+struct DeviceBudget {
+    uint64_t limit = 0, used = 0;
+};
+thread_local DeviceBudget* t_budget = nullptr;
+
+struct BudgetScope {
+    DeviceBudget* prev;
+    explicit BudgetScope(DeviceBudget* b) : prev(t_budget) { t_budget = b; }
+    ~BudgetScope() { t_budget = prev; }
+};
+
 template <class T>
 struct DVec {
     T* p = nullptr;
@@ -35,6 +49,15 @@ struct DVec {
     void ensure(size_t n, size_t keep, cudaStream_t s) {
         if (n <= cap) return;
         size_t nc = std::max<size_t>(n, cap + cap / 2 + 1024);
+        if (t_budget) {
+            const uint64_t add = (nc - cap) * sizeof(T);
+            if (t_budget->limit && t_budget->used + add > t_budget->limit)
+                throw std::runtime_error("capacity: device memory limit of " +
+                                         std::to_string(t_budget->limit) + " bytes reached (the engine "
+                                         "holds " + std::to_string(t_budget->used) + " and needs " +
+                                         std::to_string(add) + " more)");
+            t_budget->used += add;
+        }
         T* np = nullptr;
         HGX_CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&np), nc * sizeof(T), s));
         if (p && keep)
@@ -46,6 +69,7 @@ struct DVec {
     }
     void release(cudaStream_t s) {
         if (p) cudaFreeAsync(p, s);
+        if (t_budget) t_budget->used -= std::min<uint64_t>(t_budget->used, cap * sizeof(T));
         p = nullptr;
         cap = 0;
     }
@@ -282,6 +306,7 @@ struct PinnedPool {
 
 struct Engine::Impl {
     int device = 0;
+    DeviceBudget budget;
     cudaStream_t st = nullptr;
     int timing = 0;   // 0 off, 1 every stage, 2 the expand kernel only
     StageTimes times;
@@ -1813,6 +1838,7 @@ Engine::~Engine() = default;
 
 std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs, const RunOptions& opt) {
     Impl& I = *impl_;
+    BudgetScope scope(&I.budget);
     HGX_CUDA_CHECK(cudaSetDevice(I.device));
     I.reset();
     std::vector<const EvolutionSpec*> ptrs;
@@ -1827,14 +1853,26 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
     return out;
 }
 
-void Engine::reset() { impl_->reset(); }
-uint32_t Engine::admit(const EvolutionSpec& spec) { return impl_->admit(spec); }
+void Engine::reset() {
+    BudgetScope scope(&impl_->budget);
+    impl_->reset();
+}
+uint32_t Engine::admit(const EvolutionSpec& spec) {
+    BudgetScope scope(&impl_->budget);
+    return impl_->admit(spec);
+}
 std::vector<uint32_t> Engine::admit(const std::vector<EvolutionSpec>& specs) {
+    BudgetScope scope(&impl_->budget);
     std::vector<const EvolutionSpec*> ptrs;
     for (const auto& s : specs) ptrs.push_back(&s);
     return impl_->admit_many(ptrs);
 }
-bool Engine::step(const RunOptions& opt) { return impl_->level(opt); }
+bool Engine::step(const RunOptions& opt) {
+    BudgetScope scope(&impl_->budget);
+    return impl_->level(opt);
+}
+void Engine::set_device_limit(uint64_t bytes) { impl_->budget.limit = bytes; }
+uint64_t Engine::device_limit() const { return impl_->budget.limit; }
 std::vector<uint32_t> Engine::take_finished() {
     std::vector<uint32_t> f;
     f.swap(impl_->finished);
@@ -1845,6 +1883,7 @@ EvolutionResult Engine::collect(uint32_t evo, const RunOptions& opt) {
     return std::move(collect(std::vector<uint32_t>{evo}, opt)[0]);
 }
 std::vector<EvolutionResult> Engine::collect(const std::vector<uint32_t>& evos, const RunOptions& opt) {
+    BudgetScope scope(&impl_->budget);
     for (uint32_t evo : evos)
         if (evo >= impl_->h_evos.size()) throw std::invalid_argument("collect: unknown evolution id");
     if (opt.readback) return impl_->finalize_many(evos, opt);
@@ -1864,12 +1903,55 @@ uint64_t Engine::device_bytes_in_use() const {
            I.tab_vals.bytes() + I.bpairs.bytes();
 }
 uint64_t Engine::estimate_bytes(const EvolutionSpec& spec) {
-    // Per state: record (~ 6 words/edge) + SoA (40 B); per event ~ 64 B + relations.
-    uint64_t edges = 0;
-    for (const auto& r : spec.roots) edges += r.size();
-    const uint64_t states = spec.max_states ? spec.max_states : 100000;
-    const uint64_t per_state = (edges + 4ull * spec.steps) * 24 + 40;
-    return states * per_state + states * 8 * 96 + states * 64;
+    // Level by level: the largest state at depth d has E_d = E_0 + d * max(0, rhs - lhs) edges
+    // (O_d occurrences likewise); a state has at most sum over rules of E_d! / (E_d - L)! matches
+    // (ordered edge-injective tuples); states are bounded by the cap (2^22 when uncapped), events
+    // by that bound and by 64 per state, branchial pairs by 16 per event. Bytes per state, event
+    // and pair follow the engine's arrays, with 1.5x growth slack.
+    auto sat_mul = [](uint64_t a, uint64_t b) -> uint64_t {
+        return (a && b > UINT64_MAX / a) ? UINT64_MAX : a * b;
+    };
+    uint64_t e0 = 0, o0 = 0;
+    for (const auto& r : spec.roots) {
+        uint64_t o = 0;
+        for (const auto& e : r) o += e.size();
+        e0 = std::max<uint64_t>(e0, r.size());
+        o0 = std::max(o0, o);
+    }
+    int64_t grow_e = 0, grow_o = 0;
+    uint64_t lhs_max = 1, rhs_max = 0;
+    for (const auto& r : spec.rules) {
+        int64_t lo = 0, ro = 0;
+        for (const auto& e : r.lhs) lo += static_cast<int64_t>(e.size());
+        for (const auto& e : r.rhs) ro += static_cast<int64_t>(e.size());
+        grow_e = std::max<int64_t>(grow_e, static_cast<int64_t>(r.rhs.size()) - static_cast<int64_t>(r.lhs.size()));
+        grow_o = std::max<int64_t>(grow_o, ro - lo);
+        lhs_max = std::max<uint64_t>(lhs_max, r.lhs.size());
+        rhs_max = std::max<uint64_t>(rhs_max, r.rhs.size());
+    }
+    const uint64_t cap = spec.max_states ? spec.max_states : (1ull << 22);
+    uint64_t frontier = spec.roots.size(), states = spec.roots.size(), events = 0;
+    for (uint32_t d = 0; d < spec.steps && frontier && states < cap; ++d) {
+        const uint64_t E = e0 + d * static_cast<uint64_t>(grow_e);
+        uint64_t m = 0;
+        for (const auto& r : spec.rules) {
+            uint64_t p = 1;
+            for (uint64_t k = 0; k < r.lhs.size(); ++k) p = sat_mul(p, E > k ? E - k : 0);
+            m = std::min<uint64_t>(UINT64_MAX - p, m) + p;
+        }
+        const uint64_t ev = sat_mul(frontier, m);
+        events = std::min<uint64_t>(UINT64_MAX - ev, events) + ev;
+        const uint64_t fresh = std::min(cap - states, ev);
+        states += fresh;
+        frontier = fresh;
+    }
+    events = std::min(events, 64 * states);
+    const uint64_t E = e0 + spec.steps * static_cast<uint64_t>(grow_e);
+    const uint64_t O = o0 + spec.steps * static_cast<uint64_t>(grow_o);
+    const uint64_t per_state = 56 + 4 * (E + (E + 3) / 4 + O) + 48;   // SoA + record + table
+    const uint64_t per_event = 112 + 8 * lhs_max + 4 * rhs_max + 16 * 8;   // + branchial pairs
+    const uint64_t total = states * per_state + events * per_event;
+    return total + total / 2 + (1ull << 20);
 }
 cudaStream_t Engine::stream() const { return impl_->st; }
 void Engine::set_timing(int level) { impl_->timing = level; }

@@ -146,6 +146,10 @@ public:
     std::vector<EvolutionResult> collect(const std::vector<uint32_t>& evos, const RunOptions& opt = {});
     uint32_t active() const;
     uint64_t device_bytes_in_use() const;
+    // Ceiling on the bytes the engine's device arrays may hold (0 = none): a growth past it
+    // throws a capacity error instead of allocating (the call then fails with HGX_ERR_CAPACITY).
+    void set_device_limit(uint64_t bytes);
+    uint64_t device_limit() const;
     static uint64_t estimate_bytes(const EvolutionSpec& spec);
 
     cudaStream_t stream() const;

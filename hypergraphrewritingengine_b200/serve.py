@@ -39,21 +39,28 @@ class Record:
 
 
 def estimate_bytes(ev) -> int:
-    """Device-memory estimate of one evolve request (states, events, relations, tables)."""
-    edges = sum(len(st) for st in ev.roots)
-    states = ev.max_states or 100_000
-    per_state = (edges + 4 * ev.steps) * 24 + 48      # record + state arrays
-    per_event = 96                                     # event arrays + consumed lists + pairs
-    return int(states * per_state + 8 * states * per_event + 32 * states)
+    """Device-memory estimate of one evolve request: the engine's own estimate (states, events,
+    relations and dedup tables from the rules, roots, step budget and state cap; an uncapped
+    request is estimated at the states its step budget can reach, at most 2^22), through the
+    C-ABI (hgx_estimate_device_bytes; reference: hg_gpu::estimated_device_bytes)."""
+    return api.estimate_device_bytes(ev)
 
 
 class Server:
     """Continuous batching over one api.Engine."""
 
-    def __init__(self, engine: api.Engine, memory_budget: float = 140e9, max_active: int = 1 << 16):
+    def __init__(self, engine: api.Engine, memory_budget: float = 140e9, max_active: int = 1 << 16,
+                 track_device_bytes: bool = False):
         self.eng = engine
         self.budget = memory_budget
         self.max_active = max_active
+        # admission bookkeeping of the last run: requests admitted per admission call, the
+        # largest estimated footprint admitted at once, and (when tracked) the largest device
+        # footprint the engine reported after a step
+        self.track = track_device_bytes
+        self.admit_sizes: list[int] = []
+        self.peak_reserved = 0
+        self.peak_device_bytes = 0
 
     def run(self, arrivals, realtime: bool = True, admit_per_step: int | None = None):
         """Serve a stream. arrivals: list of (arrival_time_s, workloads.Evolution), sorted by
@@ -64,6 +71,7 @@ class Server:
                              "nothing would ever be admitted")
         eng = self.eng
         eng.serve_reset()
+        self.admit_sizes, self.peak_reserved, self.peak_device_bytes = [], 0, 0
         recs = [Record(i, t) for i, (t, _) in enumerate(arrivals)]
         pending = collections.deque(range(len(arrivals)))
         active = {}            # engine evolution id -> request index
@@ -104,6 +112,8 @@ class Server:
                 recs[i].meta["est"] = est
                 reserved += est
             if take:
+                self.admit_sizes.append(len(take))
+                self.peak_reserved = max(self.peak_reserved, reserved)
                 jobs, blobs = api.Engine.make_jobs([arrivals[i][1] for i in take])
                 ids = eng.serve_admit_batch(jobs, len(take))
                 t_adm = now()
@@ -122,6 +132,8 @@ class Server:
                         time.sleep(wait)
                 continue
             eng.serve_step()
+            if self.track:
+                self.peak_device_bytes = max(self.peak_device_bytes, eng.device_bytes())
             collect_finished()
         return recs
 

@@ -101,7 +101,13 @@ typedef enum hgx_option {
        the cap is not reached. 0 (default) = prefix sized by that estimate, 1 = never split,
        N >= 2 = a prefix of N frontier states whenever the frontier is larger (for tests). No
        reference counterpart; results are identical for every value. */
-    HGX_OPT_LEVEL_SPLIT = 12
+    HGX_OPT_LEVEL_SPLIT = 12,
+    /* Ceiling on the device memory the engine's arrays may hold, in bytes (0 = none, the
+       default). A growth past it fails the call with HGX_ERR_CAPACITY before allocating, instead
+       of pushing the GPU to a real out-of-memory. Replaces EvolveInput::max_device_memory_bytes
+       (gpu/include/hg_gpu/evolve.hpp:136-141), whose one-shot evolve stops at the limit with a
+       kDeviceOutOfMemory warning; the hg_gpu shim maps the error to that warning. */
+    HGX_OPT_MAX_DEVICE_BYTES = 13
 } hgx_option;
 
 /* One evolution of a batch or a served request. */
@@ -200,6 +206,18 @@ HGX_API hgx_status hgx_serve_collect(hgx_engine* engine, uint32_t evolution_id, 
 HGX_API hgx_status hgx_serve_collect_batch(hgx_engine* engine, const uint32_t* evolution_ids, uint32_t n,
                                            hgx_result** out);
 HGX_API hgx_status hgx_serve_device_bytes(hgx_engine* engine, uint64_t* bytes);
+
+/* Estimated device bytes one evolution will hold (state records, events, relations, dedup
+   tables), from its rules, roots, step budget and state cap, without running it. Replaces
+   hg_gpu::estimated_device_bytes(config_from_input(input)) (gpu/include/hg_gpu/evolve.hpp:404,
+   :409); used by the serving loop's memory-budget admission. An uncapped evolution is
+   estimated at the states its step budget can reach (bounded by 2^22). */
+HGX_API hgx_status hgx_estimate_device_bytes(const hgx_job* job, uint64_t* bytes);
+
+/* Free and total memory of a device (cudaMemGetInfo with that device current), for resolving
+   EvolveInput::max_device_memory_bytes = 0 to 90% of the device's memory as the reference does
+   (gpu/include/hg_gpu/evolve.hpp:136-141). */
+HGX_API hgx_status hgx_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
 
 /* Result accessors. Replace Hypergraph::num_states / num_events / num_canonical_states
    (hypergraph/include/hypergraph/hypergraph.hpp:567, :749, :694),

@@ -8,14 +8,15 @@
 //                         hg.causal_graph().get_causal_edges() / get_branchial_edges()
 //                         (reference: hypergraph/include/hypergraph/pattern.hpp:142-213,
 //                          parallel_evolution.hpp:743-1041, hypergraph.hpp:567-811)
-//   hgx::compat::gpu      RewriteRule / EvolveInput / EvolveResult and evolve(const EvolveInput&)
-//                         (reference: gpu/include/hg_gpu/evolve.hpp:19-173, :368)
+//   hgx::compat::gpu      RewriteRule / EvolveInput / EvolveResult, evolve(const EvolveInput&),
+//                         Engine, PersistentEvolver, EngineConfig, config_from_input,
+//                         estimated_device_bytes (reference: gpu/include/hg_gpu/evolve.hpp;
+//                         defined in hgx/hg_gpu.hpp, included at the end of this header)
 //
 // The evolution is the B200 step in WL mode: a state's canonical_hash is its WL hash, and with
 // explore_from_canonical_states_only each WL class is expanded once at its shortest depth.
 // Errors throw std::length_error (rule limits, as RuleBuilder does) or std::runtime_error
-// (everything else, with the library's message). Transitive reduction is not provided on this
-// path: requesting it throws.
+// (everything else, with the library's message).
 #pragma once
 #include <cstdint>
 #include <memory>
@@ -248,151 +249,8 @@ private:
 
 }  // namespace engine
 
-// =============================================================================================
-// The GPU-engine DTO surface (namespace hg_gpu in the reference)
-// =============================================================================================
-namespace gpu {
-
-using VertexId = uint32_t;
-using StateId = uint32_t;
-using EventId = uint32_t;
-using EdgeId = uint32_t;
-
-struct RewriteRule {
-    std::vector<std::vector<uint8_t>> lhs;
-    std::vector<std::vector<uint8_t>> rhs;
-    uint8_t num_lhs_vars = 0;
-    uint8_t num_rhs_vars = 0;
-};
-
-enum class EventCanonicalizationMode : uint8_t { None = 0, Full, Automatic };
-
-struct EvolveInput {
-    std::vector<RewriteRule> rules;
-    std::vector<std::vector<VertexId>> initial_state;
-    std::vector<std::vector<std::vector<VertexId>>> initial_states;   // takes precedence
-    uint32_t num_steps = 0;
-    bool transitive_reduction = true;           // as the reference's default
-    // None / Full (input and output WL hashes); Automatic needs edge ranks and is rejected
-    EventCanonicalizationMode event_canonicalization = EventCanonicalizationMode::None;
-    bool explore_from_canonical_states_only = true;
-    // As the reference (evolve.hpp:36): states always carry their edge contents; true also
-    // carries each state's global edge ids (EvolveResult::state_edge_ids). The reference's
-    // edge id -> vertices table (global_edges) is not provided: edges produced by events whose
-    // child was a duplicate are never materialised on this path.
-    bool edge_identity = false;
-    uint64_t max_states = 0;
-};
-
-struct CanonicalState {
-    StateId id = 0xFFFFFFFFu;
-    uint64_t canonical_hash = 0;
-    std::vector<std::vector<VertexId>> edges;
-};
-
-struct Event {
-    EventId id = 0xFFFFFFFFu;
-    EventId canonical_id = 0xFFFFFFFFu;   // first event with the same signature (= id when off)
-    uint64_t signature = 0;               // 0 under EventCanonicalizationMode::None
-    StateId input_state = 0xFFFFFFFFu, output_state = 0xFFFFFFFFu;
-    uint32_t rule = 0, step = 0;
-    std::vector<EdgeId> consumed_edges, produced_edges;
-};
-
-struct CausalEdge {
-    EventId from, to;
-};
-struct BranchialEdge {
-    EventId a, b;
-};
-
-struct EvolveResult {
-    std::vector<CanonicalState> states;
-    std::vector<std::vector<EdgeId>> state_edge_ids;   // per state, when edge_identity is set
-    std::vector<Event> events;
-    std::vector<CausalEdge> causal_edges;       // one per (producer, consumer, edge) triple
-    std::vector<BranchialEdge> branchial_edges;
-    std::vector<std::string> warnings;
-    uint64_t num_classes = 0;
-};
-
-inline EvolveResult evolve(const EvolveInput& in, int device = 0) {
-    hgx_engine* e = nullptr;
-    detail::check(hgx_engine_create(device, &e));
-    std::unique_ptr<hgx_engine, detail::EngineDeleter> eng(e);
-    for (const auto& r : in.rules) {
-        auto b = detail::rule_blob(r.lhs, r.rhs);
-        detail::check(hgx_engine_add_rule(e, b.data(), b.size()));
-    }
-    detail::check(hgx_engine_set_option(e, HGX_OPT_TRANSITIVE_REDUCTION, in.transitive_reduction));
-    detail::check(hgx_engine_set_option(e, HGX_OPT_QUOTIENT, in.explore_from_canonical_states_only));
-    detail::check(hgx_engine_set_option(e, HGX_OPT_KEEP_STATE_EDGES, 1));
-    detail::check(hgx_engine_set_option(e, HGX_OPT_MAX_STATES, in.max_states));
-    if (in.event_canonicalization == EventCanonicalizationMode::Automatic)
-        throw std::invalid_argument("event canonicalization Automatic needs edge ranks (not provided)");
-    detail::check(hgx_engine_set_option(e, HGX_OPT_EVENT_SIGNATURE_KEYS,
-                                        in.event_canonicalization == EventCanonicalizationMode::Full ? 3 : 0));
-    const auto blob = in.initial_states.empty()
-                          ? detail::roots_blob(std::vector<std::vector<std::vector<VertexId>>>{in.initial_state})
-                          : detail::roots_blob(in.initial_states);
-    hgx_result* rr = nullptr;
-    detail::check(hgx_evolve(e, blob.data(), blob.size(), in.num_steps, &rr));
-    std::unique_ptr<hgx_result, detail::ResultDeleter> res(rr);
-    EvolveResult out;
-    auto hash = detail::copy_array<uint64_t>(rr, HGX_ARR_STATE_HASH);
-    auto eoff = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_EDGE_OFF);
-    auto eids = in.edge_identity ? detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_EDGE_IDS)
-                                 : std::vector<uint32_t>{};
-    auto ar = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_ARITY);
-    auto voff = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_VERT_OFF);
-    auto verts = detail::copy_array<uint32_t>(rr, HGX_ARR_STATE_VERTS);
-    out.states.resize(hash.size());
-    if (in.edge_identity) out.state_edge_ids.resize(hash.size());
-    for (size_t s = 0; s < hash.size(); ++s) {
-        out.states[s].id = static_cast<StateId>(s);
-        out.states[s].canonical_hash = hash[s];
-        if (eoff.size() > s + 1) {
-            uint32_t v = voff[s];
-            for (uint32_t k = eoff[s]; k < eoff[s + 1]; ++k) {
-                out.states[s].edges.emplace_back(verts.begin() + v, verts.begin() + v + ar[k]);
-                v += ar[k];
-            }
-            if (in.edge_identity)
-                out.state_edge_ids[s].assign(eids.begin() + eoff[s], eids.begin() + eoff[s + 1]);
-        }
-    }
-    auto ev = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENTS);
-    auto coff = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENT_CONS_OFF);
-    auto cons = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENT_CONS);
-    auto prod = detail::copy_array<uint32_t>(rr, HGX_ARR_EVENT_PROD);
-    auto sig = detail::copy_array<uint64_t>(rr, HGX_ARR_EVENT_SIG);
-    std::unordered_map<uint64_t, EventId> first_of;
-    out.events.resize(ev.size() / 4);
-    for (size_t i = 0; i < out.events.size(); ++i) {
-        Event& x = out.events[i];
-        x.id = static_cast<EventId>(i);
-        x.canonical_id = x.id;
-        if (sig.size() == out.events.size()) {
-            x.signature = sig[i];
-            x.canonical_id = first_of.emplace(sig[i], x.id).first->second;
-        }
-        x.input_state = ev[4 * i];
-        x.output_state = ev[4 * i + 1];
-        x.rule = ev[4 * i + 2];
-        x.step = ev[4 * i + 3];
-        x.consumed_edges.assign(cons.begin() + coff[i], cons.begin() + coff[i + 1]);
-        for (uint32_t k = 0; k < prod[2 * i + 1]; ++k) x.produced_edges.push_back(prod[2 * i] + k);
-    }
-    auto ca = detail::copy_array<uint32_t>(rr, HGX_ARR_CAUSAL);
-    for (size_t i = 0; i + 2 < ca.size(); i += 3) out.causal_edges.push_back({ca[i], ca[i + 1]});
-    auto br = detail::copy_array<uint32_t>(rr, HGX_ARR_BRANCHIAL);
-    for (size_t i = 0; i + 1 < br.size(); i += 2) out.branchial_edges.push_back({br[i], br[i + 1]});
-    out.num_classes = hgx_result_count(rr, HGX_COUNT_CLASSES);
-    if (hgx_result_count(rr, HGX_COUNT_TRUNCATED))
-        out.warnings.push_back("capacity limit reached: the state cap stopped the evolution");
-    return out;
-}
-
-}  // namespace gpu
 }  // namespace compat
 }  // namespace hgx
+
+// The GPU-engine surface (hg_gpu::evolve, Engine, PersistentEvolver and their DTOs).
+#include "hg_gpu.hpp"

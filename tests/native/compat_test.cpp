@@ -54,6 +54,57 @@ int main() {
         threw = true;
     }
     ok = ok && threw;
+
+    // the rest of the hg_gpu surface: Engine, PersistentEvolver, sizing, modes, refusals
+    namespace G = hgx::compat::gpu;
+    const G::EngineConfig cfg = G::config_from_input(in);
+    G::EngineConfig bigger = cfg;
+    bigger.max_states *= 2;
+    const bool sizing = cfg.max_states >= (1u << 14) &&
+                        G::estimated_device_bytes(bigger) > G::estimated_device_bytes(cfg);
+    G::PersistentEvolver pe;
+    const auto p1 = pe.run(in);
+    const auto p2 = pe.run(in);   // the same engine, reused
+    const bool persistent = pe.has_engine() && p1.states.size() == 1952 && p2.events.size() == 5056 &&
+                            !pe.run_session(in, nullptr, 0).ok;
+    G::EvolveInput full = in;     // canonicalization None: every state its own class
+    full.rules = {{{{0, 1}, {1, 2}}, {{0, 1}, {1, 2}, {2, 0}}, 3, 3}};
+    full.initial_state = {{1, 2}, {2, 3}, {3, 1}};
+    full.canonicalization = G::CanonicalizationMode::None;
+    full.transitive_reduction = false;
+    full.edge_identity = false;
+    const auto rf = G::evolve(full);
+    const bool none_mode = rf.states.size() == 22204 && rf.events.size() == 22203 &&
+                           rf.observable_num_branchial() == 78045;
+    G::EvolveInput two = in;      // two isomorphic roots collapse under quotient_initial_states
+    two.initial_states = {{{1, 1}, {1, 1}}, {{5, 5}, {5, 5}}};
+    two.num_steps = 2;
+    const auto t_sep = G::evolve(two);
+    two.quotient_initial_states = true;
+    const auto t_one = G::evolve(two);
+    G::EvolveInput single = two;
+    single.initial_states = {{{1, 1}, {1, 1}}};
+    const auto t_single = G::evolve(single);
+    const bool roots_ok = t_one.events.size() == t_single.events.size() &&
+                          t_one.states.size() == t_single.states.size() &&
+                          t_sep.events.size() > t_one.events.size();
+    G::EvolveInput capped = in;   // a device-memory ceiling below what the run needs
+    capped.max_device_memory_bytes = 4096;
+    const auto rc = G::evolve(capped);
+    const bool oom = rc.states.empty() && !rc.warnings.empty() &&
+                     rc.warnings[0].kind == G::ErrorKind::kDeviceOutOfMemory;
+    bool sampling_refused = false;
+    try {
+        G::EvolveInput s2 = in;
+        s2.exploration_probability = 0.5f;
+        G::evolve(s2);
+    } catch (const std::invalid_argument&) {
+        sampling_refused = true;
+    }
+    std::printf("hg_gpu: sizing %d persistent %d none-mode %d roots %zu/%zu oom %d sampling refused %d\n",
+                sizing, persistent, none_mode, t_sep.events.size(), t_one.events.size(), oom,
+                sampling_refused);
+    ok = ok && sizing && persistent && none_mode && roots_ok && oom && sampling_refused;
     std::printf(ok ? "compat ok\n" : "compat MISMATCH\n");
     return ok ? 0 : 1;
 }

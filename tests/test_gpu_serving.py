@@ -51,3 +51,32 @@ def test_realtime_serving_and_plain_agree(engine):
         assert_same(norm_gpu(a.result), norm_gpu(b.result), f"request {a.rid}")
     s = summarize(served)
     assert s["p99_ms"] >= s["p50_ms"] > 0
+
+
+def test_memory_budget_binds_and_results_equal_alone():
+    """A budget that holds a few requests at a time: admission defers (several admission calls,
+    none over the budget unless a request runs alone), every result equals the request evolved
+    alone, and the device footprint the engine reports stays within the estimates admitted.
+    Requests over the budget by themselves (uncapped ones) run alone."""
+    from hypergraphrewritingengine_b200 import Engine
+    from hypergraphrewritingengine_b200.serve import estimate_bytes
+    stream = W.config5_stream(24, rate_per_s=1e9, seed=21, max_states=1024)
+    # two uncapped requests with a small step budget: estimated past the budget, so alone
+    for k in (5, 17):
+        t, ev = stream[k]
+        stream[k] = (t, W.Evolution(rules=ev.rules, roots=ev.roots, steps=2, max_states=0))
+    est = [estimate_bytes(ev) for _, ev in stream]
+    capped = sorted(e for (_, ev), e in zip(stream, est) if ev.max_states)
+    budget = capped[-1] * 3.5
+    assert est[5] > budget and est[17] > budget
+    eng = Engine(0)        # a fresh engine: its footprint is this stream's alone
+    try:
+        srv = Server(eng, memory_budget=budget, track_device_bytes=True)
+        recs = srv.run(stream, realtime=False)
+        assert len(srv.admit_sizes) > 3 and sum(srv.admit_sizes) == len(stream)
+        assert srv.peak_device_bytes <= srv.peak_reserved
+        for rec, (_, ev) in zip(recs, stream):
+            alone = eng.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            assert_same(norm_gpu(rec.result), norm_gpu(alone), f"request {rec.rid}")
+    finally:
+        eng.close()
