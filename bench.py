@@ -393,6 +393,7 @@ def main():
             line["c3"] = c3_forwarding(eng, stream, flush)
             line["batched"] = batched_vs_plain(eng)
             line["batched_cap_65536"] = batched_vs_plain(eng, max_states=1 << 16)
+            line["join_index"] = join_index_ab(eng)
             line["served"] = served_vs_plain(eng)
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -470,6 +471,48 @@ def c3_forwarding(eng, stream, flush, reps=10):
                                  "identical_to_forwarding_off": same})
     finally:
         eng.set_option(api.OPT_FORWARDING, 0)
+    return out
+
+
+def join_index_ab(eng, reps=3):
+    """The join with and without its vertex / signature indices (states past 64 edges), on the
+    batched workload (C4) and on a batch of large-state evolutions (256 draws of the same
+    generator with 65-256 initial edges, 2-4 steps, cap 4096): device time of the warp-per-child
+    expand kernel (the large-state path) and wall time of the whole batch, best of `reps`."""
+    from hypergraphrewritingengine_b200 import api
+    from hypergraphrewritingengine_b200 import workloads as W
+    work = {"c4": W.config4(n=1024),
+            "large": [W.random_evolution(i, seed=0x1A26E, edges_lo=65, edges_hi=256, steps_lo=2,
+                                         steps_hi=4) for i in range(256)]}
+    out = {}
+    eng.set_option(api.OPT_READBACK, 0)
+    eng.set_option(api.OPT_TIMING, 1)
+    try:
+        for name, evs in work.items():
+            jobs, keep = eng.make_jobs(evs)
+            row = {}
+            for index in (0, 1):
+                eng.set_option(api.OPT_JOIN_INDEX, index)
+                best = None
+                for _ in range(reps + 1):
+                    outs = (api.ctypes.c_void_p * len(evs))()
+                    t0 = time.perf_counter()
+                    api._check(eng._L.hgx_evolve_batch(eng._h, jobs, len(evs), outs))
+                    dt = time.perf_counter() - t0
+                    ev_total = sum(int(eng._L.hgx_result_count(outs[i], 1)) for i in range(len(evs)))
+                    for i in range(len(evs)):
+                        eng._L.hgx_result_free(outs[i])
+                    st, _ = eng.stage_times()
+                    xs = eng.expand_stats()
+                    cur = {"wall_ms": dt * 1e3, "device_ms": st["total"], "count_ms": st["count"],
+                           "warp_expand_ms": xs["warp_ns"] / 1e6, "events": ev_total}
+                    best = cur if best is None or cur["wall_ms"] < best["wall_ms"] else best
+                row["index_on" if index else "index_off"] = best
+            out[name] = row
+    finally:
+        eng.set_option(api.OPT_JOIN_INDEX, 1)
+        eng.set_option(api.OPT_TIMING, 0)
+        eng.set_option(api.OPT_READBACK, 1)
     return out
 
 

@@ -28,12 +28,14 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhgx.so")
+# HGX_LIB names another build of the library (for comparing builds side by side)
+LIB_PATH = os.environ.get("HGX_LIB", os.path.join(HERE, "libhgx.so"))
 
 HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_ERR_INTERNAL = range(6)
 (OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
  OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING, OPT_CHUNK_MIN,
- OPT_EVENT_SIGNATURE_KEYS, OPT_LANE_JOIN, OPT_LEVEL_SPLIT, OPT_MAX_DEVICE_BYTES) = range(14)
+ OPT_EVENT_SIGNATURE_KEYS, OPT_LANE_JOIN, OPT_LEVEL_SPLIT, OPT_MAX_DEVICE_BYTES,
+ OPT_JOIN_INDEX) = range(15)
 (COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
  COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES,
  COUNT_CANONICAL_EVENTS) = range(11)

@@ -233,6 +233,7 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
         case HGX_OPT_CHUNK_MIN: e->opt.chunk_min = value; return HGX_OK;
         case HGX_OPT_LEVEL_SPLIT: e->opt.level_split = value; return HGX_OK;
         case HGX_OPT_MAX_DEVICE_BYTES: e->engine.set_device_limit(value); return HGX_OK;
+        case HGX_OPT_JOIN_INDEX: e->opt.join_index = value != 0; return HGX_OK;
         case HGX_OPT_LANE_JOIN:
             if (value > 2) return fail(HGX_ERR_INVALID, "lane join must be 0 (autotuned), 1 or 2");
             e->opt.lane_join = static_cast<uint32_t>(value);

@@ -123,6 +123,9 @@ DevRule pack_rule(const RuleSpec& r) {
     }
     d.rhs_total = static_cast<uint8_t>(off);
     d.new_mask = rhs_mask & ~lhs_mask;
+    d.rhs_uni = r.rhs.empty() ? 0 : static_cast<uint8_t>(r.rhs[0].size());
+    for (const auto& e : r.rhs)
+        if (e.size() != d.rhs_uni) d.rhs_uni = 0;
     {
         // RHS connectivity over its variables (union-find on 32 labels)
         uint8_t up[kMaxVars];
@@ -168,7 +171,7 @@ enum class LayoutKind { Count, Lane, Warp };
 // Shared-memory carve-up per warp. Count: the parent and the join. Lane: plus the parent's
 // per-vertex occurrence lists and a 32-match batch. Warp: plus the warp-per-child WL arrays.
 Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kind, bool fwd = false,
-                   uint32_t mcap = kLaneJoinCap) {
+                   uint32_t mcap = kLaneJoinCap, bool index = false) {
     const bool wl = kind == LayoutKind::Warp;
     const bool lane = kind == LayoutKind::Lane;
     Layout L;
@@ -233,6 +236,15 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.o_vtab = take(4 * L.VT, 4);
         L.o_vtid = take(2 * L.VT, 2);
     }
+    if (index && !lane && NE > kJoinIndexMin) {
+        L.XI = 1;
+        L.o_xready = take(4, 4);
+        L.o_xoff = take(4 * (NOCC + 1), 4);
+        L.o_xinc = take(2 * NOCC, 2);
+        L.o_bkey = take(8 * (kSigBuckets + 1), 8);
+        L.o_boff = take(4 * (kSigBuckets + 1), 4);
+        L.o_blist = take(2 * NE, 2);
+    }
     if (wl) {
         uint32_t n2 = 64;   // distinct-colour hash set: >= 2 slots per vertex, + a zero flag
         while (n2 < 2 * L.V) n2 <<= 1;
@@ -246,6 +258,7 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.o_pnbr = take(2 * NOCC * (rm.arity - 1), 2);
         L.o_pnn = take(2 * kLaneVMax, 2);
         L.o_pconn = take(4, 4);
+        L.o_pcnt = take(4 * kLaneVMax, 4);
         L.o_pdeg = take(2 * kLaneVMax, 2);
         L.MCAP = std::max<uint32_t>(1, std::min<uint32_t>(mcap, kLaneJoinCap));
         L.region_bytes = align_up(off, 16);   // batch and match list last: regions >= 1 stop here
@@ -1379,7 +1392,8 @@ struct Engine::Impl {
         const bool fwd = opt.forwarding != 0;
         A.fwd_mode = opt.forwarding;
         A.ev_keys = opt.event_keys;
-        const Layout Lc = make_layout(ne_bound, nocc_bound, rm, LayoutKind::Count, fwd);
+        const Layout Lc = make_layout(ne_bound, nocc_bound, rm, LayoutKind::Count, fwd, kLaneJoinCap,
+                                      opt.join_index != 0);
         fmode.ensure(F, 0, st);
         A.fmode = fmode.p;
         LaunchShape sc = warp_shape(k_count, Lc, F);
@@ -1488,7 +1502,8 @@ struct Engine::Impl {
             const uint32_t mne = std::max<uint32_t>(fmax_ne, 1), mno = std::max<uint32_t>(fmax_nocc, 1);
             const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane, fwd,
                                           fmax_cnt);
-            const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp, fwd);
+            const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp, fwd, kLaneJoinCap,
+                                          opt.join_index != 0);
             // lane kernel join: autotuned per bucket of children per frontier state (the walk
             // amortises its count-and-emit passes over many children per state)
             const uint64_t per_state = n_ev / std::max<uint32_t>(F, 1);

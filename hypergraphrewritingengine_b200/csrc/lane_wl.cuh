@@ -149,47 +149,73 @@ HGX_NOINLINE uint64_t lane_component_term(const uint8_t* pear, const uint16_t* p
     return cs;
 }
 
+// Occurrence count of a packed per-position count word (one byte per position).
+HGX_HD uint32_t lane_bytesum(uint32_t c) { return (c * 0x01010101u) >> 24; }
+
+// pinfo: bit 0 = the parent is connected; bits 8.. = A when every parent edge has arity A (2..4),
+// else 0. With A set and every RHS edge of arity A too (R.rhs_uni == A), a vertex's initial
+// colour follows from its occurrence counts per position (pcnt: byte q = occurrences at position
+// q), since the sorted (arity, position) multiset is then the positions in ascending order with
+// their multiplicities, and no truncation applies (every vertex has at least as many neighbour
+// entries as occurrences when A >= 2).
 template <int VM, int NM>
 HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const uint16_t* vloc,
                              const uint16_t* poff, const uint16_t* pocc, const uint16_t* pdeg,
                              const uint16_t* pnn, const uint16_t* pnoff, const uint16_t* pnbr,
-                             bool pconn, uint32_t pne, uint32_t nvp, const DevRule& R,
-                             const uint8_t* slot, WlInfo& info) {
+                             const uint32_t* pcnt, uint32_t pinfo, uint32_t pne, uint32_t nvp,
+                             const DevRule& R, const uint8_t* slot, WlInfo& info) {
     const uint8_t* rpos = slot;
     const uint8_t* prodv = slot + R.n_lhs;
     const uint32_t V = nvp + R.n_fresh;
     const uint32_t ne = pne - R.n_lhs + R.n_rhs;
+    const bool pconn = (pinfo & 1u) != 0;
+    const uint32_t A = (pinfo >> 8) == R.rhs_uni ? (pinfo >> 8) : 0u;   // uniform arity, or 0
     info.rounds = info.nv = info.nocc = info.nbr = 0;
     if (ne == 0) return kEmptyStateHash;
 
     uint64_t rmask = 0;
         #pragma unroll 1
     for (uint32_t k = 0; k < R.n_lhs; ++k) rmask |= 1ull << rpos[k];
-    uint32_t dn[VM];   // degree | neighbour count << 16
-        #pragma unroll 1
-    for (uint32_t v = 0; v < V; ++v) dn[v] = v < nvp ? (pdeg[v] | (uint32_t(pnn[v]) << 16)) : 0u;
-        #pragma unroll 1
-    for (uint32_t k = 0; k < R.n_lhs; ++k) {
-        const uint32_t e = rpos[k], a = pear[e], vo = pevo[e];
+    // uniform arity: occurrences by position (byte q); otherwise degree | neighbour count << 16
+    uint32_t dn[VM];
+    if (A) {
                 #pragma unroll 1
-        for (uint32_t q = 0; q < a; ++q) {
-            const uint32_t v = vloc[vo + q];
-            dn[v] -= 1u + ((a - 1u) << 16);
+        for (uint32_t v = 0; v < V; ++v) dn[v] = v < nvp ? pcnt[v] : 0u;
+                #pragma unroll 1
+        for (uint32_t k = 0; k < R.n_lhs; ++k) {
+            const uint32_t vo = pevo[rpos[k]];
+                        #pragma unroll 1
+            for (uint32_t q = 0; q < A; ++q) dn[vloc[vo + q]] -= 1u << (8 * q);
         }
-    }
-        #pragma unroll 1
-    for (uint32_t k = 0; k < R.n_rhs; ++k) {
-        const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
                 #pragma unroll 1
-        for (uint32_t q = 0; q < a; ++q) {
-            const uint32_t v = prodv[o + q];
-            dn[v] += 1u + ((a - 1u) << 16);
+        for (uint32_t p = 0; p < R.rhs_total; ++p) dn[prodv[p]] += 1u << (8 * (p % A));
+    } else {
+                #pragma unroll 1
+        for (uint32_t v = 0; v < V; ++v) dn[v] = v < nvp ? (pdeg[v] | (uint32_t(pnn[v]) << 16)) : 0u;
+                #pragma unroll 1
+        for (uint32_t k = 0; k < R.n_lhs; ++k) {
+            const uint32_t e = rpos[k], a = pear[e], vo = pevo[e];
+                        #pragma unroll 1
+            for (uint32_t q = 0; q < a; ++q) {
+                const uint32_t v = vloc[vo + q];
+                dn[v] -= 1u + ((a - 1u) << 16);
+            }
+        }
+                #pragma unroll 1
+        for (uint32_t k = 0; k < R.n_rhs; ++k) {
+            const uint32_t a = R.rhs_ar[k], o = R.rhs_off[k];
+                        #pragma unroll 1
+            for (uint32_t q = 0; q < a; ++q) {
+                const uint32_t v = prodv[o + q];
+                dn[v] += 1u + ((a - 1u) << 16);
+            }
         }
     }
     uint32_t nv = 0, cap = 1, nocc = 0, nbr = 0, alive = 0;   // alive: vertices of degree > 0
         #pragma unroll 1
     for (uint32_t v = 0; v < V; ++v) {
-        const uint32_t d = dn[v] & 0xFFFFu, m = dn[v] >> 16;
+        const uint32_t d = A ? lane_bytesum(dn[v]) : dn[v] & 0xFFFFu;
+        const uint32_t m = A ? d * (A - 1u) : dn[v] >> 16;
         nv += d ? 1u : 0u;
         alive |= (d ? 1u : 0u) << v;
         cap = m > cap ? m : cap;
@@ -212,8 +238,21 @@ HGX_HD uint64_t lane_wl_core(const uint8_t* pear, const uint16_t* pevo, const ui
     uint64_t* cur = cura;   // this round's colours
     uint64_t* nxt = curb;   // the next round's (the two swap every round)
     // initial colours
+    if (A) {
+                #pragma unroll 1
+        for (uint32_t v = 0; v < V; ++v) {
+            const uint32_t c = dn[v];
+            uint64_t h = fnv(kFnvOffset, static_cast<uint64_t>(lane_bytesum(c)));
+                        #pragma unroll 1
+            for (uint32_t q = 0; q < A; ++q) {
+                                #pragma unroll 1
+                for (uint32_t j = (c >> (8 * q)) & 0xFFu; j; --j) h = fnv(fnv(h, A), q);
+            }
+            cur[v] = ((alive >> v) & 1u) ? h : 0;
+        }
+    }
         #pragma unroll 1
-    for (uint32_t v = 0; v < V; ++v) {
+    for (uint32_t v = 0; v < V && !A; ++v) {
         cur[v] = 0;
         if (!((alive >> v) & 1u)) continue;
         uint32_t n = 0;

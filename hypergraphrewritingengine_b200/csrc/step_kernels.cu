@@ -163,8 +163,10 @@ __device__ Parent load_parent(const DevPtrs& P, const Layout& L, char* sm, uint3
     pa.ne = P.st_ne[sid];
     pa.nocc = P.st_nocc[sid];
     pa.nvp = 0;
+    if (L.XI && lane == 0) *smp<uint32_t>(sm, L.o_xready) = 0;   // no join index yet
     if (pa.ne > L.NE || pa.nocc > L.NOCC) {
         if (lane == 0) atomicOr(P.err, kErrStateTooLarge);
+        __syncwarp();
         pa.ne = 0;
         pa.nocc = 0;
         return pa;
@@ -270,6 +272,154 @@ __device__ __forceinline__ void load_rule(char* sm, const Layout& L, const DevRu
 }
 
 // ------------------------------------------------------------------------------------------
+// Join indices of a staged state of more than kJoinIndexMin edges, built once per staging in the
+// warp's shared memory and used by every join over the state (all rules, all slices):
+//   * vertex index (the reference's InvertedVertexIndex, hypergraph/include/hypergraph/
+//     index.hpp:134-230): per local vertex, the state positions of the edges holding it, each
+//     edge once. A pattern edge with a bound variable draws its candidates from the bound vertex
+//     of smallest degree instead of from every edge.
+//   * signature index (SignatureIndex, index.hpp:30-130; signatures as in common/include/
+//     hgcommon/signature_core.hpp:24-84): the edges bucketed by arity and vertex-repetition
+//     pattern (nibble q = the first position holding the same vertex as position q). A pattern
+//     edge with no bound variable draws its candidates from the buckets whose edges repeat a
+//     vertex wherever the pattern repeats a variable. Built only when the state's edges fall in
+//     at most kSigBuckets signatures; edges of arity 16 share one bucket that is always searched.
+// Every candidate still passes the full test, so the indices only skip edges that would fail it.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t edge_signature(const uint16_t* v, uint32_t a) {
+    if (a >= 16) return ~1ull;                 // the unindexed bucket
+    uint64_t code = uint64_t(a) << 60;
+    for (uint32_t q = 1; q < a; ++q) {
+        uint32_t r = 0;
+        while (v[r] != v[q]) ++r;              // r <= q
+        code |= uint64_t(r) << (4 * q);
+    }
+    return code;
+}
+
+// Pattern edge (arity a, variables pv) against a bucket key: equal arity, and every position
+// whose variable repeats an earlier one holds the same vertex there.
+__device__ __forceinline__ bool signature_compatible(const uint8_t* pv, uint32_t a, uint64_t key) {
+    if (key == ~1ull) return a >= 16;
+    if ((key >> 60) != a) return false;
+    for (uint32_t q = 1; q < a; ++q) {
+        uint32_t r = 0;
+        while (pv[r] != pv[q]) ++r;
+        if (r != q && ((key >> (4 * q)) & 15u) != ((key >> (4 * r)) & 15u)) return false;
+    }
+    return true;
+}
+
+__device__ void build_join_index(const Layout& L, char* sm, const Parent& pa) {
+    if (!L.XI || pa.ne <= kJoinIndexMin) return;
+    const uint32_t lane = lane_id();
+    const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+    const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    uint32_t* xoff = smp<uint32_t>(sm, L.o_xoff);
+    uint16_t* xinc = smp<uint16_t>(sm, L.o_xinc);
+    uint64_t* bkey = smp<uint64_t>(sm, L.o_bkey);
+    uint32_t* boff = smp<uint32_t>(sm, L.o_boff);
+    uint16_t* blist = smp<uint16_t>(sm, L.o_blist);
+    uint32_t* misc = smp<uint32_t>(sm, L.o_misc);   // [0] bucket count (kSigBuckets+1 = overflow)
+    // vertex index: degrees (an edge counts once per distinct vertex), scan, fill
+    for (uint32_t v = lane; v <= pa.nvp; v += 32) xoff[v] = 0;
+    if (lane == 0) misc[0] = 0;
+    __syncwarp();
+    for (uint32_t e = lane; e < pa.ne; e += 32) {
+        const uint32_t a = pear[e], vo = pevo[e];
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t v = vloc[vo + q];
+            bool first = true;
+            for (uint32_t r = 0; r < q && first; ++r) first = vloc[vo + r] != v;
+            if (first) atomicAdd(&xoff[v + 1], 1u);
+        }
+    }
+    __syncwarp();
+    uint32_t run = 0;
+    for (uint32_t b = 0; b <= pa.nvp; b += 32) {
+        const uint32_t i = b + lane;
+        const uint32_t c = i <= pa.nvp ? xoff[i] : 0u;
+        const uint32_t inc = warp_incl_scan(c);
+        __syncwarp();
+        if (i <= pa.nvp) xoff[i] = run + inc;   // xoff[v + 1] = end of v's list
+        run += __shfl_sync(0xFFFFFFFFu, inc, 31);
+        __syncwarp();
+    }
+    // fill from each list's end backwards (the order inside a list does not matter: candidates
+    // are collected into a bitmask over state positions)
+    for (uint32_t e = lane; e < pa.ne; e += 32) {
+        const uint32_t a = pear[e], vo = pevo[e];
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t v = vloc[vo + q];
+            bool first = true;
+            for (uint32_t r = 0; r < q && first; ++r) first = vloc[vo + r] != v;
+            if (first) xinc[atomicSub(&xoff[v + 1], 1u) - 1u] = static_cast<uint16_t>(e);
+        }
+    }
+    __syncwarp();
+    // xoff[v + 1] now holds the start of v's list: shift back (xoff[nvp] = total)
+    for (uint32_t b = 0; b <= pa.nvp; b += 32) {
+        const uint32_t i = b + lane;
+        const uint32_t x = i + 1 <= pa.nvp ? xoff[i + 1] : run;
+        __syncwarp();
+        if (i <= pa.nvp) xoff[i] = i == 0 ? 0u : x;
+        __syncwarp();
+    }
+    // signature index: the distinct keys of each 32-edge chunk (match_any), appended to the
+    // bucket list one leader at a time; more than kSigBuckets keys leaves it unbuilt
+    for (uint32_t b = 0; b < pa.ne && misc[0] <= kSigBuckets; b += 32) {
+        const uint32_t e = b + lane;
+        const uint64_t key = e < pa.ne ? edge_signature(&vloc[pevo[e]], pear[e]) : ~0ull;
+        const uint32_t grp = __match_any_sync(0xFFFFFFFFu, key);
+        uint32_t leaders = __ballot_sync(0xFFFFFFFFu, e < pa.ne && (__ffs(grp) - 1) == static_cast<int>(lane));
+        while (leaders) {
+            const int l = __ffs(leaders) - 1;
+            leaders &= leaders - 1;
+            const uint64_t k = __shfl_sync(0xFFFFFFFFu, key, l);
+            const uint32_t nb = misc[0];
+            const bool hit = lane < min(nb, kSigBuckets) && bkey[lane] == k;
+            if (!__any_sync(0xFFFFFFFFu, hit) && lane == 0 && nb <= kSigBuckets) {
+                if (nb < kSigBuckets) bkey[nb] = k;
+                misc[0] = nb + 1;
+            }
+            __syncwarp();
+        }
+    }
+    const uint32_t nb = misc[0];
+    const bool sig = nb <= kSigBuckets;
+    if (sig) {
+        // bucket sizes, offsets, then the lists (each edge into its bucket)
+        for (uint32_t k = lane; k <= nb; k += 32) boff[k] = 0;
+        __syncwarp();
+        for (uint32_t e = lane; e < pa.ne; e += 32) {
+            const uint64_t key = edge_signature(&vloc[pevo[e]], pear[e]);
+            uint32_t k = 0;
+            while (k < nb && bkey[k] != key) ++k;
+            atomicAdd(&boff[k + 1], 1u);
+        }
+        __syncwarp();
+        if (lane == 0)
+            for (uint32_t k = 1; k <= nb; ++k) boff[k] += boff[k - 1];
+        __syncwarp();
+        for (uint32_t e = lane; e < pa.ne; e += 32) {
+            const uint64_t key = edge_signature(&vloc[pevo[e]], pear[e]);
+            uint32_t k = 0;
+            while (k < nb && bkey[k] != key) ++k;
+            blist[atomicSub(&boff[k + 1], 1u) - 1u] = static_cast<uint16_t>(e);
+        }
+        __syncwarp();
+        // boff[k + 1] now holds the start of bucket k: shift back
+        if (lane == 0) {
+            for (uint32_t k = 0; k < nb; ++k) boff[k] = boff[k + 1];
+            boff[nb] = pa.ne;
+        }
+    }
+    if (lane == 0) *smp<uint32_t>(sm, L.o_xready) = 1u | (sig ? 2u : 0u) | (nb << 8);
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------------------------------
 // The join. One warp holds one partial match; at every depth the 32 lanes test the state's
 // edges against the next pattern edge in parallel and a ballot compacts the survivors into a
 // candidate bitmask. Candidates are taken in ascending state position, so matches come out in
@@ -286,23 +436,67 @@ __device__ void compute_cands(const Layout& L, char* sm, const DevRule& R, uint3
     const uint32_t* taken = smp<uint32_t>(sm, L.o_taken);
     const uint32_t a = R.lhs_ar[p];
     const uint8_t* pv = &R.lhs_vars[R.lhs_off[p]];
-    for (uint32_t b = 0; b < pa.ne; b += 32) {
-        const uint32_t i = b + lane;
-        bool ok = false;
-        if (i < pa.ne && pear[i] == a && !((taken[i >> 5] >> (i & 31u)) & 1u)) {
-            ok = true;
-            const uint32_t vo = pevo[i];
-            for (uint32_t q = 0; q < a && ok; ++q) {
-                const uint32_t var = pv[q];
-                const uint32_t x = vloc[vo + q];
-                if ((mask >> var) & 1u) {
-                    ok = (bind[var] == x);
-                } else {
-                    for (uint32_t r = 0; r < q; ++r)
-                        if (pv[r] == var) { ok = (vloc[vo + r] == x); break; }
-                }
+    // state edge i can take pattern edge p under the current binding
+    auto ok_at = [&](uint32_t i) -> bool {
+        if (pear[i] != a || ((taken[i >> 5] >> (i & 31u)) & 1u)) return false;
+        const uint32_t vo = pevo[i];
+        bool ok = true;
+        for (uint32_t q = 0; q < a && ok; ++q) {
+            const uint32_t var = pv[q];
+            const uint32_t x = vloc[vo + q];
+            if ((mask >> var) & 1u) {
+                ok = (bind[var] == x);
+            } else {
+                for (uint32_t r = 0; r < q; ++r)
+                    if (pv[r] == var) { ok = (vloc[vo + r] == x); break; }
             }
         }
+        return ok;
+    };
+    const uint32_t xr = L.XI ? *smp<uint32_t>(sm, L.o_xready) : 0u;
+    if (xr) {
+        // indexed candidates: the edges of the bound vertex of smallest degree, else the edges of
+        // the signature buckets compatible with the pattern edge
+        const uint32_t* xoff = smp<uint32_t>(sm, L.o_xoff);
+        uint32_t best = 0xFFFFFFFFu, bx = 0;
+        for (uint32_t q = 0; q < a; ++q) {
+            const uint32_t var = pv[q];
+            if (!((mask >> var) & 1u)) continue;
+            const uint32_t x = bind[var];
+            const uint32_t deg = xoff[x + 1] - xoff[x];
+            if (deg < best) { best = deg; bx = x; }
+        }
+        const bool use_v = best != 0xFFFFFFFFu;
+        if (use_v || (xr & 2u)) {
+            const uint32_t nw = (pa.ne + 31) >> 5;
+            for (uint32_t w = lane; w < nw; w += 32) cand[w] = 0;
+            __syncwarp();
+            if (use_v) {
+                const uint16_t* list = smp<uint16_t>(sm, L.o_xinc) + xoff[bx];
+                for (uint32_t j = lane; j < best; j += 32) {
+                    const uint32_t i = list[j];
+                    if (ok_at(i)) atomicOr(&cand[i >> 5], 1u << (i & 31u));
+                }
+            } else {
+                const uint64_t* bkey = smp<uint64_t>(sm, L.o_bkey);
+                const uint32_t* boff = smp<uint32_t>(sm, L.o_boff);
+                const uint16_t* blist = smp<uint16_t>(sm, L.o_blist);
+                const uint32_t nb = xr >> 8;
+                for (uint32_t k = 0; k < nb; ++k) {
+                    if (!signature_compatible(pv, a, bkey[k])) continue;
+                    for (uint32_t j = boff[k] + lane; j < boff[k + 1]; j += 32) {
+                        const uint32_t i = blist[j];
+                        if (ok_at(i)) atomicOr(&cand[i >> 5], 1u << (i & 31u));
+                    }
+                }
+            }
+            __syncwarp();
+            return;
+        }
+    }
+    for (uint32_t b = 0; b < pa.ne; b += 32) {
+        const uint32_t i = b + lane;
+        const bool ok = i < pa.ne && ok_at(i);
         const uint32_t bal = __ballot_sync(0xFFFFFFFFu, ok);
         if (lane == 0) cand[b >> 5] = bal;
     }
@@ -993,8 +1187,14 @@ __device__ uint32_t build_parent_csr(const Layout& L, char* sm, const Parent& pa
     uint16_t* pnn = smp<uint16_t>(sm, L.o_pnn);
     uint16_t* pnoff = smp<uint16_t>(sm, L.o_pnoff);
     uint16_t* pnbr = smp<uint16_t>(sm, L.o_pnbr);
+    uint32_t* pcnt = smp<uint32_t>(sm, L.o_pcnt);
     const uint32_t v = lane;
     uint32_t d = 0, nn = 0, adj = 0;   // adj: vertices sharing an edge with v (nvp <= 32)
+    uint32_t cnt = 0;                  // occurrences of v by position (byte q, positions < 4)
+    const uint32_t a0 = pa.ne ? pear[0] : 0u;
+    bool uni = a0 >= 2 && a0 <= 4;     // every edge has arity a0 (lanes check their share)
+    for (uint32_t e = lane; e < pa.ne; e += 32) uni = uni && pear[e] == a0;
+    uni = __all_sync(0xFFFFFFFFu, uni);
     if (v < pa.nvp)
         for (uint32_t e = 0; e < pa.ne; ++e) {
             const uint32_t a = pear[e], vo = pevo[e];
@@ -1002,6 +1202,7 @@ __device__ uint32_t build_parent_csr(const Layout& L, char* sm, const Parent& pa
                 if (vloc[vo + q] == v) {
                     ++d;
                     nn += a - 1;
+                    cnt += q < 4 ? 1u << (8 * q) : 0u;
                     for (uint32_t k = 0; k < a; ++k) adj |= 1u << vloc[vo + k];
                 }
         }
@@ -1015,6 +1216,7 @@ __device__ uint32_t build_parent_csr(const Layout& L, char* sm, const Parent& pa
     const uint32_t inc = warp_incl_scan(d);
     const uint32_t incn = warp_incl_scan(nn);
     if (v < pa.nvp) {
+        pcnt[v] = cnt;
         poff[v] = static_cast<uint16_t>(inc - d);
         pdeg[v] = static_cast<uint16_t>(d);
         pnn[v] = static_cast<uint16_t>(nn);
@@ -1034,7 +1236,7 @@ __device__ uint32_t build_parent_csr(const Layout& L, char* sm, const Parent& pa
         poff[pa.nvp] = static_cast<uint16_t>(inc);
         pnoff[pa.nvp] = static_cast<uint16_t>(incn);
         const uint32_t all = pa.nvp >= 32 ? 0xFFFFFFFFu : (1u << pa.nvp) - 1u;
-        *smp<uint32_t>(sm, L.o_pconn) = (pa.nvp && reach == all) ? 1u : 0u;
+        *smp<uint32_t>(sm, L.o_pconn) = ((pa.nvp && reach == all) ? 1u : 0u) | ((uni ? a0 : 0u) << 8);
     }
     const uint32_t nnmax = warp_max32(nn);
     __syncwarp();
@@ -1048,8 +1250,8 @@ __device__ __forceinline__ uint64_t lane_wl(const Layout& L, char* sm, const Par
                                 smp<uint16_t>(sm, L.o_vloc), smp<uint16_t>(sm, L.o_poff),
                                 smp<uint16_t>(sm, L.o_pocc), smp<uint16_t>(sm, L.o_pdeg),
                                 smp<uint16_t>(sm, L.o_pnn), smp<uint16_t>(sm, L.o_pnoff),
-                                smp<uint16_t>(sm, L.o_pnbr), *smp<uint32_t>(sm, L.o_pconn) != 0,
-                                pa.ne, pa.nvp, R, slot, info);
+                                smp<uint16_t>(sm, L.o_pnbr), smp<uint32_t>(sm, L.o_pcnt),
+                                *smp<uint32_t>(sm, L.o_pconn), pa.ne, pa.nvp, R, slot, info);
 }
 
 }  // namespace
@@ -1100,6 +1302,7 @@ __global__ void k_count(DevPtrs P, LevelArgs A, Layout L) {
         if (f >= A.n_frontier) break;
         const uint32_t sid = A.frontier[f];
         const Parent pa = load_parent(P, L, sm, sid);
+        build_join_index(L, sm, pa);
         const DevEvo ev = P.evos[P.st_evo[sid]];
         // lane-per-child eligibility: few enough vertices and a bounded neighbour count
         bool lane_ok = pa.nvp <= kLaneVMax && pa.ne <= kLaneEMax && pa.ne > 0;
@@ -1254,6 +1457,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
         const DevEvo ev = P.evos[evo];
         if (lane == 0 && c_lo == 0) b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
         if (kLane) build_parent_csr(L, sm, pa);
+        else build_join_index(L, sm, pa);
         for (uint32_t r = 0; r < A.rules_stride && r < ev.rule_count; ++r) {
             const uint32_t item = f * A.rules_stride + r;
             if (lane == 0 && c_lo == 0) b_stage += 4ull * pa.ne + 4ull * pa.nocc;   // join: ids and vertices

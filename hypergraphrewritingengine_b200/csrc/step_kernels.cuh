@@ -136,13 +136,20 @@ struct Layout {
     uint32_t MCAP;      // matches the lane walk stages per (state, rule) (<= kLaneJoinCap)
     uint32_t region_bytes;   // lane layout without the trailing batch and match list (a warp's
                              // further parent regions need no batch or match list of their own)
-    uint32_t o_pconn;   // u32: 1 when the parent is connected
+    uint32_t o_pconn;   // u32: bit 0 = the parent is connected; bits 8.. = the arity every
+                        // parent edge has when it is 2..4 (else 0)
+    uint32_t o_pcnt;    // u32 per parent vertex: occurrences at position q in byte q (positions
+                        // 0..3; filled when the parent's edges have one arity)
     // match forwarding: seeded schedule, creating event's consumed edges, delta matches (and a
     // sorted copy), a 32-match chunk of forwarded matches
     uint32_t o_sched2, o_fkc, o_dkey, o_dpos, o_dkey2, o_dpos2, o_fkey, o_fpos;
     uint32_t SB;                                                    // bytes per batch slot
     uint32_t VT, o_vtab, o_vtid;   // vertex hash table for large states (VT slots, 0 = unused)
     uint32_t o_srt;                // warp WL: sort buffer of the distinct-colour count
+    // join indices of a staged state past kJoinIndexMin edges (XI = 1; count and warp layouts):
+    // vertex -> state positions of the edges holding it (CSR), and the edges bucketed by
+    // signature (at most kSigBuckets buckets); o_xready: bit 0 vertex index, bit 1 signature index
+    uint32_t XI, o_xready, o_xoff, o_xinc, o_bkey, o_boff, o_blist;
     uint32_t bytes;
 };
 

@@ -107,7 +107,14 @@ typedef enum hgx_option {
        of pushing the GPU to a real out-of-memory. Replaces EvolveInput::max_device_memory_bytes
        (gpu/include/hg_gpu/evolve.hpp:136-141), whose one-shot evolve stops at the limit with a
        kDeviceOutOfMemory warning; the hg_gpu shim maps the error to that warning. */
-    HGX_OPT_MAX_DEVICE_BYTES = 13
+    HGX_OPT_MAX_DEVICE_BYTES = 13,
+    /* Join indices for staged states of more than 64 edges: 1 (default) = candidates for a
+       pattern edge come from the bound vertex of smallest degree (the reference's
+       InvertedVertexIndex, hypergraph/include/hypergraph/index.hpp:134-230) or, with no bound
+       variable, from the signature buckets it is compatible with (SignatureIndex, index.hpp:30-130;
+       common/include/hgcommon/signature_core.hpp:24-84); 0 = every edge is tested. Results are
+       identical. */
+    HGX_OPT_JOIN_INDEX = 14
 } hgx_option;
 
 /* One evolution of a batch or a served request. */

@@ -16,7 +16,7 @@ int main(int argc, char** argv) {
     const int trials = argc > 1 ? atoi(argv[1]) : 20000;
     std::mt19937_64 rng(12345);
     auto U = [&](int lo, int hi) { return lo + int(rng() % uint64_t(hi - lo + 1)); };
-    int fails = 0, shortcut = 0;
+    int fails = 0, shortcut = 0, uniform = 0;
     for (int t = 0; t < trials; ++t) {
         // parent: ne edges of arity in [amin, amax] over nverts labels
         const int amin = U(1, 3), amax = amin + U(0, 2);
@@ -122,10 +122,23 @@ int main(int argc, char** argv) {
         for (int k = 0; k < R.n_lhs; ++k)
             for (int q = 0; q < pear[slot[k]]; ++q) covers = covers && inp[vloc[pevo[slot[k]] + q]];
         if (R.n_lhs > 0 && rroots == 1 && covers) R.flags |= kRuleRhsJoinsLhs;
+        // per-position occurrence counts and the uniform-arity flag, as the expand kernel stages
+        // them (an arity of 2..4 shared by every parent edge; the rule's RHS arity, if uniform)
+        std::vector<uint32_t> pcnt(nvp, 0);
+        for (int e = 0; e < ne; ++e)
+            for (int q = 0; q < pear[e] && q < 4; ++q) pcnt[vloc[pevo[e] + q]] += 1u << (8 * q);
+        uint32_t uni = pear[0];
+        for (int e = 0; e < ne; ++e) uni = pear[e] == uni ? uni : 0u;
+        if (uni < 2 || uni > 4) uni = 0;
+        R.rhs_uni = R.n_rhs ? R.rhs_ar[0] : 0;
+        for (int k = 0; k < R.n_rhs; ++k) R.rhs_uni = R.rhs_ar[k] == R.rhs_uni ? R.rhs_uni : 0;
+        uniform += (uni && uni == R.rhs_uni) ? 1 : 0;
+        const uint32_t pinfo = (pconn ? 1u : 0u) | (uni << 8);
         WlInfo info;
         const uint64_t got = lane_wl_core<32, 256>(pear.data(), pevo.data(), vloc.data(), poff.data(),
                                                    pocc.data(), pdeg.data(), pnn.data(), pnoff.data(),
-                                                   pnbr.data(), pconn, uint32_t(ne), nvp, R, slot.data(), info);
+                                                   pnbr.data(), pcnt.data(), pinfo, uint32_t(ne), nvp,
+                                                   R, slot.data(), info);
         const uint64_t want = hgx_oracle::wl_hash(child);
         shortcut += pconn && (R.flags & kRuleRhsJoinsLhs) ? 1 : 0;
         if (got != want) {
@@ -134,6 +147,7 @@ int main(int argc, char** argv) {
             ++fails;
         }
     }
-    std::printf("%d / %d mismatches (%d with the connectivity shortcut)\n", fails, trials, shortcut);
+    std::printf("%d / %d mismatches (%d with the connectivity shortcut, %d with uniform arity)\n",
+                fails, trials, shortcut, uniform);
     return fails ? 1 : 0;
 }

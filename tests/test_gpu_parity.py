@@ -250,3 +250,46 @@ def test_lane_join_variants_match_oracle(engine, join):
             assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} join={join}")
     finally:
         engine.set_option(api.OPT_LANE_JOIN, 0)
+
+
+def _large_state_cases():
+    """Evolutions whose states pass 64 edges (the join indices' range): served-workload draws
+    with large initial states (up to 256 edges, rules with repeated variables among them), a
+    100-edge hub, and two disconnected LHS edges (candidates from the signature buckets)."""
+    out = []
+    for t, ev in W.config5_stream(200, rate_per_s=1e9, seed=0xC0FFEE, max_states=400):
+        if ev.meta["n_edges"] > 64:
+            out.append(W.Evolution(rules=ev.rules, roots=ev.roots, steps=min(ev.steps, 3),
+                                   max_states=400, name=f"large-{ev.name}"))
+    out.append(W.Evolution(rules=[cases.C2_RULE], roots=[[[1, k] for k in range(2, 102)]], steps=2,
+                           max_states=3000, name="hub-100"))
+    out.append(W.Evolution(rules=[([[0, 0, 1], [2, 3, 3]], [[0, 1, 4], [2, 3, 4], [4, 4, 0]])],
+                           roots=[[[k % 23 + 1, k % 23 + 1, k % 7 + 30] if k % 3 == 0 else
+                                   [k % 11 + 1, k % 13 + 40, k % 13 + 40] for k in range(90)]],
+                           steps=2, max_states=2000, name="disconnected-lhs"))
+    return out
+
+
+@pytest.mark.parametrize("index", [1, 0])
+def test_join_index_modes_match_oracle(engine, index):
+    """The join with and without the vertex / signature indices (states past 64 edges) gives the
+    oracle's result, alone and in a batch, with and without match forwarding."""
+    from hypergraphrewritingengine_b200 import api
+    evs = _large_state_cases()
+    assert len(evs) >= 8
+    engine.set_option(api.OPT_JOIN_INDEX, index)
+    try:
+        for fwd in (0, 1):
+            engine.set_option(api.OPT_FORWARDING, fwd)
+            for ev, res in zip(evs, engine.evolve_batch(evs)):
+                ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+                assert res.truncated == ref["truncated"], ev.name
+                assert_same(norm_gpu(res), norm_oracle(ref), f"{ev.name} index={index} fwd={fwd}")
+        engine.set_option(api.OPT_FORWARDING, 0)
+        for ev in evs[-2:]:
+            res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            ref = pyoracle.evolve(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+            assert_same(norm_gpu(res), norm_oracle(ref), f"single {ev.name} index={index}")
+    finally:
+        engine.set_option(api.OPT_FORWARDING, 0)
+        engine.set_option(api.OPT_JOIN_INDEX, 1)

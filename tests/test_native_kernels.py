@@ -24,6 +24,8 @@ def test_lane_wl_matches_oracle(tmp_path):
     assert "0 / 20000 mismatches" in out.stdout
     # children hashed through the connectivity shortcut (connected parent, joining RHS)
     assert int(out.stdout.split("(")[1].split()[0]) > 1000, out.stdout
+    # children hashed through the uniform-arity initial colours (counts by position)
+    assert int(out.stdout.split(", ")[1].split()[0]) > 1000, out.stdout
 
 
 def _build_compat(tmp_path):
