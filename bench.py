@@ -29,8 +29,10 @@ rule and the initial state), generated in-process.
           (one evolution per call), same GPU, identical per-evolution outputs (key multisets).
 * served  a Poisson request stream served with continuous batching vs. one request per call.
 
-Multi-GPU: the path does not shard (one evolution per device); --gpus N runs N replicas under
-torchrun and reports the aggregate with the max-over-ranks time ("scaling": "weak").
+Multi-GPU: the single large evolution does not shard; --gpus N runs N replicas of it under
+torchrun and reports the aggregate with the max-over-ranks time ("scaling": "weak"). The batched
+workload does shard (independent evolutions, no exchange step): the line adds "sharded_batch",
+1024 random evolutions per rank split by shard.assign, max-over-ranks time.
 """
 from __future__ import annotations
 
@@ -349,6 +351,7 @@ def main():
         d2h = res.bytes()
         assert res.num_events == events and res.num_states == states
     e2e_t = max_over_ranks(dist, statistics.mean(e2e_s))
+    sharded = sharded_batch(eng, dist, world, rank, barrier) if world > 1 and not args.no_extras else None
 
     if rank != 0:
         if dist is not None:
@@ -386,6 +389,8 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
+    if sharded:
+        line["sharded_batch"] = sharded
     if world == 1:
         line["cpu_baseline"] = cpu_baseline_reference()
         if not args.no_extras:
@@ -472,6 +477,42 @@ def c3_forwarding(eng, stream, flush, reps=10):
     finally:
         eng.set_option(api.OPT_FORWARDING, 0)
     return out
+
+
+def sharded_batch(eng, dist, world, rank, barrier, per_rank=1024):
+    """The batched workload split over the ranks with no exchange step (weak scaling: 1024
+    random evolutions per rank, size-balanced by the engine's byte estimate, one engine per
+    GPU), counts read back; time = max over ranks of the batch's wall time."""
+    import torch
+    from hypergraphrewritingengine_b200 import api, shard
+    from hypergraphrewritingengine_b200 import workloads as W
+    evs = W.config4(n=per_rank * world)
+    idx, mine = shard.local_share(evs, rank, world)
+    jobs, keep = eng.make_jobs(mine)
+    out = (api.ctypes.c_void_p * max(len(mine), 1))()
+    eng.set_option(api.OPT_READBACK, 0)
+    try:
+        ts = []
+        for i in range(3):
+            barrier()
+            t0 = time.perf_counter()
+            if mine:
+                api._check(eng._L.hgx_evolve_batch(eng._h, jobs, len(mine), out))
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+            events = sum(int(eng._L.hgx_result_count(out[k], 1)) for k in range(len(mine)))
+            for k in range(len(mine)):
+                eng._L.hgx_result_free(out[k])
+    finally:
+        eng.set_option(api.OPT_READBACK, 1)
+    t = max_over_ranks(dist, min(ts[1:]))
+    tot = torch.tensor([float(events), float(len(mine))], dtype=torch.float64, device="cuda")
+    dist.all_reduce(tot)
+    return {"workload": f"c4 split over {world} ranks: {per_rank} random evolutions per rank "
+                        "(seed 0x5EED, cap 4096 states each), size-balanced by the byte estimate, "
+                        "no exchange step", "scaling": "weak", "evolutions": int(tot[1].item()),
+            "events": int(tot[0].item()), "ms_max_over_ranks": t * 1e3,
+            "events_per_s": tot[0].item() / t}
 
 
 def join_index_ab(eng, reps=3):

@@ -128,3 +128,18 @@ def test_gpu_backend_header_compiles_and_links(tmp_path):
                            "-L", os.path.dirname(build.LIB), "-lhgx",
                            "-Wl,-rpath," + os.path.dirname(build.LIB), "-o", str(exe)])
     assert exe.exists()
+
+
+@needs_gxx
+@pytest.mark.skipif(not HAVE_REF, reason="needs the reference tree (its hg_gpu_backend.hpp)")
+def test_drop_in_backend_file_compiles_against_the_reference_header(tmp_path):
+    """The replacement hg_gpu_backend.cpp shown in INTEGRATION.md, compiled against the
+    reference's own hg_gpu_backend.hpp (GpuJob, HostBridge, the run_gpu_evolution declaration)."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    m = re.search(r"```cpp\n(// paclet_source/hg_gpu_backend.cpp\n.*?)```", doc, re.S)
+    assert m, "INTEGRATION.md lost the drop-in file"
+    src = tmp_path / "hg_gpu_backend.cpp"
+    src.write_text(m.group(1))
+    subprocess.check_call(["g++", "-std=c++17", "-O1", "-c", "-DHG_GPU_BACKEND=1",
+                           "-I", os.path.join(REF, "paclet_source"), "-I", os.path.join(ROOT, "include"),
+                           str(src), "-o", str(tmp_path / "hg_gpu_backend.o")])
