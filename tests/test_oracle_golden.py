@@ -130,3 +130,23 @@ def test_state_cap_truncates_at_first_excess_event():
     # the capped run is a prefix of the uncapped one in canonical event order
     n = len(capped["events"])
     assert np.array_equal(capped["events"][:, 2:], full["events"][:n, 2:])
+
+
+def _corpus():
+    import json
+    import os
+    p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden_corpus.json")
+    return json.load(open(p))["cases"]
+
+
+def test_oracle_matches_reference_golden_corpus():
+    """The reference's shared engine corpus (reference/golden_corpus.wl, 12 MultiwaySystem cases
+    in full multiway): classes, raw events, causal pairs of the transitively reduced relation and
+    branchial pairs, all equal (WL classes coincide with the IR classes on every case)."""
+    import numpy as np
+    for c in _corpus():
+        r = pyoracle.evolve(c["rules"], [c["init"]], c["steps"], quotient=False, tr=True)
+        got = {"states": len(np.unique(r["state_hash"])), "raw_events": len(r["events"]),
+               "causal": len({(int(a), int(b)) for a, b, _ in r["causal"]}),
+               "branchial": len(r["branchial"])}
+        assert got == c["expected"], c["name"]
