@@ -58,7 +58,7 @@ EXPORTS = (
     "hgx_result_count",
     "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
     "hgx_engine_stream", "hgx_hash_states_noalloc", "hgx_result_view",
-    "hgx_estimate_device_bytes", "hgx_device_memory",
+    "hgx_estimate_device_bytes", "hgx_device_memory", "hgx_result_views",
 )
 
 
@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH):
                                      ctypes.c_uint32, vp, vp, vp], ctypes.c_int),
         "hgx_estimate_device_bytes": ([ctypes.POINTER(Job), u64p], ctypes.c_int),
         "hgx_device_memory": ([ctypes.c_int, u64p, u64p], ctypes.c_int),
+        "hgx_result_views": ([vp, ctypes.POINTER(vp), u64p], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -283,16 +284,16 @@ def _read_result(handle) -> EvolveResult:
     owner = _ResultOwner(handle)
     cnt = lambda w: int(L.hgx_result_count(handle, w))  # noqa: E731
     arrays = {}
+    ptrs = (ctypes.c_void_p * 14)()
+    counts = (ctypes.c_uint64 * 14)()
+    _check(L.hgx_result_views(handle, ptrs, counts))
     for what in range(14):
-        ptr = ctypes.c_void_p()
-        n = ctypes.c_uint64()
-        _check(L.hgx_result_view(handle, what, ctypes.byref(ptr), ctypes.byref(n)))
         dt = _ARR_TYPES.get(what, np.uint32)
-        n = int(n.value)
-        if n == 0 or not ptr.value:
+        n, p = int(counts[what]), ptrs[what]
+        if n == 0 or not p:
             a = np.zeros(0, dt)
         else:
-            buf = (ctypes.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr.value)
+            buf = (ctypes.c_char * (n * np.dtype(dt).itemsize)).from_address(p)
             buf._owner = owner
             a = np.frombuffer(buf, dtype=dt)
         w = _ARR_SHAPES.get(what)

@@ -429,6 +429,15 @@ hgx_status hgx_result_view(const hgx_result* res, hgx_array what, const void** p
     return HGX_OK;
 }
 
+hgx_status hgx_result_views(const hgx_result* res, const void** ptrs, uint64_t* counts) {
+    if (!res || !ptrs || !counts) return fail(HGX_ERR_INVALID, "null argument");
+    for (int i = 0; i < hgx::ResultArrays::kArrays; ++i) {
+        ptrs[i] = res->ptr[i];
+        counts[i] = res->count[i];
+    }
+    return HGX_OK;
+}
+
 void hgx_result_free(hgx_result* r) { delete r; }
 
 hgx_status hgx_engine_stage_times(hgx_engine* e, double* out, uint64_t* launches) {

@@ -273,40 +273,107 @@ struct LaunchShape {
     uint32_t grid, block, smem;
 };
 
-// Page-locked host blocks for results, recycled when a result is freed. Shared with the results
-// it hands out, so a result may outlive the engine that produced it.
+// Page-locked host memory for results, recycled when a result is freed. Shared with the results
+// it hands out, so a result may outlive the engine that produced it. Page-locking is slow (a
+// cudaHostAlloc costs far more than the copy it serves), so memory is kept rather than returned:
+//   * a result of at most kSmall bytes is carved from a kSlab slab (16-byte aligned, bump
+//     pointer); a slab whose results are all freed is reset and reused;
+//   * a larger result gets its own power-of-two block; freed blocks are kept (best fit on reuse)
+//     up to kKeepBytes in total, the smallest returned to the system beyond that.
 struct PinnedPool {
+    static constexpr size_t kSmall = 4u << 20, kSlab = 32u << 20;
+    static constexpr size_t kKeepBytes = size_t(2) << 30;
+    struct Slab {
+        uint8_t* base = nullptr;
+        size_t top = 0;
+        uint32_t live = 0;
+    };
     std::mutex mu;
+    std::vector<Slab*> slabs;          // every slab (owned)
+    Slab* cur = nullptr;               // the slab small results are carved from
     std::vector<std::pair<size_t, void*>> free_blocks;
+    size_t free_bytes = 0;
+
     ~PinnedPool() {
         for (auto& b : free_blocks) cudaFreeHost(b.second);
+        for (Slab* sl : slabs) {
+            cudaFreeHost(sl->base);
+            delete sl;
+        }
     }
-    void* get(size_t bytes, size_t& cap) {
+
+    // `bytes` of page-locked memory; the returned owner releases it (the pool outlives it).
+    static std::shared_ptr<void> acquire(const std::shared_ptr<PinnedPool>& pool, size_t bytes,
+                                         uint8_t** out) {
+        bytes = std::max<size_t>((bytes + 15) / 16 * 16, 16);
+        PinnedPool& P = *pool;
+        if (bytes <= kSmall) {
+            Slab* sl = nullptr;
+            size_t at = 0;
+            {
+                std::lock_guard<std::mutex> lock(P.mu);
+                if (!P.cur || P.cur->top + bytes > kSlab) {
+                    P.cur = nullptr;
+                    for (Slab* c : P.slabs)
+                        if (c->live == 0) { c->top = 0; P.cur = c; break; }
+                }
+                if (P.cur) {
+                    sl = P.cur;
+                    at = sl->top;
+                    sl->top += bytes;
+                    ++sl->live;
+                }
+            }
+            if (!sl) {   // a new slab (allocated outside the lock)
+                void* b = nullptr;
+                HGX_CUDA_CHECK(cudaHostAlloc(&b, kSlab, cudaHostAllocDefault));
+                std::lock_guard<std::mutex> lock(P.mu);
+                sl = new Slab;
+                sl->base = static_cast<uint8_t*>(b);
+                sl->top = bytes;
+                sl->live = 1;
+                P.slabs.push_back(sl);
+                P.cur = sl;
+                at = 0;
+            }
+            *out = sl->base + at;
+            return std::shared_ptr<void>(*out, [pool, sl](void*) {
+                std::lock_guard<std::mutex> lock(pool->mu);
+                --sl->live;
+            });
+        }
+        size_t cap = 0;
+        void* p = nullptr;
         {
-            std::lock_guard<std::mutex> lock(mu);
-            size_t best = free_blocks.size();
-            for (size_t i = 0; i < free_blocks.size(); ++i)
-                if (free_blocks[i].first >= bytes &&
-                    (best == free_blocks.size() || free_blocks[i].first < free_blocks[best].first))
+            std::lock_guard<std::mutex> lock(P.mu);
+            size_t best = P.free_blocks.size();
+            for (size_t i = 0; i < P.free_blocks.size(); ++i)
+                if (P.free_blocks[i].first >= bytes &&
+                    (best == P.free_blocks.size() || P.free_blocks[i].first < P.free_blocks[best].first))
                     best = i;
-            if (best != free_blocks.size()) {
-                auto b = free_blocks[best];
-                free_blocks.erase(free_blocks.begin() + best);
-                cap = b.first;
-                return b.second;
+            if (best != P.free_blocks.size()) {
+                cap = P.free_blocks[best].first;
+                p = P.free_blocks[best].second;
+                P.free_bytes -= cap;
+                P.free_blocks.erase(P.free_blocks.begin() + best);
             }
         }
-        cap = 1 << 20;
-        while (cap < bytes) cap <<= 1;
-        void* p = nullptr;
-        HGX_CUDA_CHECK(cudaHostAlloc(&p, cap, cudaHostAllocDefault));
-        return p;
+        if (!p) {
+            cap = kSmall * 2;
+            while (cap < bytes) cap <<= 1;
+            HGX_CUDA_CHECK(cudaHostAlloc(&p, cap, cudaHostAllocDefault));
+        }
+        *out = static_cast<uint8_t*>(p);
+        return std::shared_ptr<void>(p, [pool, cap](void* q) { pool->put(q, cap); });
     }
+
     void put(void* p, size_t cap) {
         std::lock_guard<std::mutex> lock(mu);
         free_blocks.emplace_back(cap, p);
-        if (free_blocks.size() > 4) {   // keep a few blocks; return the smallest to the system
+        free_bytes += cap;
+        while (free_bytes > kKeepBytes && !free_blocks.empty()) {   // return the smallest
             auto it = std::min_element(free_blocks.begin(), free_blocks.end());
+            free_bytes -= it->first;
             cudaFreeHost(it->second);
             free_blocks.erase(it);
         }
@@ -997,11 +1064,9 @@ struct Engine::Impl {
             HGX_CUDA_CHECK(cudaMemsetAsync(dp(8), 0, 4, st));
             HGX_CUDA_CHECK(cudaMemsetAsync(dp(11), 0, 4, st));
         }
-        size_t cap = 0;
-        uint8_t* h = static_cast<uint8_t*>(pinned->get(total, cap));
-        auto pool = pinned;
+        uint8_t* h = nullptr;
         auto flat = std::make_shared<ResultArrays>();
-        flat->owner = std::shared_ptr<void>(h, [pool, cap](void* p) { pool->put(p, cap); });
+        flat->owner = PinnedPool::acquire(pinned, total, &h);
         auto d2h_from = [&](int i, const void* src) {
             const size_t bytes = count[i] * arr_elem_bytes(i);
             if (bytes) HGX_CUDA_CHECK(cudaMemcpyAsync(h + off[i], src, bytes, cudaMemcpyDeviceToHost, st));
@@ -1194,10 +1259,8 @@ struct Engine::Impl {
                                                                 map_e.p, stage, d_sec);
             check_launch();
         }
-        size_t cap = 0;
-        uint8_t* h = static_cast<uint8_t*>(pinned->get(std::max<uint64_t>(total, 16), cap));
-        auto pool = pinned;
-        std::shared_ptr<void> owner(h, [pool, cap](void* p) { pool->put(p, cap); });
+        uint8_t* h = nullptr;
+        std::shared_ptr<void> owner = PinnedPool::acquire(pinned, std::max<uint64_t>(total, 16), &h);
         if (total) HGX_CUDA_CHECK(cudaMemcpyAsync(h, stage, total, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         for (uint32_t k = 0; k < K; ++k) {
@@ -1807,7 +1870,13 @@ struct Engine::Impl {
                 }
             }
             if (n_new) {
-                k_materialize<<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
+                // lanes per state: the level's largest parent in one pass
+                if (fmax_ne <= 8)
+                    k_materialize<8><<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
+                else if (fmax_ne <= 16)
+                    k_materialize<16><<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
+                else
+                    k_materialize<32><<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
                 check_launch();
             }
             toc(times.materialize);

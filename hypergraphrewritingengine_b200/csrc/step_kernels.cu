@@ -596,7 +596,8 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
 // ------------------------------------------------------------------------------------------
 template <class F>
 __device__ uint32_t lane_walk(const Layout& L, const char* sm, const DevRule& R, const Parent& pa,
-                              uint32_t e0, F&& on_match) {
+                              uint32_t e0, F&& on_match, uint32_t j1_lo = 0,
+                              uint32_t j1_hi = 0xFFFFFFFFu) {
     const uint8_t* pear = smp<uint8_t>(const_cast<char*>(sm), L.o_pear);
     const uint16_t* pevo = smp<uint16_t>(const_cast<char*>(sm), L.o_pevo);
     const uint16_t* vloc = smp<uint16_t>(const_cast<char*>(sm), L.o_vloc);
@@ -647,7 +648,9 @@ __device__ uint32_t lane_walk(const Layout& L, const char* sm, const DevRule& R,
             continue;
         }
         bool ok = false;
-        for (; j < pa.ne; ++j)
+        const uint32_t jend = d == 1 ? min(pa.ne, j1_hi) : pa.ne;
+        if (d == 1 && j < j1_lo) j = j1_lo;
+        for (; j < jend; ++j)
             if (!((used >> j) & 1ull) && try_bind(d, j)) { ok = true; break; }
         if (ok) {
             pick[d] = j;
@@ -665,12 +668,22 @@ __device__ uint32_t lane_walk(const Layout& L, const char* sm, const DevRule& R,
     return found;
 }
 
-// Matches of (state, rule) by lane walks over every first edge, warp total.
+// Matches of (state, rule) by lane walks over every first edge, warp total. A state of at most 16
+// (8) edges gives each first edge 2 (4) lanes, which split the second position's candidates.
 __device__ uint32_t lane_join_count(const Layout& L, const char* sm, const DevRule& R,
                                     const Parent& pa) {
     uint32_t c = 0;
+    const uint32_t lane = lane_id();
+    const uint32_t parts = (R.n_lhs < 2 || pa.ne > 16) ? 1u : (pa.ne <= 8 ? 4u : 2u);
+    if (parts > 1) {
+        const uint32_t e0 = lane / parts, part = lane % parts;
+        const uint32_t span = (pa.ne + parts - 1) / parts;
+        if (e0 < pa.ne)
+            c = lane_walk(L, sm, R, pa, e0, [](uint32_t) {}, part * span, (part + 1) * span);
+        return warp_sum32(c);
+    }
     for (uint32_t b = 0; b < pa.ne; b += 32)
-        if (b + lane_id() < pa.ne) c += lane_walk(L, sm, R, pa, b + lane_id(), [](uint32_t) {});
+        if (b + lane < pa.ne) c += lane_walk(L, sm, R, pa, b + lane, [](uint32_t) {});
     return warp_sum32(c);
 }
 
@@ -2412,21 +2425,40 @@ __global__ void k_evsig(DevPtrs P, LevelArgs A, int pass) {
     }
 }
 
+// Inclusive scan inside segments of S lanes (S = 32: the whole warp).
+template <uint32_t S>
+__device__ __forceinline__ uint32_t seg_incl_scan(uint32_t x) {
+#pragma unroll
+    for (uint32_t d = 1; d < S; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d, S);
+        if ((lane_id() & (S - 1)) >= d) x += y;
+    }
+    return x;
+}
+
 // Write the edge record of every new state: parent edges minus consumed, then produced.
+// Groups of 32 new states per warp share one arena reservation and one level-maximum update;
+// the group's states are then written 32 / S at a time, one per segment of S lanes (lanes =
+// parent edges), S chosen on the host from the level's largest parent (8, 16 or 32 edges per
+// pass), so a small parent does not leave most of the warp idle.
+template <uint32_t S>
 __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
-    __shared__ uint32_t bind_sm[8][kMaxVars];
-    __shared__ uint32_t cons_sm[8][kMaxPatternEdges];
+    constexpr uint32_t G = 32 / S;
+    __shared__ uint32_t bind_sm[8][G][kMaxVars];
+    __shared__ uint32_t cons_sm[8][G][kMaxPatternEdges];
     const uint32_t lane = lane_id();
     const uint32_t w = threadIdx.x >> 5;
-    uint32_t* bind = bind_sm[w];
-    uint32_t* cons = cons_sm[w];
+    const uint32_t seg = lane / S, sl = lane & (S - 1);
+    const uint32_t segbits = S == 32 ? 0xFFFFFFFFu : ((1u << S) - 1u);
+    uint32_t* bind = bind_sm[w][seg];
+    uint32_t* cons = cons_sm[w][seg];
     // groups of 32 new states per warp: record sizes by lane, one arena reservation per group
     for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g * 32ull < n_new;
          g += (gridDim.x * blockDim.x) >> 5) {
         const uint32_t jl = g * 32 + lane;
         uint32_t words = 0, gne = 0, gnocc = 0;
-        // lane k loads state k's event, parent and rule once; the serial loop below takes them
-        // by shuffle instead of repeating the chain of dependent loads per state
+        // lane k loads state k's event, parent and rule once; the loop below takes them by
+        // shuffle instead of repeating the chain of dependent loads per state
         uint32_t e_l = 0, f_l = 0, r_l = 0, pne_l = 0, pnocc_l = 0, coff_l = 0, pid_l = 0, fid_l = 0;
         unsigned long long poff_l = 0;
         if (jl < n_new) {
@@ -2461,29 +2493,42 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
         }
         const unsigned long long my_off = base + inc - words;
         const uint32_t cnt = min(32u, n_new - g * 32);
-        for (uint32_t k = 0; k < cnt; ++k) {
+        for (uint32_t k0 = 0; k0 < cnt; k0 += G) {
+            const uint32_t k = k0 + seg;               // this segment's state in the group
+            const bool act = k < cnt;
+            const uint32_t src = act ? k : 0u;
             const uint32_t j = g * 32 + k;
-            const unsigned long long off = __shfl_sync(0xFFFFFFFFu, my_off, k);
+            const unsigned long long off = __shfl_sync(0xFFFFFFFFu, my_off, src);
             const uint32_t sid = A.state_base + j;
-            const DevRule& R = P.rules[__shfl_sync(0xFFFFFFFFu, r_l, k)];
-            const uint32_t pne = __shfl_sync(0xFFFFFFFFu, pne_l, k);
-            const uint32_t pnocc = __shfl_sync(0xFFFFFFFFu, pnocc_l, k);
-            const uint32_t coff = __shfl_sync(0xFFFFFFFFu, coff_l, k);
-            const uint32_t* prec = P.arena + __shfl_sync(0xFFFFFFFFu, poff_l, k);
+            const DevRule& R = P.rules[__shfl_sync(0xFFFFFFFFu, r_l, src)];
+            // every lane takes part in every shuffle (a full-mask shuffle that some lanes skip
+            // never completes); inactive segments then zero what they took
+            const uint32_t pne_s = __shfl_sync(0xFFFFFFFFu, pne_l, src);
+            const uint32_t pne = act ? pne_s : 0u;
+            const uint32_t pnocc = __shfl_sync(0xFFFFFFFFu, pnocc_l, src);
+            const uint32_t coff = __shfl_sync(0xFFFFFFFFu, coff_l, src);
+            const uint32_t* prec = P.arena + __shfl_sync(0xFFFFFFFFu, poff_l, src);
+            const uint32_t pid = __shfl_sync(0xFFFFFFFFu, pid_l, src);
+            const uint32_t fid = __shfl_sync(0xFFFFFFFFu, fid_l, src);
             const uint32_t paw = (pne + 3) >> 2;
-            const uint32_t ne = pne - R.n_lhs + R.n_rhs;
-            const uint32_t nocc = pnocc - R.lhs_total + R.rhs_total;
+            const uint32_t ne = act ? pne - R.n_lhs + R.n_rhs : 0u;
+            const uint32_t nocc = act ? pnocc - R.lhs_total + R.rhs_total : 0u;
             const uint32_t aw = (ne + 3) >> 2;
             uint32_t* rec = P.arena + off;
             uint8_t* rar = reinterpret_cast<uint8_t*>(rec + ne);
             uint32_t* rv = rec + ne + aw;
-            if (lane < R.n_lhs) cons[lane] = P.ev_cons[coff + lane];
-            for (uint32_t t = lane; t < aw; t += 32) rec[ne + t] = 0;   // arity padding bytes
+            if (act)
+                for (uint32_t t = sl; t < R.n_lhs; t += S) cons[t] = P.ev_cons[coff + t];
+            if (act)
+                for (uint32_t t = sl; t < aw; t += S) rec[ne + t] = 0;   // arity padding bytes
             __syncwarp();
             // kept parent edges; a consumed edge binds its pattern edge's variables instead
+            uint32_t pne_max = pne;
+#pragma unroll
+            for (uint32_t d = S; d < 32; d <<= 1) pne_max = max(pne_max, __shfl_xor_sync(0xFFFFFFFFu, pne_max, d));
             uint32_t run_e = 0, run_pv = 0, run_cv = 0;
-            for (uint32_t b = 0; b < pne; b += 32) {
-                const uint32_t i = b + lane;
+            for (uint32_t b = 0; b < pne_max; b += S) {
+                const uint32_t i = b + sl;
                 uint32_t id = 0, a = 0, hit = kNone;
                 if (i < pne) {
                     id = prec[i];
@@ -2492,41 +2537,41 @@ __global__ void k_materialize(DevPtrs P, LevelArgs A, uint32_t n_new) {
                         if (cons[k2] == id) hit = k2;
                 }
                 const bool keep = i < pne && hit == kNone;
-                const uint32_t pinc = warp_incl_scan(a);
+                const uint32_t pinc = seg_incl_scan<S>(a);
                 const uint32_t ka = keep ? a : 0u;
-                const uint32_t kinc = warp_incl_scan(ka);
-                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, keep);
-                const uint32_t src = run_pv + pinc - a;
+                const uint32_t kinc = seg_incl_scan<S>(ka);
+                const uint32_t bal = (__ballot_sync(0xFFFFFFFFu, keep) >> (seg * S)) & segbits;
+                const uint32_t sv = run_pv + pinc - a;
                 if (keep) {
-                    const uint32_t c = run_e + __popc(bal & ((1u << lane) - 1u));
+                    const uint32_t c = run_e + __popc(bal & ((1u << sl) - 1u));
                     rec[c] = id;
                     rar[c] = static_cast<uint8_t>(a);
                     const uint32_t dst = run_cv + kinc - ka;
-                    for (uint32_t q = 0; q < a; ++q) rv[dst + q] = prec[pne + paw + src + q];
+                    for (uint32_t q = 0; q < a; ++q) rv[dst + q] = prec[pne + paw + sv + q];
                 } else if (hit != kNone) {
                     for (uint32_t q = 0; q < a; ++q)
-                        bind[R.lhs_vars[R.lhs_off[hit] + q]] = prec[pne + paw + src + q];
+                        bind[R.lhs_vars[R.lhs_off[hit] + q]] = prec[pne + paw + sv + q];
                 }
                 run_e += __popc(bal);
-                run_pv += __shfl_sync(0xFFFFFFFFu, pinc, 31);
-                run_cv += __shfl_sync(0xFFFFFFFFu, kinc, 31);
+                run_pv += __shfl_sync(0xFFFFFFFFu, pinc, S - 1, S);
+                run_cv += __shfl_sync(0xFFFFFFFFu, kinc, S - 1, S);
             }
             __syncwarp();
             // produced edges
-            const uint32_t pid = __shfl_sync(0xFFFFFFFFu, pid_l, k);
-            const uint32_t fid = __shfl_sync(0xFFFFFFFFu, fid_l, k);
-            for (uint32_t k2 = lane; k2 < R.n_rhs; k2 += 32) {
-                rec[run_e + k2] = pid + k2;
-                rar[run_e + k2] = R.rhs_ar[k2];
-            }
-            for (uint32_t t = lane; t < R.rhs_total; t += 32) {
-                const uint32_t var = R.rhs_vars[t];
-                rv[run_cv + t] = ((R.new_mask >> var) & 1u) ? fid + R.fresh_rank[var] : bind[var];
-            }
-            if (lane == 0) {
-                P.st_off[sid] = off;
-                P.st_ne[sid] = ne;
-                P.st_nocc[sid] = nocc;
+            if (act) {
+                for (uint32_t k2 = sl; k2 < R.n_rhs; k2 += S) {
+                    rec[run_e + k2] = pid + k2;
+                    rar[run_e + k2] = R.rhs_ar[k2];
+                }
+                for (uint32_t t = sl; t < R.rhs_total; t += S) {
+                    const uint32_t var = R.rhs_vars[t];
+                    rv[run_cv + t] = ((R.new_mask >> var) & 1u) ? fid + R.fresh_rank[var] : bind[var];
+                }
+                if (sl == 0) {
+                    P.st_off[sid] = off;
+                    P.st_ne[sid] = ne;
+                    P.st_nocc[sid] = nocc;
+                }
             }
             __syncwarp();
         }

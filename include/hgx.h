@@ -238,6 +238,9 @@ HGX_API void hgx_result_free(hgx_result* result);
    single-evolution result), *count is its element count; valid until hgx_result_free. */
 HGX_API hgx_status hgx_result_view(const hgx_result* result, hgx_array what, const void** ptr,
                                    uint64_t* count);
+/* Every array at once: ptrs[a] / counts[a] for each hgx_array a (14 entries each), as
+   hgx_result_view gives them one by one. */
+HGX_API hgx_status hgx_result_views(const hgx_result* result, const void** ptrs, uint64_t* counts);
 
 /* Device time per stage of the last evolve call, in milliseconds (HGX_OPT_TIMING must be on):
    out[0..7] = count, scan, expand, select, materialize, branchial, roots, total.
