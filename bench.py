@@ -612,7 +612,7 @@ def batched_vs_plain(eng, n=1024, max_states=4096):
                                           "key multisets of every evolution"}
 
 
-def served_vs_plain(eng, n=400, rates=(100.0, 1000.0, float("inf"))):
+def served_vs_plain(eng, n=400, rates=(100.0, 1000.0, 3000.0, 10000.0, float("inf"))):
     """Poisson stream of random evolve requests (initial edges lognormal, median 16, max 256;
     2-8 steps; WL quotient, cap 4096 states), served with continuous batching vs. one request per
     call in arrival order, at arrival rates up to saturation (inf = all requests at t=0)."""
