@@ -334,7 +334,10 @@ def main():
     states = counts["states"]
     value = world * events / (t_ms / 1e3)
 
-    # ---- e2e through the C-ABI with host buffers
+    # ---- e2e through the C-ABI with host buffers; the result is what the reference's
+    # hg_gpu::evolve returns by default (edge_identity false: state edge contents without their
+    # global edge ids)
+    eng.set_option(_api.OPT_KEEP_STATE_EDGE_IDS, 0)
     rb, sb = encode_rules(ev.rules), encode_roots(ev.roots)
     h2d = rb.nbytes + sb.nbytes
     e2e_s = []
@@ -351,6 +354,7 @@ def main():
         d2h = res.bytes()
         assert res.num_events == events and res.num_states == states
     e2e_t = max_over_ranks(dist, statistics.mean(e2e_s))
+    eng.set_option(_api.OPT_KEEP_STATE_EDGE_IDS, 1)
     sharded = sharded_batch(eng, dist, world, rank, barrier) if world > 1 and not args.no_extras else None
 
     if rank != 0:
@@ -375,7 +379,11 @@ def main():
                    "branchial_per_step": counts["branchial"], "truncated_at_cap": counts["truncated"]},
         "unique_states_per_s": world * states / (t_ms / 1e3),
         "e2e": {"value": world * events / e2e_t, "unit": "events/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3},
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t * 1e3,
+                "result": "every state (WL hash, depth, edge arities and vertices), every event "
+                          "(in, out, rule, step, consumed and produced edges), causal triples, "
+                          "branchial pairs; state edge ids left out as in hg_gpu::EvolveResult "
+                          "by default (EvolveInput::edge_identity false)"},
         "roofline": {"bound": "hbm", "kernel": "k_expand_lanes2 (lane expand)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                      "traffic": traffic, "peak_kind": f"{peak_kind} (copy bandwidth)",

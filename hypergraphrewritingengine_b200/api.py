@@ -35,7 +35,7 @@ HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_
 (OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
  OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING, OPT_CHUNK_MIN,
  OPT_EVENT_SIGNATURE_KEYS, OPT_LANE_JOIN, OPT_LEVEL_SPLIT, OPT_MAX_DEVICE_BYTES,
- OPT_JOIN_INDEX) = range(15)
+ OPT_JOIN_INDEX, OPT_KEEP_STATE_EDGE_IDS) = range(16)
 (COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
  COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES,
  COUNT_CANONICAL_EVENTS) = range(11)

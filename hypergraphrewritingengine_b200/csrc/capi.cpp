@@ -234,6 +234,7 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
         case HGX_OPT_LEVEL_SPLIT: e->opt.level_split = value; return HGX_OK;
         case HGX_OPT_MAX_DEVICE_BYTES: e->engine.set_device_limit(value); return HGX_OK;
         case HGX_OPT_JOIN_INDEX: e->opt.join_index = value != 0; return HGX_OK;
+        case HGX_OPT_KEEP_STATE_EDGE_IDS: e->opt.keep_state_edge_ids = value != 0; return HGX_OK;
         case HGX_OPT_LANE_JOIN:
             if (value > 2) return fail(HGX_ERR_INVALID, "lane join must be 0 (autotuned), 1 or 2");
             e->opt.lane_join = static_cast<uint32_t>(value);
@@ -402,7 +403,7 @@ uint64_t hgx_result_count(const hgx_result* res, hgx_count what) {
         case HGX_COUNT_BRANCHIAL: return res->count[HGX_ARR_BRANCHIAL] / 2;
         case HGX_COUNT_TRUNCATED: return r.truncated ? 1 : 0;
         case HGX_COUNT_CONSUMED: return res->count[HGX_ARR_EVENT_CONS];
-        case HGX_COUNT_STATE_EDGES: return res->count[HGX_ARR_STATE_EDGE_IDS];
+        case HGX_COUNT_STATE_EDGES: return res->count[HGX_ARR_STATE_ARITY];
         case HGX_COUNT_STATE_VERTS: return res->count[HGX_ARR_STATE_VERTS];
         case HGX_COUNT_RAW_STATES: return r.n_roots + res->count[HGX_ARR_EVENTS] / 4;
         case HGX_COUNT_CANONICAL_EVENTS: return r.n_canonical_events;

@@ -1024,11 +1024,12 @@ struct Engine::Impl {
         HGX_CUDA_CHECK(cudaStreamSynchronize(st));
         const uint32_t C = E ? clast + h_rules[rlast].n_lhs - c0 : 0;
         const bool se = opt.keep_state_edges;
+        const bool si = se && opt.keep_state_edge_ids;
         // host block layout (hgx_array order), 16-byte aligned sections
         const bool sg = opt.event_keys != 0;
         uint64_t count[ResultArrays::kArrays] = {
             S, S, 4ull * E, 3ull * K, 2 * B, uint64_t(E) + 1, C, 2ull * E,
-            se ? S + 1ull : 1, se ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0, sg ? E : 0};
+            se ? S + 1ull : 1, si ? T : 0, se ? T : 0, se ? S + 1ull : 1, se ? V : 0, sg ? E : 0};
         uint64_t off[ResultArrays::kArrays];
         uint64_t total = 0;
         for (int i = 0; i < ResultArrays::kArrays; ++i) {
@@ -1057,7 +1058,8 @@ struct Engine::Impl {
             check_launch();
         }
         if (se) {
-            k_fin_states<<<grid_for(uint64_t(S) * 32, 256), 256, 0, st>>>(ptrs(), S, eoff, voff, dp(9),
+            k_fin_states<<<grid_for(uint64_t(S) * 32, 256), 256, 0, st>>>(ptrs(), S, eoff, voff,
+                                                                         si ? dp(9) : nullptr,
                                                                          dp(10), dp(12));
             check_launch();
         } else {
@@ -1117,6 +1119,7 @@ struct Engine::Impl {
         std::vector<EvolutionResult> out(K);
         if (!K) return out;
         const bool se = opt.keep_state_edges, sg = opt.event_keys != 0;
+        const bool si = se && opt.keep_state_edge_ids;
         // concatenated id ranges (states, events, pairs) and each evolution's start in them
         std::vector<uint64_t> rs, rc, re, rce, rp, rcp;
         std::vector<uint32_t> tab(4 * (K + 1) + K, 0);
@@ -1218,7 +1221,7 @@ struct Engine::Impl {
             const uint64_t Ck = bnd[2 * (K + 1) + k + 1] - bnd[2 * (K + 1) + k];
             const uint64_t Kk = bnd[3 * (K + 1) + k + 1] - bnd[3 * (K + 1) + k];
             const uint64_t c[kArr] = {Sk, Sk, 4 * Ek, 3 * Kk, 2 * Bk, Ek + 1, Ck, 2 * Ek,
-                                      se ? Sk + 1 : 1, se ? Tk : 0, se ? Tk : 0, se ? Sk + 1 : 1,
+                                      se ? Sk + 1 : 1, si ? Tk : 0, se ? Tk : 0, se ? Sk + 1 : 1,
                                       se ? Vk : 0, sg ? Ek : 0};
             for (uint32_t a = 0; a < kArr; ++a) {
                 sec[uint64_t(k) * kArr + a] = total;
@@ -1238,7 +1241,8 @@ struct Engine::Impl {
             k_fin_offsets_multi<<<grid_for(S + K, 256), 256, 0, st>>>(sne, NS, d_sb, K, stage, d_sec, HGX_ARR_STATE_EDGE_OFF);
             k_fin_offsets_multi<<<grid_for(S + K, 256), 256, 0, st>>>(sno, NS, d_sb, K, stage, d_sec, HGX_ARR_STATE_VERT_OFF);
             check_launch();
-            k_fin_records_multi<<<grid_for(S * 32, 256), 256, 0, st>>>(ptrs(), sids, NS, d_sb, K, sne, sno, stage, d_sec);
+            k_fin_records_multi<<<grid_for(S * 32, 256), 256, 0, st>>>(ptrs(), sids, NS, d_sb, K, sne, sno, stage, d_sec,
+                                                                        si ? 1 : 0);
             check_launch();
         } else {
             k_fin_zero_multi<<<grid_for(K, 256), 256, 0, st>>>(stage, d_sec, K, HGX_ARR_STATE_EDGE_OFF);

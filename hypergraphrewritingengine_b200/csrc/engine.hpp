@@ -84,6 +84,7 @@ struct EvolutionResult {
 
 struct RunOptions {
     bool keep_state_edges = true;    // read back every state's edge record
+    bool keep_state_edge_ids = true; // ... including its global edge ids (else arities, vertices)
     bool readback = true;            // false: leave results on the device, return counts
     bool causal = true;
     bool branchial = true;

@@ -2093,7 +2093,7 @@ __global__ void k_fin_offsets_multi(const uint32_t* scan, uint32_t n, const uint
 
 __global__ void k_fin_records_multi(DevPtrs P, const uint32_t* sids, uint32_t n, const uint32_t* sb,
                                     uint32_t K, const uint32_t* eoff, const uint32_t* voff,
-                                    uint8_t* stage, const uint64_t* sec) {
+                                    uint8_t* stage, const uint64_t* sec, int with_ids) {
     const uint32_t lane = lane_id();
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n;
          i += (gridDim.x * blockDim.x) >> 5) {
@@ -2105,7 +2105,7 @@ __global__ void k_fin_records_multi(DevPtrs P, const uint32_t* sids, uint32_t n,
         const uint32_t ne = P.st_ne[s], nocc = P.st_nocc[s], aw = (ne + 3) >> 2;
         const uint32_t* rec = P.arena + P.st_off[s];
         for (uint32_t t = lane; t < ne; t += 32) {
-            oids[e0 + t] = rec[t];
+            if (with_ids) oids[e0 + t] = rec[t];
             oar[e0 + t] = (rec[ne + (t >> 2)] >> ((t & 3u) * 8u)) & 0xFFu;
         }
         for (uint32_t t = lane; t < nocc; t += 32) overts[v0 + t] = rec[ne + aw + t];
@@ -2688,7 +2688,7 @@ __global__ void k_fin_states(DevPtrs P, uint32_t n, const uint32_t* eoff, const 
         const uint32_t* rec = P.arena + P.st_off[s];
         const uint32_t e0 = eoff[s], v0 = voff[s];
         for (uint32_t i = lane; i < ne; i += 32) {
-            ids[e0 + i] = rec[i];
+            if (ids) ids[e0 + i] = rec[i];   // null: the ids are not part of the result
             ar[e0 + i] = (rec[ne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
         }
         for (uint32_t j = lane; j < nocc; j += 32) verts[v0 + j] = rec[ne + aw + j];

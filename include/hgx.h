@@ -114,7 +114,12 @@ typedef enum hgx_option {
        variable, from the signature buckets it is compatible with (SignatureIndex, index.hpp:30-130;
        common/include/hgcommon/signature_core.hpp:24-84); 0 = every edge is tested. Results are
        identical. */
-    HGX_OPT_JOIN_INDEX = 14
+    HGX_OPT_JOIN_INDEX = 14,
+    /* With HGX_OPT_KEEP_STATE_EDGES: 1 (default) = the state records carry their global edge
+       ids (HGX_ARR_STATE_EDGE_IDS); 0 = arities and vertices only, HGX_ARR_STATE_EDGE_IDS empty.
+       The reference's results carry the ids only under EvolveInput::edge_identity
+       (gpu/include/hg_gpu/evolve.hpp:36, default false); the hg_gpu shim maps it here. */
+    HGX_OPT_KEEP_STATE_EDGE_IDS = 15
 } hgx_option;
 
 /* One evolution of a batch or a served request. */
@@ -156,7 +161,7 @@ typedef enum hgx_array {
     HGX_ARR_EVENT_CONS = 6,      /* [u32 x CONSUMED] consumed edge ids, pattern order */
     HGX_ARR_EVENT_PROD = 7,      /* [u32 x EVENTS*2] (first produced edge id, count) */
     HGX_ARR_STATE_EDGE_OFF = 8,  /* [u32 x STATES+1] (needs HGX_OPT_KEEP_STATE_EDGES) */
-    HGX_ARR_STATE_EDGE_IDS = 9,  /* [u32 x STATE_EDGES] */
+    HGX_ARR_STATE_EDGE_IDS = 9,  /* [u32 x STATE_EDGES] (empty under HGX_OPT_KEEP_STATE_EDGE_IDS = 0) */
     HGX_ARR_STATE_ARITY = 10,    /* [u32 x STATE_EDGES] */
     HGX_ARR_STATE_VERT_OFF = 11, /* [u32 x STATES+1] */
     HGX_ARR_STATE_VERTS = 12,    /* [u32 x STATE_VERTS] */

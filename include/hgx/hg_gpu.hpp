@@ -435,6 +435,7 @@ public:
         compat::detail::check(hgx_engine_set_option(e, HGX_OPT_TRANSITIVE_REDUCTION, input.transitive_reduction));
         compat::detail::check(hgx_engine_set_option(e, HGX_OPT_QUOTIENT, quotient));
         compat::detail::check(hgx_engine_set_option(e, HGX_OPT_KEEP_STATE_EDGES, 1));
+        compat::detail::check(hgx_engine_set_option(e, HGX_OPT_KEEP_STATE_EDGE_IDS, input.edge_identity));
         compat::detail::check(hgx_engine_set_option(e, HGX_OPT_MAX_STATES, input.max_states));
         compat::detail::check(hgx_engine_set_option(e, HGX_OPT_RECORD_CAUSAL, input.record.causal));
         compat::detail::check(hgx_engine_set_option(e, HGX_OPT_RECORD_BRANCHIAL, input.record.branchial));

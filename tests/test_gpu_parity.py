@@ -293,3 +293,27 @@ def test_join_index_modes_match_oracle(engine, index):
     finally:
         engine.set_option(api.OPT_FORWARDING, 0)
         engine.set_option(api.OPT_JOIN_INDEX, 1)
+
+
+def test_state_edge_ids_optional(engine):
+    """HGX_OPT_KEEP_STATE_EDGE_IDS = 0 leaves the global edge ids out of the state records (the
+    reference's default, edge_identity false); everything else is unchanged, alone and batched."""
+    import numpy as np
+    from hypergraphrewritingengine_b200 import api
+    ev = W.config2(5)
+    evs = W.config4(n=12, max_states=256)
+    full = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True)
+    full_b = engine.evolve_batch(evs)
+    engine.set_option(api.OPT_KEEP_STATE_EDGE_IDS, 0)
+    try:
+        slim = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=True)
+        slim_b = engine.evolve_batch(evs)
+    finally:
+        engine.set_option(api.OPT_KEEP_STATE_EDGE_IDS, 1)
+    for a, b in [(full, slim)] + list(zip(full_b, slim_b)):
+        assert len(b.state_edge_ids) == 0 and len(a.state_edge_ids) == len(a.state_arity)
+        for f in ("state_hash", "events", "causal", "branchial", "state_edge_off", "state_arity",
+                  "state_vert_off", "state_verts"):
+            assert np.array_equal(getattr(a, f), getattr(b, f)), f
+        assert all(a.state_edges(s) == b.state_edges(s) for s in range(0, a.num_states, 97))
+        assert b.bytes() < a.bytes()
