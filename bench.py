@@ -249,6 +249,9 @@ def main():
                     help="small-state join: 0 autotuned (default), 1 warp join, 2 lane walk")
     ap.add_argument("--profile-run", action="store_true",
                     help="run the workload once, device-resident, and exit (for profilers)")
+    ap.add_argument("--profile-workload", default="c2", choices=["c2", "c4", "large"],
+                    help="--profile-run workload: c2 (--levels levels), c4 (1024 random "
+                         "evolutions) or large (256 random evolutions with 65-256-edge states)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -256,10 +259,22 @@ def main():
         from hypergraphrewritingengine_b200 import Engine
         from hypergraphrewritingengine_b200 import workloads as W
         from hypergraphrewritingengine_b200 import api
-        ev = W.config2(args.levels)
         eng = Engine(0)
         eng.set_option(api.OPT_LANE_JOIN, args.lane_join)
-        c = eng.counts(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+        if args.profile_workload == "c2":
+            ev = W.config2(args.levels)
+            c = eng.counts(ev.rules, ev.roots, ev.steps, quotient=True, max_states=ev.max_states)
+        else:
+            evs = (W.config4(n=1024) if args.profile_workload == "c4" else
+                   [W.random_evolution(i, seed=0x1A26E, edges_lo=65, edges_hi=256, steps_lo=2,
+                                       steps_hi=4) for i in range(256)])
+            jobs, keep = eng.make_jobs(evs)
+            out = (api.ctypes.c_void_p * len(evs))()
+            eng.set_option(api.OPT_READBACK, 0)
+            api._check(eng._L.hgx_evolve_batch(eng._h, jobs, len(evs), out))
+            c = {"events": sum(int(eng._L.hgx_result_count(out[i], 1)) for i in range(len(evs)))}
+            for i in range(len(evs)):
+                eng._L.hgx_result_free(out[i])
         print(json.dumps(c))
         return
 
@@ -524,7 +539,7 @@ def sharded_batch(eng, dist, world, rank, barrier, per_rank=1024):
 
 
 def join_index_ab(eng, reps=3):
-    """The join with and without its vertex / signature indices (states past 64 edges), on the
+    """The join with and without its vertex / signature indices (states past 96 edges), on the
     batched workload (C4) and on a batch of large-state evolutions (256 draws of the same
     generator with 65-256 initial edges, 2-4 steps, cap 4096): device time of the warp-per-child
     expand kernel (the large-state path) and wall time of the whole batch, best of `reps`."""

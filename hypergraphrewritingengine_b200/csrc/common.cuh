@@ -50,7 +50,7 @@ constexpr uint32_t kHashOccMin = 96;
 
 // Join indices: states of more than kJoinIndexMin edges staged for the warp join carry a vertex
 // index and, when their edges fall in at most kSigBuckets signatures, a signature index.
-constexpr uint32_t kJoinIndexMin = 64;
+constexpr uint32_t kJoinIndexMin = 96;
 constexpr uint32_t kSigBuckets = 16;
 
 // (Writing the multiply by the prime 2^40 + 0x1b3 as a shift and a 32-bit multiply measured

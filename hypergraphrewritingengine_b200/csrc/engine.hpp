@@ -104,7 +104,7 @@ struct RunOptions {
     uint32_t lane_join = 0;
     // Capped single evolution: 0 = split a level at the estimated cut, 1 = never, N >= 2 = at N.
     uint64_t level_split = 0;
-    // Join indices (vertex and signature) for staged states past 64 edges: 1 = on, 0 = every
+    // Join indices (vertex and signature) for staged states past 96 edges: 1 = on, 0 = every
     // candidate is tested against every edge. Results are identical.
     uint32_t join_index = 1;
 };

@@ -503,12 +503,29 @@ __device__ void compute_cands(const Layout& L, char* sm, const DevRule& R, uint3
     __syncwarp();
 }
 
+// Skipping in the warp join: at the last pattern position every candidate is one match, so a
+// caller that does not need a run of leading matches (a slice that starts past them, or a
+// count) takes the whole candidate set at once -- its popcount -- instead of walking it. The
+// policy says how many leading matches the caller still wants skipped (left) and learns how many
+// were (take); `want` and the counter are warp-uniform.
+struct NoSkip {
+    __device__ uint32_t left() const { return 0u; }
+    __device__ void take(uint32_t) const {}
+};
+struct SkipCounter {
+    uint32_t* n;     // matches passed so far (enumerated or skipped)
+    uint32_t want;   // skip while fewer than this have passed
+    __device__ uint32_t left() const { return want > *n ? want - *n : 0u; }
+    __device__ void take(uint32_t c) const { *n += c; }
+};
+
 // sched: the binding order of the LHS positions; seed >= 0 pins the first scheduled position to
-// that state position (a seeded join: every emitted match uses it there).
-template <class F>
+// that state position (a seeded join: every emitted match uses it there). limit: stop once this
+// many matches have passed (enumerated or skipped).
+template <class F, class Skip = NoSkip>
 __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Parent& pa,
                           const uint8_t* sched, int seed, F&& on_match,
-                          uint32_t limit = 0xFFFFFFFFu) {
+                          uint32_t limit = 0xFFFFFFFFu, Skip skip = Skip()) {
     const uint32_t lane = lane_id();
     const uint32_t n = R.n_lhs;
     const uint32_t nw = (pa.ne + 31) >> 5;
@@ -527,6 +544,19 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
     __syncwarp();
     uint32_t mask = 0;
     uint32_t d = 0;
+    // the candidates of the last position at depth dd, taken whole when the caller skips them all
+    auto try_skip = [&](uint32_t dd) {
+        const uint32_t want = skip.left();
+        if (!want) return;
+        uint32_t c = 0;
+        for (uint32_t w = lane; w < nw; w += 32) c += __popc(cand[dd * L.W + w]);
+        c = warp_sum32(c);
+        if (c == 0 || c > want) return;
+        skip.take(c);
+        limit -= c;
+        for (uint32_t w = lane; w < nw; w += 32) cand[dd * L.W + w] = 0;
+        __syncwarp();
+    };
     compute_cands(L, sm, R, sched[0], pa, mask, cand);
     if (seed >= 0) {
         // keep only the seed among the first position's candidates
@@ -534,6 +564,7 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
             cand[w] &= (static_cast<uint32_t>(seed) >> 5) == w ? (1u << (seed & 31)) : 0u;
         __syncwarp();
     }
+    if (n == 1) try_skip(0);
     while (true) {
         int pick = -1;
         for (uint32_t w = 0; w < nw; ++w) {
@@ -581,6 +612,7 @@ __device__ void warp_join(const Layout& L, char* sm, const DevRule& R, const Par
             mask = nm;
             ++d;
             compute_cands(L, sm, R, sched[d], pa, mask, cand + d * L.W);
+            if (d + 1 == n) try_skip(d);
         }
     }
     __syncwarp();
@@ -1144,12 +1176,12 @@ __device__ void fwd_emit(const Layout& L, char* sm, const DevRule& R, const uint
 }
 
 // Every match of the staged state in canonical order: the full join, or forwarding.
-template <class F>
+template <class F, class Skip = NoSkip>
 __device__ void enumerate_matches(const DevPtrs& P, const Layout& L, char* sm, const DevRule& R,
                                   const Parent& pa, const Fwd& f, F&& on_match,
-                                  uint32_t limit = 0xFFFFFFFFu) {
+                                  uint32_t limit = 0xFFFFFFFFu, Skip skip = Skip()) {
     if (!f.on) {
-        warp_join(L, sm, R, pa, R.sched, -1, on_match, limit);
+        warp_join(L, sm, R, pa, R.sched, -1, on_match, limit, skip);
         return;
     }
     const uint32_t lane = lane_id();
@@ -1344,7 +1376,8 @@ __global__ void __launch_bounds__(256, 4) k_count(DevPtrs P, LevelArgs A, Layout
                 fwd_on = fw.on;
                 if (fw.on) cnt = fwd_count(P, L, sm, R, pa, fw);
                 else if (pa.ne <= kLaneEMax && R.n_lhs <= kLaneJoinLhs) cnt = lane_join_count(L, sm, R, pa);
-                else warp_join(L, sm, R, pa, R.sched, -1, [&](uint32_t) { ++cnt; });
+                else warp_join(L, sm, R, pa, R.sched, -1, [&](uint32_t) { ++cnt; }, 0xFFFFFFFFu,
+                               SkipCounter{&cnt, 0xFFFFFFFFu});
             }
             if (lane == 0) A.counts[f * A.rules_stride + r] = cnt;
             max_cnt = max(max_cnt, cnt);
@@ -1593,6 +1626,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                 const uint32_t hi = min(rn, c_hi - rb);
                 uint32_t idx = 0;
                 uint8_t rpos[kMaxPatternEdges];
+                // matches before the slice are skipped whole at the last position (popcounts)
                 enumerate_matches(P, L, sm, R, pa, fwd, [&](uint32_t nm) {
                     if (idx >= lo && idx < hi) {
                         for (uint32_t k = 0; k < R.n_lhs; ++k) rpos[k] = static_cast<uint8_t>(match[k]);
@@ -1603,7 +1637,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                         __syncwarp();
                     }
                     ++idx;
-                }, hi);
+                }, hi, SkipCounter{&idx, lo});
             }
         }
     }

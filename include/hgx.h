@@ -108,7 +108,7 @@ typedef enum hgx_option {
        (gpu/include/hg_gpu/evolve.hpp:136-141), whose one-shot evolve stops at the limit with a
        kDeviceOutOfMemory warning; the hg_gpu shim maps the error to that warning. */
     HGX_OPT_MAX_DEVICE_BYTES = 13,
-    /* Join indices for staged states of more than 64 edges: 1 (default) = candidates for a
+    /* Join indices for staged states of more than 96 edges: 1 (default) = candidates for a
        pattern edge come from the bound vertex of smallest degree (the reference's
        InvertedVertexIndex, hypergraph/include/hypergraph/index.hpp:134-230) or, with no bound
        variable, from the signature buckets it is compatible with (SignatureIndex, index.hpp:30-130;

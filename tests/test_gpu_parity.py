@@ -253,7 +253,7 @@ def test_lane_join_variants_match_oracle(engine, join):
 
 
 def _large_state_cases():
-    """Evolutions whose states pass 64 edges (the join indices' range): served-workload draws
+    """Evolutions whose states pass 64 edges (the join indices apply past 96): served-workload draws
     with large initial states (up to 256 edges, rules with repeated variables among them), a
     100-edge hub, and two disconnected LHS edges (candidates from the signature buckets)."""
     out = []
@@ -265,14 +265,14 @@ def _large_state_cases():
                            max_states=3000, name="hub-100"))
     out.append(W.Evolution(rules=[([[0, 0, 1], [2, 3, 3]], [[0, 1, 4], [2, 3, 4], [4, 4, 0]])],
                            roots=[[[k % 23 + 1, k % 23 + 1, k % 7 + 30] if k % 3 == 0 else
-                                   [k % 11 + 1, k % 13 + 40, k % 13 + 40] for k in range(90)]],
+                                   [k % 11 + 1, k % 13 + 40, k % 13 + 40] for k in range(120)]],
                            steps=2, max_states=2000, name="disconnected-lhs"))
     return out
 
 
 @pytest.mark.parametrize("index", [1, 0])
 def test_join_index_modes_match_oracle(engine, index):
-    """The join with and without the vertex / signature indices (states past 64 edges) gives the
+    """The join with and without the vertex / signature indices (states past 96 edges) gives the
     oracle's result, alone and in a batch, with and without match forwarding."""
     from hypergraphrewritingengine_b200 import api
     evs = _large_state_cases()
