@@ -170,8 +170,10 @@ enum class LayoutKind { Count, Lane, Warp };
 
 // Shared-memory carve-up per warp. Count: the parent and the join. Lane: plus the parent's
 // per-vertex occurrence lists and a 32-match batch. Warp: plus the warp-per-child WL arrays.
+// NV: the most distinct vertices a staged state of this layout has (0 = bound them by NOCC); the
+// warp layout's per-vertex WL arrays and the vertex hash table are sized by it.
 Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kind, bool fwd = false,
-                   uint32_t mcap = kLaneJoinCap, bool index = false) {
+                   uint32_t mcap = kLaneJoinCap, bool index = false, uint32_t NV = 0) {
     const bool wl = kind == LayoutKind::Warp;
     const bool lane = kind == LayoutKind::Lane;
     Layout L;
@@ -182,9 +184,11 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
     L.NOCC = NOCC;
     L.CNE = NE + rm.rhs;
     L.CNOCC = NOCC + rm.rhs_total;
-    L.V = NOCC + rm.fresh;
+    L.NV = NV ? std::min(std::max<uint32_t>(NV, 1), NOCC) : NOCC;
+    L.V = L.NV + rm.fresh;
     L.W = (NE + 31) / 32;
-    L.NBR = wl ? L.CNOCC * rm.arity : 0;
+    // neighbour-sort entries of one WL round: sum over occurrences of max(a - 1, 1)
+    L.NBR = wl ? L.CNOCC * std::max<uint32_t>(rm.arity - 1, 1) : 0;
     uint32_t off = 0;
     auto take = [&](uint32_t bytes, uint32_t align) {
         off = align_up(off, align);
@@ -201,7 +205,7 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
     }
     L.o_peid = take(4 * NE, 4);
     L.o_occ = take(4 * (wl ? L.CNOCC : NOCC), 4);
-    L.o_deg = take(4 * (wl ? L.V : NOCC), 4);
+    L.o_deg = take(4 * (wl ? std::max(L.V, NOCC) : NOCC), 4);   // also load_parent's first-occurrence scratch
     if (wl) {
         L.o_ooff = take(4 * (L.V + 1), 4);
         L.o_nbo = take(4 * (L.V + 1), 4);
@@ -231,8 +235,8 @@ Layout make_layout(uint32_t NE, uint32_t NOCC, const RuleMax& rm, LayoutKind kin
         L.o_sched2 = take(kMaxPatternEdges, 1);
     }
     if (NOCC > kHashOccMin) {
-        L.VT = 1;
-        while (L.VT < 2 * NOCC) L.VT <<= 1;
+        L.VT = 64;   // load <= 1/2 over the state's distinct vertices
+        while (L.VT < 2 * L.NV) L.VT <<= 1;
         L.o_vtab = take(4 * L.VT, 4);
         L.o_vtid = take(2 * L.VT, 2);
     }
@@ -406,7 +410,7 @@ struct Engine::Impl {
     DVec<DevRule> rules;
     DVec<DevEvo> evos;
     DVec<uint64_t> st_off, st_hash;
-    DVec<uint32_t> st_ne, st_nocc, st_evo, st_depth, st_event, st_ev0, st_evn;
+    DVec<uint32_t> st_ne, st_nocc, st_evo, st_depth, st_event, st_ev0, st_evn, st_nv, ev_nv;
     DVec<uint32_t> arena;
     DVec<unsigned long long> arena_top;
     DVec<uint32_t> edge_creator;
@@ -505,7 +509,7 @@ struct Engine::Impl {
         cudaSetDevice(device);
         cudaStreamSynchronize(st);
         for (auto* v : std::initializer_list<DVec<uint32_t>*>{
-                 &st_ne, &st_nocc, &st_evo, &st_depth, &st_event, &st_ev0, &st_evn, &arena,
+                 &st_ne, &st_nocc, &st_evo, &st_depth, &st_event, &st_ev0, &st_evn, &st_nv, &ev_nv, &arena,
                  &edge_creator, &ev_in,
                  &ev_rule, &ev_coff, &ev_prod, &ev_fresh, &ev_out, &ev_cons, &ev_cprod,
                  &state_of_arrival, &tab_vals, &evo_cut, &evo_first_ev, &evo_last_ev,
@@ -588,6 +592,8 @@ struct Engine::Impl {
         P.st_event = st_event.p;
         P.st_ev0 = st_ev0.p;
         P.st_evn = st_evn.p;
+        P.st_nv = st_nv.p;
+        P.ev_nv = ev_nv.p;
         P.st_hash = st_hash.p;
         P.arena = arena.p;
         P.arena_top = arena_top.p;
@@ -929,6 +935,7 @@ struct Engine::Impl {
         st_event.ensure(n, k, st);
         st_ev0.ensure(n, k, st);
         st_evn.ensure(n, k, st);
+        st_nv.ensure(n, k, st);
     }
 
     void grow_events(uint64_t n) {
@@ -941,6 +948,7 @@ struct Engine::Impl {
         ev_out.ensure(n, k, st);
         ev_kept.ensure(n, k, st);
         ev_hash.ensure(n, k, st);
+        ev_nv.ensure(n, k, st);
         state_of_arrival.ensure(n, k, st);
     }
 
@@ -1483,7 +1491,7 @@ struct Engine::Impl {
 
         // ---- sync 1: level totals, per-evolution event ranges, exact frontier maxima
         const size_t nevo = h_evos.size();
-        const size_t w1 = 4 + 4 * nevo;
+        const size_t w1 = 5 + 4 * nevo;
         sync_pack.ensure(w1, 0, st);
         unsigned long long* hs = sync_host(std::max<size_t>(w1, (7 * nevo + 4 + 1) / 2));
         k_sync1_pack<<<grid_for(std::max<size_t>(nevo, 1), 256), 256, 0, st>>>(
@@ -1497,12 +1505,13 @@ struct Engine::Impl {
                                  uint32_t(hs[1] >> 32), uint32_t(hs[2]), uint32_t(hs[2] >> 32)};
         const uint32_t fmax_cnt = uint32_t(hs[3]);
         const uint32_t n_warp_states = uint32_t(hs[3] >> 32);   // 0: no warp-path launches
+        const uint32_t fmax_nv = uint32_t(hs[4]);                // largest frontier vertex count
         std::vector<uint32_t> h_first(nevo), h_last(nevo);
-        std::vector<unsigned long long> h_classes(hs + 4, hs + 4 + nevo),
-            h_states_ev(hs + 4 + nevo, hs + 4 + 2 * nevo), h_sigs(hs + 4 + 2 * nevo, hs + 4 + 3 * nevo);
+        std::vector<unsigned long long> h_classes(hs + 5, hs + 5 + nevo),
+            h_states_ev(hs + 5 + nevo, hs + 5 + 2 * nevo), h_sigs(hs + 5 + 2 * nevo, hs + 5 + 3 * nevo);
         for (size_t e = 0; e < nevo; ++e) {
-            h_first[e] = uint32_t(hs[4 + 3 * nevo + e]);
-            h_last[e] = uint32_t(hs[4 + 3 * nevo + e] >> 32);
+            h_first[e] = uint32_t(hs[5 + 3 * nevo + e]);
+            h_last[e] = uint32_t(hs[5 + 3 * nevo + e] >> 32);
         }
         auto h_states_now = [&](uint32_t e) { return static_cast<uint64_t>(h_states_ev[e]); };
         const uint32_t n_ev = tot[0], n_cons_lv = tot[1], n_prod = tot[2], n_fresh = tot[3];
@@ -1570,7 +1579,7 @@ struct Engine::Impl {
             const Layout Ll = make_layout(std::min<uint32_t>(mne, kLaneEMax), mno, rm, LayoutKind::Lane, fwd,
                                           fmax_cnt);
             const Layout Lw = make_layout(mne, mno, rm, LayoutKind::Warp, fwd, kLaneJoinCap,
-                                          opt.join_index != 0);
+                                          opt.join_index != 0, fmax_nv);
             // lane kernel join: autotuned per bucket of children per frontier state (the walk
             // amortises its count-and-emit passes over many children per state)
             const uint64_t per_state = n_ev / std::max<uint32_t>(F, 1);

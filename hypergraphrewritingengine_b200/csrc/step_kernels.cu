@@ -214,15 +214,25 @@ __device__ Parent load_parent(const DevPtrs& P, const Layout& L, char* sm, uint3
         const uint32_t TS = L.VT;
         for (uint32_t t = lane; t < TS; t += 32) tab[t] = kNone;
         __syncwarp();
+        bool full = false;   // a vertex found no slot: more distinct vertices than the layout holds
         for (uint32_t j = lane; j < pa.nocc; j += 32) {
             const uint32_t v = glob[j];
             uint32_t h = (v * 2654435761u) & (TS - 1);
+            bool placed = false;
             for (uint32_t probe = 0; probe < TS; ++probe) {
                 const uint32_t prev = atomicCAS(&tab[h], kNone, v);
-                if (prev == kNone || prev == v) break;
+                if (prev == kNone || prev == v) { placed = true; break; }
                 h = (h + 1) & (TS - 1);
             }
+            full |= !placed;
             first[j] = h;
+        }
+        if (__any_sync(0xFFFFFFFFu, full)) {
+            if (lane == 0) atomicOr(P.err, kErrStateTooLarge);
+            __syncwarp();
+            pa.ne = 0;
+            pa.nocc = 0;
+            return pa;
         }
         __syncwarp();
         uint32_t ids = 0;
@@ -237,6 +247,11 @@ __device__ Parent load_parent(const DevPtrs& P, const Layout& L, char* sm, uint3
         for (uint32_t j = lane; j < pa.nocc; j += 32) vloc[j] = tid[first[j]];
         __syncwarp();
         pa.nvp = ids;
+        if (ids > L.NV) {   // more vertices than the layout's per-vertex arrays hold
+            if (lane == 0) atomicOr(P.err, kErrStateTooLarge);
+            __syncwarp();
+            pa.ne = pa.nocc = pa.nvp = 0;
+        }
         return pa;
     }
     run = 0;
@@ -261,6 +276,11 @@ __device__ Parent load_parent(const DevPtrs& P, const Layout& L, char* sm, uint3
     }
     __syncwarp();
     pa.nvp = run;
+    if (run > L.NV) {   // more vertices than the layout's per-vertex arrays hold
+        if (lane == 0) atomicOr(P.err, kErrStateTooLarge);
+        __syncwarp();
+        pa.ne = pa.nocc = pa.nvp = 0;
+    }
     return pa;
 }
 
@@ -1326,6 +1346,7 @@ __global__ void k_roots(DevPtrs P, const uint32_t* sids, uint32_t n, uint32_t* w
         const uint64_t h = warp_wl(L, sm, pa.ne, pa.nvp, info);
         if (lane == 0) {
             P.st_hash[sid] = h;
+            P.st_nv[sid] = pa.nvp;
             const uint32_t a = P.st_event[sid];
             P.ev_hash[a] = h;
             table_insert(P, P.evos[P.st_evo[sid]], h, a);
@@ -1529,6 +1550,7 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                 P.ev_prod[e] = pid;
                 P.ev_fresh[e] = fresh0 + idx * R.n_fresh;
                 P.ev_hash[e] = h;
+                P.ev_nv[e] = info.nv;
                 for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = peid[rpos[k]];
                 P.ev_bmask[e] = branch_mask(R.n_lhs, pa.ne, rpos);
                 for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
@@ -1744,7 +1766,7 @@ __global__ void k_evo_causal(DevPtrs P, uint32_t n_events, unsigned long long* o
 // size the expand layouts) and how many states with children are off the lane path
 // (level_max[5]; none: the warp-path launches are skipped).
 __global__ void k_frontier_events(DevPtrs P, LevelArgs A, uint32_t* evo_last, uint32_t* evo_frange) {
-    uint32_t mne = 0, mno = 0, n_warp = 0;
+    uint32_t mne = 0, mno = 0, mnv = 0, n_warp = 0;
     for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < A.n_frontier;
          f += gridDim.x * blockDim.x) {
         const uint32_t sid = A.frontier[f];
@@ -1753,6 +1775,7 @@ __global__ void k_frontier_events(DevPtrs P, LevelArgs A, uint32_t* evo_last, ui
         P.st_evn[sid] = A.item_ev[t + 1] - A.item_ev[t];
         mne = max(mne, P.st_ne[sid]);
         mno = max(mno, P.st_nocc[sid]);
+        mnv = max(mnv, P.st_nv[sid]);
         const bool children = A.item_ev[t + A.rules_stride] != A.item_ev[t];
         n_warp += (!(A.fmode[f] & 1u) && children) ? 1u : 0u;
         const uint32_t evo = P.st_evo[sid];
@@ -1768,10 +1791,12 @@ __global__ void k_frontier_events(DevPtrs P, LevelArgs A, uint32_t* evo_last, ui
     }
     mne = warp_max32(mne);
     mno = warp_max32(mno);
+    mnv = warp_max32(mnv);
     n_warp = warp_sum32(n_warp);
     if (lane_id() == 0) {
         atomicMax(&A.level_max[2], mne);
         atomicMax(&A.level_max[3], mno);
+        atomicMax(&A.level_max[6], mnv);
         if (n_warp) atomicAdd(&A.level_max[5], n_warp);
     }
 }
@@ -1797,12 +1822,13 @@ __global__ void k_sync1_pack(const uint32_t* item_ev, const uint32_t* item_cons,
         out[1] = item_prod[ni] | (u64(item_fresh[ni]) << 32);
         out[2] = level_max[2] | (u64(level_max[3]) << 32);
         out[3] = level_max[4] | (u64(level_max[5]) << 32);
+        out[4] = level_max[6];
     }
     for (uint32_t e = t; e < nevo; e += gridDim.x * blockDim.x) {
-        out[4 + e] = classes[e];
-        out[4 + nevo + e] = states[e];
-        out[4 + 2ull * nevo + e] = sigs ? sigs[e] : 0ull;
-        out[4 + 3ull * nevo + e] = first[e] | (u64(last[e]) << 32);
+        out[5 + e] = classes[e];
+        out[5 + nevo + e] = states[e];
+        out[5 + 2ull * nevo + e] = sigs ? sigs[e] : 0ull;
+        out[5 + 3ull * nevo + e] = first[e] | (u64(last[e]) << 32);
     }
 }
 
@@ -1895,6 +1921,7 @@ __global__ void __launch_bounds__(256, kWalk ? 4 : 3) k_expand_lanes2(DevPtrs P,
             P.ev_prod[e] = pid;
             P.ev_fresh[e] = ri.fresh0 + idx * R.n_fresh;
             P.ev_hash[e] = h;
+            P.ev_nv[e] = info.nv;
             for (uint32_t k = 0; k < R.n_lhs; ++k) P.ev_cons[coff + k] = peid[slot[k]];
             P.ev_bmask[e] = branch_mask(R.n_lhs, pa.ne, slot);
             for (uint32_t k = 0; k < R.n_rhs; ++k) P.edge_creator[pid + k] = e;
@@ -2511,6 +2538,7 @@ __global__ void __launch_bounds__(256, 4) k_materialize(DevPtrs P, LevelArgs A, 
             gne = pne_l - R.n_lhs + R.n_rhs;
             gnocc = pnocc_l - R.lhs_total + R.rhs_total;
             words = gne + ((gne + 3) >> 2) + gnocc;
+            P.st_nv[A.state_base + jl] = P.ev_nv[e_l];
         }
         const uint32_t inc = warp_incl_scan(words);
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);

@@ -33,6 +33,7 @@ struct DevPtrs {
     uint32_t* st_event;     // arrival (event or root pseudo-event) that created it
     uint32_t* st_ev0;       // first event of the state's expansion (single-rule evolutions)
     uint32_t* st_evn;       // events of the state's expansion
+    uint32_t* st_nv;        // distinct vertices of the state
     uint64_t* st_hash;
     uint32_t* arena;        // per-state records: ids[ne] | arity bytes[ceil(ne/4) words] | verts[nocc]
     unsigned long long* arena_top;
@@ -48,6 +49,7 @@ struct DevPtrs {
     uint32_t* ev_out;       // output state (the class representative in quotient mode)
     uint8_t*  ev_kept;      // 0 when a state cap cut the event off
     uint64_t* ev_hash;      // WL hash of the output state
+    uint32_t* ev_nv;        // distinct vertices of the output state
     uint32_t* ev_cons;      // consumed edge ids, pattern order
     uint32_t* ev_cprod;     // producer event of each consumed edge
     uint32_t* state_of_arrival;
@@ -123,6 +125,7 @@ struct LevelArgs {
 // Per-warp shared-memory carve-up, sized on the host from the level's largest state.
 struct Layout {
     uint32_t NE, NOCC, CNE, CNOCC, V, W, NBR;
+    uint32_t NV;        // distinct vertices a staged state may have (V = NV + fresh variables)
     uint32_t o_cur, o_nxt, o_csum, o_ccnt, o_nbr;                  // u64
     uint32_t o_peid, o_occ, o_ooff, o_nbo, o_deg, o_nn, o_comp;     // u32
     uint32_t o_cand, o_taken, o_misc;                               // u32
