@@ -71,8 +71,13 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """SM clocks and clock-event (throttle) reasons sampled while running: through NVML every
+    10 ms on the device torch uses (found by PCI bus id), else nvidia-smi every 200 ms. Reads
+    only; changes no setting."""
 
+    # NVML clock-event reason bits (nvmlClocksEventReason*)
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -80,9 +85,47 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.lines = []
+        self.samples = []          # (sm MHz, max MHz, reason bits) from NVML
         self.proc = None
+        self.stop = threading.Event()
+        self.t = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.gpu)
+        bus = getattr(props, "pci_bus_id", None)
+        if bus is None:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+        dom, dev = getattr(props, "pci_domain_id", 0), getattr(props, "pci_device_id", 0)
+        for i in range(pynvml.nvmlDeviceGetCount()):
+            h = pynvml.nvmlDeviceGetHandleByIndex(i)
+            pci = pynvml.nvmlDeviceGetPciInfo(h)
+            if (pci.bus, pci.device, pci.domain) == (bus, dev, dom):
+                return pynvml, h
+        raise RuntimeError("no NVML device with the PCI address torch reports")
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def run():
+                while not self.stop.is_set():
+                    try:
+                        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                             nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.01)
+            self.t = threading.Thread(target=run, daemon=True)
+            self.t.start()
+            self.source = "nvml, 10 ms"
+            return self
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -90,6 +133,7 @@ class ClockSampler:
                 stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.source = "nvidia-smi, 200 ms"
         except OSError:
             self.proc = None
         return self
@@ -99,15 +143,22 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        elif self.t is not None:
+            self.t.join(timeout=1)
 
     def summary(self):
         mhz, mx, reasons = [], 0.0, set()
+        for sm, smax, bits in self.samples:
+            mhz.append(float(sm))
+            mx = max(mx, float(smax))
+            reasons.update(n for b, n in self.REASONS.items() if bits & b)
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
@@ -122,7 +173,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(mhz)}
+                "reasons": sorted(reasons), "samples": len(mhz), "source": self.source}
 
 
 def max_over_ranks(dist, value: float, device: str = "cuda") -> float:
