@@ -35,7 +35,7 @@ HGX_OK, HGX_ERR_INVALID, HGX_ERR_CUDA, HGX_ERR_CAPACITY, HGX_ERR_NO_DEVICE, HGX_
 (OPT_QUOTIENT, OPT_MAX_STATES, OPT_TRANSITIVE_REDUCTION, OPT_RECORD_CAUSAL, OPT_RECORD_BRANCHIAL,
  OPT_KEEP_STATE_EDGES, OPT_TIMING, OPT_READBACK, OPT_FORWARDING, OPT_CHUNK_MIN,
  OPT_EVENT_SIGNATURE_KEYS, OPT_LANE_JOIN, OPT_LEVEL_SPLIT, OPT_MAX_DEVICE_BYTES,
- OPT_JOIN_INDEX, OPT_KEEP_STATE_EDGE_IDS) = range(16)
+ OPT_JOIN_INDEX, OPT_KEEP_STATE_EDGE_IDS, OPT_STREAM_RESULT) = range(17)
 (COUNT_STATES, COUNT_EVENTS, COUNT_CLASSES, COUNT_CAUSAL, COUNT_BRANCHIAL, COUNT_TRUNCATED,
  COUNT_CONSUMED, COUNT_STATE_EDGES, COUNT_STATE_VERTS, COUNT_RAW_STATES,
  COUNT_CANONICAL_EVENTS) = range(11)
@@ -56,7 +56,7 @@ EXPORTS = (
     "hgx_evolve_batch", "hgx_serve_reset", "hgx_serve_admit", "hgx_serve_admit_batch", "hgx_serve_step",
     "hgx_serve_take_finished", "hgx_serve_collect", "hgx_serve_collect_batch", "hgx_serve_device_bytes",
     "hgx_result_count",
-    "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats",
+    "hgx_result_copy", "hgx_result_free", "hgx_engine_stage_times", "hgx_engine_expand_stats", "hgx_engine_result_stats",
     "hgx_engine_stream", "hgx_hash_states_noalloc", "hgx_result_view",
     "hgx_estimate_device_bytes", "hgx_device_memory", "hgx_result_views",
 )
@@ -112,6 +112,7 @@ def load_library(path: str = LIB_PATH):
         "hgx_result_view": ([vp, ctypes.c_int, ctypes.POINTER(vp), u64p], ctypes.c_int),
         "hgx_engine_stage_times": ([vp, ctypes.POINTER(ctypes.c_double), u64p], ctypes.c_int),
         "hgx_engine_expand_stats": ([vp, u64p], ctypes.c_int),
+        "hgx_engine_result_stats": ([vp, u64p], ctypes.c_int),
         "hgx_engine_stream": ([vp, ctypes.POINTER(vp)], ctypes.c_int),
         "hgx_hash_states_noalloc": ([vp, vp, vp, vp, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_uint32, vp, vp, vp], ctypes.c_int),
@@ -273,7 +274,7 @@ class _ResultOwner:
             pass
 
 
-_ARR_TYPES = {ARR_STATE_HASH: np.uint64, ARR_EVENT_SIG: np.uint64}
+_ARR_TYPES = {ARR_STATE_HASH: np.uint64, ARR_EVENT_SIG: np.uint64, ARR_STATE_ARITY: np.uint8}
 _ARR_SHAPES = {ARR_EVENTS: 4, ARR_CAUSAL: 3, ARR_BRANCHIAL: 2, ARR_EVENT_PROD: 2}
 
 
@@ -433,6 +434,13 @@ class Engine:
         return dict(zip(("stage_bytes", "hbm_bytes", "children", "wl_rounds", "launches",
                          "warp_stage_bytes", "warp_hbm_bytes", "warp_children", "warp_rounds",
                          "warp_ns", "walk_launches"), list(out)))
+
+    def result_stats(self):
+        """Whether the last result was streamed (copied out range by range during the run) and
+        in how many chunks."""
+        out = (ctypes.c_uint64 * 2)()
+        _check(self._L.hgx_engine_result_stats(self._h, out))
+        return {"streamed": bool(out[0]), "chunks": int(out[1])}
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

@@ -235,6 +235,10 @@ hgx_status hgx_engine_set_option(hgx_engine* e, hgx_option opt, uint64_t value) 
         case HGX_OPT_MAX_DEVICE_BYTES: e->engine.set_device_limit(value); return HGX_OK;
         case HGX_OPT_JOIN_INDEX: e->opt.join_index = value != 0; return HGX_OK;
         case HGX_OPT_KEEP_STATE_EDGE_IDS: e->opt.keep_state_edge_ids = value != 0; return HGX_OK;
+        case HGX_OPT_STREAM_RESULT:
+            if (value > 2) return fail(HGX_ERR_INVALID, "stream result: 0 off, 1 results of 64 MB or more, 2 always");
+            e->opt.stream_result = static_cast<uint32_t>(value);
+            return HGX_OK;
         case HGX_OPT_LANE_JOIN:
             if (value > 2) return fail(HGX_ERR_INVALID, "lane join must be 0 (autotuned), 1 or 2");
             e->opt.lane_join = static_cast<uint32_t>(value);
@@ -415,7 +419,10 @@ hgx_status hgx_result_copy(const hgx_result* res, hgx_array what, void* dst, siz
     if (!res || (!dst && bytes)) return fail(HGX_ERR_INVALID, "null argument");
     if (static_cast<int>(what) < 0 || static_cast<int>(what) >= hgx::ResultArrays::kArrays)
         return fail(HGX_ERR_INVALID, "unknown array");
-    const size_t need = res->count[what] * ((what == HGX_ARR_STATE_HASH || what == HGX_ARR_EVENT_SIG) ? 8 : 4);
+    const size_t elem = (what == HGX_ARR_STATE_HASH || what == HGX_ARR_EVENT_SIG) ? 8
+                        : what == HGX_ARR_STATE_ARITY                          ? 1
+                                                                              : 4;
+    const size_t need = res->count[what] * elem;
     if (bytes < need) return fail(HGX_ERR_INVALID, "hgx_result_copy: destination too small");
     if (need) std::memcpy(dst, res->ptr[what], need);
     return HGX_OK;
@@ -470,6 +477,14 @@ hgx_status hgx_engine_expand_stats(hgx_engine* e, uint64_t* out) {
     out[8] = t.warp_rounds;
     out[9] = static_cast<uint64_t>(t.expand_warp * 1e6);   // warp kernel time, ns
     out[10] = t.walk_launches;
+    return HGX_OK;
+}
+
+hgx_status hgx_engine_result_stats(hgx_engine* e, uint64_t* out) {
+    if (!e || !out) return fail(HGX_ERR_INVALID, "null argument");
+    const auto& t = e->engine.times();
+    out[0] = t.result_streamed;
+    out[1] = t.result_chunks;
     return HGX_OK;
 }
 

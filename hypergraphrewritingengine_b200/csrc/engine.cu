@@ -60,9 +60,12 @@ struct DVec {
         }
         T* np = nullptr;
         HGX_CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&np), nc * sizeof(T), s));
-        if (p && keep)
-            HGX_CUDA_CHECK(cudaMemcpyAsync(np, p, std::min(keep, cap) * sizeof(T),
-                                           cudaMemcpyDeviceToDevice, s));
+        if (p && keep) {   // by the SMs, not a copy engine (see k_copy_bytes)
+            const uint64_t bytes = std::min(keep, cap) * sizeof(T);
+            k_copy_bytes<<<static_cast<uint32_t>(std::min<uint64_t>((bytes + 4095) / 4096, 1184)), 256, 0, s>>>(
+                reinterpret_cast<const uint8_t*>(p), reinterpret_cast<uint8_t*>(np), bytes);
+            HGX_CUDA_CHECK(cudaGetLastError());
+        }
         if (p) HGX_CUDA_CHECK(cudaFreeAsync(p, s));
         p = np;
         cap = nc;
@@ -78,6 +81,7 @@ struct DVec {
 
 // Bytes per element of result array i (the hashes and signatures are u64).
 inline uint64_t arr_elem_bytes(int i) {
+    if (i == HGX_ARR_STATE_ARITY) return 1;
     return (i == HGX_ARR_STATE_HASH || i == HGX_ARR_EVENT_SIG) ? 8 : 4;
 }
 
@@ -165,6 +169,12 @@ DevRule pack_rule(const RuleSpec& r) {
 }
 
 uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+// A streamed result's level is split into parts of at least this many frontier states.
+constexpr uint32_t kStreamPartStates = 16384;
+// Results streamed only when the last one was at least this large (a small result's copy is
+// shorter than the per-range work streaming adds).
+constexpr uint64_t kStreamMinBytes = 64ull << 20;
 
 enum class LayoutKind { Count, Lane, Warp };
 
@@ -286,7 +296,7 @@ struct LaunchShape {
 //     up to kKeepBytes in total, the smallest returned to the system beyond that.
 struct PinnedPool {
     static constexpr size_t kSmall = 4u << 20, kSlab = 32u << 20;
-    static constexpr size_t kKeepBytes = size_t(2) << 30;
+    static constexpr size_t kKeepBytes = size_t(8) << 30;
     struct Slab {
         uint8_t* base = nullptr;
         size_t top = 0;
@@ -363,8 +373,10 @@ struct PinnedPool {
             }
         }
         if (!p) {
-            cap = kSmall * 2;
-            while (cap < bytes) cap <<= 1;
+            size_t pow2 = kSmall * 2;
+            while (pow2 < bytes) pow2 <<= 1;
+            const size_t step = std::max<size_t>(pow2 / 8, kSmall * 2);   // within 1/8 of the need
+            cap = std::max<size_t>((bytes + step - 1) / step * step, kSmall * 2);
             HGX_CUDA_CHECK(cudaHostAlloc(&p, cap, cudaHostAllocDefault));
         }
         *out = static_cast<uint8_t*>(p);
@@ -460,6 +472,369 @@ struct Engine::Impl {
         return h_sync;
     }
 
+    // Small device-to-host reads and device-to-device copies of the engine stream run on the SMs
+    // (k_copy_bytes, into mapped page-locked memory for the reads): they never wait on a copy
+    // engine behind the streamed result's copies. sync_st() synchronises the stream and moves the
+    // reads to their destinations.
+    uint8_t* rb = nullptr;
+    size_t rb_cap = 0, rb_top = 0;
+    struct RbCopy {
+        void* dst;
+        size_t off, bytes;
+    };
+    std::vector<RbCopy> rb_pending;
+    static uint32_t copy_grid(uint64_t bytes) {
+        return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>((bytes + 4095) / 4096, kNumSMs * 8)));
+    }
+    void copy_d2d(void* dst, const void* src, uint64_t bytes) {
+        if (!bytes) return;
+        k_copy_bytes<<<copy_grid(bytes), 256, 0, st>>>(static_cast<const uint8_t*>(src),
+                                                       static_cast<uint8_t*>(dst), bytes);
+        check_launch();
+    }
+    void readback(void* dst, const void* src, size_t bytes) {
+        if (!bytes) return;
+        if (!sr.on) {   // no result copies in flight: a plain copy
+            HGX_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+            return;
+        }
+        const size_t sz = (bytes + 15) / 16 * 16;
+        if (rb_top + sz > rb_cap) {
+            sync_st();   // the pending reads land first
+            if (sz > rb_cap) {
+                if (rb) HGX_CUDA_CHECK(cudaFreeHost(rb));
+                rb = nullptr;
+                rb_cap = std::max<size_t>(sz, std::max<size_t>(2 * rb_cap, 1 << 20));
+                HGX_CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&rb), rb_cap, cudaHostAllocMapped));
+            }
+        }
+        uint8_t* d = nullptr;
+        HGX_CUDA_CHECK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d), rb, 0));
+        k_copy_bytes<<<copy_grid(bytes), 256, 0, st>>>(static_cast<const uint8_t*>(src), d + rb_top, bytes);
+        check_launch();
+        rb_pending.push_back({dst, rb_top, bytes});
+        rb_top += sz;
+    }
+    void sync_st() {
+        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        for (const RbCopy& c : rb_pending) std::memcpy(c.dst, rb + c.off, c.bytes);
+        rb_pending.clear();
+        rb_top = 0;
+    }
+
+    // ---- streamed result of a single evolution: each finished frontier range's share of the
+    // result arrays is finalised on the engine stream into a chunk buffer and copied to the host
+    // on the copy stream while the next ranges compute, straight to its final place in the
+    // result's per-array page-locked blocks (every array is appended in id order, range by range).
+    cudaStream_t cst = nullptr;
+    struct ResultStream {
+        bool on = false, failed = false, pending = false;
+        bool se = false, si = false, causal = false, branchial = false;
+        uint32_t R = 0, rule_begin = 0, c0 = 0;
+        bool c0_known = false;
+        uint64_t s_done = 0, e_done = 0, b_done = 0;      // states / events / pairs streamed
+        uint64_t used[ResultArrays::kArrays] = {};        // elements written per array
+        uint64_t cap[ResultArrays::kArrays] = {};         // elements of room per array
+        uint8_t* h[ResultArrays::kArrays] = {};
+        std::shared_ptr<void> own[ResultArrays::kArrays];
+        uint64_t tot[4] = {};                             // consumed, causal, state edges, verts
+        // the prepared chunk whose copies are not issued yet; every chunk buffer stays allocated
+        // until the run's copies are done (a buffer freed on the copy stream and reused on the
+        // engine stream would make the engine stream wait for those copies)
+        uint8_t* dbuf = nullptr;
+        std::vector<uint8_t*> bufs;
+        uint64_t doff[ResultArrays::kArrays] = {}, dcount[ResultArrays::kArrays] = {};
+        uint32_t* hsz = nullptr;                          // its device-sized counts (page-locked)
+        cudaEvent_t ready = nullptr;
+    } sr;
+    uint64_t sr_hint[ResultArrays::kArrays] = {};        // room the last streamed result needed
+    DVec<uint32_t> sr_dev;                               // [0..3] running totals, [4..7] chunk sizes
+
+    // Whether array i's page-locked block has room for `need` elements. Blocks are sized when the
+    // stream begins (from the last result of this engine) and never grown: a result that
+    // outgrows them is copied whole at the end instead.
+    bool sr_room(int i, uint64_t need) {
+        if (need <= sr.cap[i]) return true;
+        sr.failed = true;
+        return false;
+    }
+
+    static bool stream_eligible(const RunOptions& opt, size_t nevo) {
+        return opt.readback && opt.stream_result && !opt.event_keys && nevo == 1;
+    }
+
+    // Streams the result of the (single) evolution just admitted when the engine's last result
+    // gives the size of every array (blocks from the pool; small arrays move to small blocks at
+    // the end, so a large block goes back to the pool with the run).
+    void stream_begin(const RunOptions& opt) {
+        sr.on = false;
+        if (!stream_eligible(opt, h_evos.size())) return;
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            sr.used[i] = sr.cap[i] = 0;
+            sr.h[i] = nullptr;
+            sr.own[i].reset();
+        }
+        uint64_t hinted = 0;
+        for (int i = 0; i < ResultArrays::kArrays; ++i) hinted += sr_hint[i] * arr_elem_bytes(i);
+        if (!sr_hint[HGX_ARR_STATE_HASH]) return;                           // no result yet
+        if (opt.stream_result == 1 && hinted < kStreamMinBytes) return;     // too small to gain
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            if (!sr_hint[i]) continue;
+            const uint64_t eb = arr_elem_bytes(i);
+            uint8_t* p = nullptr;
+            sr.own[i] = PinnedPool::acquire(pinned, sr_hint[i] * eb, &p);
+            sr.h[i] = p;
+            sr.cap[i] = sr_hint[i];
+        }
+        for (auto& t : sr.tot) t = 0;
+        sr.on = true;
+        sr.failed = sr.pending = sr.c0_known = false;
+        sr.se = opt.keep_state_edges;
+        sr.si = opt.keep_state_edges && opt.keep_state_edge_ids;
+        sr.causal = opt.causal;
+        sr.branchial = opt.branchial;
+        sr.R = static_cast<uint32_t>(n_roots_admitted);
+        sr.rule_begin = h_evos[0].rule_begin;
+        sr.s_done = 0;
+        sr.e_done = sr.R;
+        sr.b_done = 0;
+        sr_dev.ensure(8, 0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(sr_dev.p, 0, 8 * sizeof(uint32_t), st));
+    }
+
+    // Issues the prepared chunk's copies. The engine stream must have been synchronised since the
+    // chunk was prepared (its device-sized counts are then in sr.hsz).
+    void stream_issue() {
+        if (!sr.pending) return;
+        const uint32_t C = sr.hsz[0], K = sr.hsz[1], T = sr.hsz[2], V = sr.hsz[3];
+        sr.dcount[HGX_ARR_EVENT_CONS] = C;
+        sr.dcount[HGX_ARR_CAUSAL] = 3ull * K;
+        sr.dcount[HGX_ARR_STATE_EDGE_IDS] = sr.si ? T : 0;
+        sr.dcount[HGX_ARR_STATE_ARITY] = sr.se ? T : 0;
+        sr.dcount[HGX_ARR_STATE_VERTS] = sr.se ? V : 0;
+        sr.tot[0] += C;
+        sr.tot[1] += K;
+        sr.tot[2] += T;
+        sr.tot[3] += V;
+        bool room = true;
+        for (int i = 0; i < ResultArrays::kArrays; ++i)
+            if (sr.dcount[i]) room = sr_room(i, sr.used[i] + sr.dcount[i] + 1) && room;   // + 1: a closing offset
+        if (!room) {
+            sr.dbuf = nullptr;
+            sr.pending = false;
+            return;
+        }
+        HGX_CUDA_CHECK(cudaStreamWaitEvent(cst, sr.ready, 0));
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            if (!sr.dcount[i]) continue;
+            const uint64_t eb = arr_elem_bytes(i);
+            HGX_CUDA_CHECK(cudaMemcpyAsync(sr.h[i] + sr.used[i] * eb, sr.dbuf + sr.doff[i],
+                                           sr.dcount[i] * eb, cudaMemcpyDeviceToHost, cst));
+            sr.used[i] += sr.dcount[i];
+        }
+        sr.dbuf = nullptr;
+        sr.pending = false;
+        ++times.result_chunks;
+    }
+
+    // After a frontier range: finalise what it added (states [s_done, q3), events [q0, q1), pairs
+    // [q4, q5) of the single evolution; q from the range's per-evolution ranges) into a chunk
+    // buffer. max_ne / max_no bound the edges and occurrences of its states.
+    void stream_prep(const uint32_t* q, uint64_t max_ne, uint64_t max_no) {
+        if (!sr.on || sr.failed) return;
+        if (sr.pending) {   // no synchronisation since the last chunk: take its counts now
+            sync_st();
+            stream_issue();
+        }
+        const uint64_t s1 = std::max<uint64_t>(q[3], sr.s_done);
+        const bool ev_any = q[1] > q[0];
+        if ((ev_any && q[0] != sr.e_done) || (q[5] > q[4] && q[4] != sr.b_done) ||
+            (q[3] > q[2] && q[2] < sr.s_done)) {
+            sr.failed = true;   // not one contiguous continuation: the whole result at the end
+            return;
+        }
+        const uint64_t nS = s1 - sr.s_done, nE = ev_any ? q[1] - q[0] : 0;
+        const uint64_t nB = (sr.branchial && q[5] > q[4]) ? q[5] - q[4] : 0;
+        if (!nS && !nE && !nB) return;
+        if (nE && !sr.c0_known) {
+            readback(&sr.c0, ev_coff.p + sr.R, 4);
+            sync_st();
+            sr.c0_known = true;
+        }
+        const uint64_t Cb = nE * std::max<uint32_t>(rm.lhs, 1);
+        const uint64_t Tb = sr.se ? nS * std::max<uint64_t>(max_ne, 1) : 0;
+        const uint64_t Vb = sr.se ? nS * std::max<uint64_t>(max_no, 1) : 0;
+        // chunk buffer: the result arrays' slices (bounds for the device-sized ones), then the
+        // causal counts
+        uint64_t cnt[ResultArrays::kArrays] = {nS, nS, 4 * nE, sr.causal ? 3 * Cb : 0, 2 * nB, nE, Cb,
+                                               2 * nE, sr.se ? nS + 1 : 0, sr.si ? Tb : 0, Tb,
+                                               sr.se ? nS + 1 : 0, Vb, 0};
+        uint64_t total = 0;
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            sr.doff[i] = total;
+            total += (cnt[i] * arr_elem_bytes(i) + 15) / 16 * 16;
+        }
+        const uint64_t o_ccnt = total;
+        total += (nE + 1) * 4;
+        HGX_CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&sr.dbuf), std::max<uint64_t>(total, 16), st));
+        sr.bufs.push_back(sr.dbuf);
+        auto dp = [&](int i) { return reinterpret_cast<uint32_t*>(sr.dbuf + sr.doff[i]); };
+        HGX_CUDA_CHECK(cudaMemsetAsync(sr_dev.p + 4, 0, 4 * sizeof(uint32_t), st));
+        if (nS) {
+            copy_d2d(sr.dbuf + sr.doff[0], st_hash.p + sr.s_done, nS * 8);
+            copy_d2d(sr.dbuf + sr.doff[1], st_depth.p + sr.s_done, nS * 4);
+        }
+        const uint32_t first = static_cast<uint32_t>(q[0]), ne32 = static_cast<uint32_t>(nE);
+        if (nE) {
+            k_fin_events<<<grid_for(nE, 256), 256, 0, st>>>(ptrs(), first, ne32, sr.rule_begin, dp(2), dp(5),
+                                                             dp(7), sr.c0);
+            check_launch();
+            uint32_t* tmp = sr_dev.p + 4;   // reused: the chunk's consumed count lands in sizes[0]
+            k_fin_cons_chunk<<<grid_for(nE, 256), 256, 0, st>>>(ptrs(), first, ne32, dp(6), tmp);
+            check_launch();
+            k_fin_advance<<<1, 32, 0, st>>>(tmp, sr_dev.p, sr_dev.p + 4, 0);
+            check_launch();
+            if (sr.causal) {
+                uint32_t* ccnt = reinterpret_cast<uint32_t*>(sr.dbuf + o_ccnt);
+                k_fin_causal<<<grid_for(nE, 256), 256, 0, st>>>(ptrs(), sr.R, first, ne32, ccnt, nullptr, nullptr, 0);
+                check_launch();
+                scan(ccnt, ccnt, ne32);
+                k_fin_causal<<<grid_for(nE, 256), 256, 0, st>>>(ptrs(), sr.R, first, ne32, nullptr, ccnt, dp(3), 1);
+                check_launch();
+                k_fin_advance<<<1, 32, 0, st>>>(ccnt + nE, sr_dev.p, sr_dev.p + 4, 1);
+                check_launch();
+            }
+        }
+        if (nB) {
+            k_fin_shift<<<grid_for(2 * nB, 256), 256, 0, st>>>(bpairs.p + 2 * q[4], 2 * nB, sr.R, dp(4));
+            check_launch();
+        }
+        if (sr.se && nS) {
+            const uint32_t s0 = static_cast<uint32_t>(sr.s_done), ns32 = static_cast<uint32_t>(nS);
+            scan(st_ne.p + s0, dp(8), ns32);
+            scan(st_nocc.p + s0, dp(11), ns32);
+            k_fin_states<<<grid_for(nS * 32, 256), 256, 0, st>>>(ptrs(), s0, ns32, dp(8), dp(11),
+                                                                sr.si ? dp(9) : nullptr,
+                                                                sr.dbuf + sr.doff[10], dp(12));
+            check_launch();
+            k_fin_rebase<<<grid_for(nS, 256), 256, 0, st>>>(dp(8), ns32, sr_dev.p, 2);
+            check_launch();
+            k_fin_advance<<<1, 32, 0, st>>>(dp(8) + nS, sr_dev.p, sr_dev.p + 4, 2);
+            check_launch();
+            k_fin_rebase<<<grid_for(nS, 256), 256, 0, st>>>(dp(11), ns32, sr_dev.p, 3);
+            check_launch();
+            k_fin_advance<<<1, 32, 0, st>>>(dp(11) + nS, sr_dev.p, sr_dev.p + 4, 3);
+            check_launch();
+        }
+        readback(sr.hsz, sr_dev.p + 4, 4 * sizeof(uint32_t));
+        HGX_CUDA_CHECK(cudaEventRecord(sr.ready, st));
+        // the element counts known now (the device-sized ones are filled in at issue)
+        for (int i = 0; i < ResultArrays::kArrays; ++i) sr.dcount[i] = 0;
+        sr.dcount[HGX_ARR_STATE_HASH] = nS;
+        sr.dcount[HGX_ARR_STATE_DEPTH] = nS;
+        sr.dcount[HGX_ARR_EVENTS] = 4 * nE;
+        sr.dcount[HGX_ARR_BRANCHIAL] = 2 * nB;
+        sr.dcount[HGX_ARR_EVENT_CONS_OFF] = nE;
+        sr.dcount[HGX_ARR_EVENT_PROD] = 2 * nE;
+        sr.dcount[HGX_ARR_STATE_EDGE_OFF] = sr.se ? nS : 0;
+        sr.dcount[HGX_ARR_STATE_VERT_OFF] = sr.se ? nS : 0;
+        sr.pending = true;
+        sr.s_done = s1;
+        if (nE) sr.e_done = q[1];
+        if (q[5] > q[4]) sr.b_done = q[5];
+    }
+
+    // Room for the next streamed result: this one's sizes and a sixteenth more.
+    void stream_hints(const uint64_t* count) {
+        for (int i = 0; i < ResultArrays::kArrays; ++i)
+            sr_hint[i] = count[i] ? count[i] + count[i] / 16 + 64 : 0;
+        sr_hint[HGX_ARR_STATE_HASH] = std::max<uint64_t>(sr_hint[HGX_ARR_STATE_HASH], 1);
+    }
+
+    // The chunk buffers, once the copy stream is done with them.
+    void stream_free_bufs() {
+        HGX_CUDA_CHECK(cudaStreamSynchronize(cst));
+        for (uint8_t* b : sr.bufs) HGX_CUDA_CHECK(cudaFreeAsync(b, st));
+        sr.bufs.clear();
+    }
+
+    // Drops a stream that could not finish (the result is then finalised whole).
+    void stream_abort() {
+        sr.dbuf = nullptr;
+        sr.pending = false;
+        stream_free_bufs();
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            sr.own[i].reset();
+            sr.h[i] = nullptr;
+            sr.cap[i] = sr.used[i] = 0;
+        }
+        sr.on = false;
+    }
+
+    // The streamed result: the last chunk's copies, the closing offsets, the counts. Empty (no
+    // flat arrays) when a block had no room: the caller then finalises the result whole.
+    EvolutionResult finalize_streamed() {
+        if (sr.s_done < n_states) {   // states no range streamed (the roots of a run of no levels)
+            const uint32_t q[7] = {uint32_t(sr.e_done), uint32_t(sr.e_done), uint32_t(sr.s_done),
+                                   uint32_t(n_states), uint32_t(sr.b_done), uint32_t(sr.b_done), 0};
+            stream_prep(q, ne_bound, nocc_bound);
+        }
+        if (sr.failed) return {};
+        sync_st();
+        stream_issue();
+        if (sr.failed) return {};
+        stream_free_bufs();
+        // closing entries of the offset arrays: total consumed / state edges / state vertices
+        const int closing[3] = {HGX_ARR_EVENT_CONS_OFF, HGX_ARR_STATE_EDGE_OFF, HGX_ARR_STATE_VERT_OFF};
+        const uint64_t value[3] = {sr.tot[0], sr.se ? sr.tot[2] : 0, sr.se ? sr.tot[3] : 0};
+        for (int j = 0; j < 3; ++j) {
+            const int i = closing[j];
+            if (!sr_room(i, sr.used[i] + 1)) break;
+            reinterpret_cast<uint32_t*>(sr.h[i])[sr.used[i]] = static_cast<uint32_t>(value[j]);
+            sr.used[i] += 1;
+        }
+        if (sr.failed) return {};
+        EvolutionResult r;
+        auto owners = std::make_shared<std::vector<std::shared_ptr<void>>>();
+        auto flat = std::make_shared<ResultArrays>();
+        for (int i = 0; i < ResultArrays::kArrays; ++i) {
+            const uint64_t eb = arr_elem_bytes(i);
+            if (sr.own[i] && sr.used[i] * eb <= PinnedPool::kSmall / 4 &&
+                sr.cap[i] * eb > PinnedPool::kSmall) {
+                // a small array in a large kept block: move it to a small one, free the large one
+                uint8_t* p = nullptr;
+                std::shared_ptr<void> own = PinnedPool::acquire(pinned, std::max<uint64_t>(sr.used[i] * eb, 16), &p);
+                std::memcpy(p, sr.h[i], sr.used[i] * eb);
+                sr.own[i] = std::move(own);
+                sr.h[i] = p;
+            }
+            if (sr.own[i]) owners->push_back(sr.own[i]);
+            flat->ptr[i] = sr.h[i];
+            flat->count[i] = sr.used[i];
+            sr.own[i].reset();
+            sr.h[i] = nullptr;
+        }
+        stream_hints(flat->count);
+        flat->owner = owners;
+        unsigned long long classes = 0;
+        uint32_t stopped = 0;
+        readback(&classes, evo_classes.p, 8);
+        readback(&stopped, evo_stopped.p, 4);
+        sync_st();
+        r.flat = flat;
+        r.n_roots = sr.R;
+        r.num_classes = classes;
+        r.n_canonical_events = flat->count[HGX_ARR_EVENT_CONS_OFF] - 1;
+        times.result_streamed = 1;
+        r.truncated = stopped != 0;
+        if (r.truncated)
+            r.warnings.push_back(
+                "capacity limit reached: the state cap stopped the evolution; the states, events "
+                "and relations returned are valid and incomplete");
+        sr.on = false;
+        return r;
+    }
+
     // host mirrors
     std::vector<DevRule> h_rules;
     std::vector<DevEvo> h_evos;
@@ -478,8 +853,11 @@ struct Engine::Impl {
             throw std::runtime_error("hgx: no CUDA device available (the step has no CPU fallback)");
         HGX_CUDA_CHECK(cudaSetDevice(device));
         HGX_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        HGX_CUDA_CHECK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
         HGX_CUDA_CHECK(cudaEventCreate(&ev_a));
         HGX_CUDA_CHECK(cudaEventCreate(&ev_b));
+        HGX_CUDA_CHECK(cudaEventCreateWithFlags(&sr.ready, cudaEventDisableTiming));
+        HGX_CUDA_CHECK(cudaMallocHost(reinterpret_cast<void**>(&sr.hsz), 4 * sizeof(uint32_t)));
         cudaMemPool_t pool;
         HGX_CUDA_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
         uint64_t thr = UINT64_MAX;
@@ -547,6 +925,13 @@ struct Engine::Impl {
         fin_tab.release(st);
         fin_sec.release(st);
         sync_pack.release(st);
+        sr_dev.release(st);
+        cudaStreamSynchronize(cst);
+        for (uint8_t* b : sr.bufs) cudaFreeAsync(b, st);
+        cudaStreamDestroy(cst);
+        cudaEventDestroy(sr.ready);
+        if (sr.hsz) cudaFreeHost(sr.hsz);
+        if (rb) cudaFreeHost(rb);
         if (h_sync) cudaFreeHost(h_sync);
         rules.release(st);
         evos.release(st);
@@ -558,6 +943,7 @@ struct Engine::Impl {
     }
 
     void reset() {
+        if (sr.on) stream_abort();   // a run that ended in an error
         h_rules.clear();
         h_evos.clear();
         evo_ranges.clear();
@@ -1013,7 +1399,7 @@ struct Engine::Impl {
         uint32_t* eoff = fin_cnt.p + E + 1;         // [S+1]
         uint32_t* voff = eoff + S + 1;              // [S+1]
         if (E && opt.causal) {
-            k_fin_causal<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), R, E, ccnt, nullptr, nullptr, 0);
+            k_fin_causal<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), R, R, E, ccnt, nullptr, nullptr, 0);
             check_launch();
             scan(ccnt, ccnt, E);
         } else {
@@ -1058,7 +1444,7 @@ struct Engine::Impl {
             HGX_CUDA_CHECK(cudaMemsetAsync(dp(5), 0, 4, st));
         }
         if (K) {
-            k_fin_causal<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), R, E, nullptr, ccnt, dp(3), 1);
+            k_fin_causal<<<grid_for(E, 256), 256, 0, st>>>(ptrs(), R, R, E, nullptr, ccnt, dp(3), 1);
             check_launch();
         }
         if (B) {
@@ -1066,9 +1452,9 @@ struct Engine::Impl {
             check_launch();
         }
         if (se) {
-            k_fin_states<<<grid_for(uint64_t(S) * 32, 256), 256, 0, st>>>(ptrs(), S, eoff, voff,
+            k_fin_states<<<grid_for(uint64_t(S) * 32, 256), 256, 0, st>>>(ptrs(), 0, S, eoff, voff,
                                                                          si ? dp(9) : nullptr,
-                                                                         dp(10), dp(12));
+                                                                         d + off[10], dp(12));
             check_launch();
         } else {
             HGX_CUDA_CHECK(cudaMemsetAsync(dp(8), 0, 4, st));
@@ -1384,26 +1770,37 @@ struct Engine::Impl {
             if (F > opt.level_split) P = static_cast<uint32_t>(opt.level_split);
         } else if (one_capped && opt.level_split == 0 && hist.valid && F >= 4096) {
             unsigned long long have[2];
-            HGX_CUDA_CHECK(cudaMemcpyAsync(&have[0], evo_classes.p, 8, cudaMemcpyDeviceToHost, st));
-            HGX_CUDA_CHECK(cudaMemcpyAsync(&have[1], evo_states.p, 8, cudaMemcpyDeviceToHost, st));
-            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+            readback(&have[0], evo_classes.p, 8);
+            readback(&have[1], evo_states.p, 8);
+            sync_st();
             const uint64_t h = h_evos[0].quotient ? have[0] : have[1];
             const uint64_t remaining = h_evos[0].max_states > h ? h_evos[0].max_states - h : 0;
             const double need = double(remaining) * (h_evos[0].quotient ? hist.ev_per_new : 1.0);
             const double est = need / std::max(hist.ev_per_state, 1e-9) * 1.15 + 256;
             if (est < 0.8 * double(F)) P = static_cast<uint32_t>(est);
         }
-        level_range(opt, 0, P);
+        // the level's frontier ranges: [0, P), in up to four parts when the result streams (each
+        // part's share of the result is copied out while the next computes), then [P, F)
+        std::vector<std::pair<uint32_t, uint32_t>> parts;
+        const uint32_t K = sr.on ? std::min<uint32_t>(4, std::max<uint32_t>(1, P / kStreamPartStates)) : 1;
+        for (uint32_t j = 0; j < K; ++j)
+            parts.emplace_back(uint32_t(uint64_t(P) * j / K), uint32_t(uint64_t(P) * (j + 1) / K));
+        if (P < F) parts.emplace_back(P, F);
         bool cut = false;
-        if (P < F) {
-            uint32_t stopped = 0;
-            HGX_CUDA_CHECK(cudaMemcpyAsync(&stopped, evo_stopped.p, 4, cudaMemcpyDeviceToHost, st));
-            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
-            if (!stopped) level_range(opt, P, F);
-            HGX_CUDA_CHECK(cudaMemcpyAsync(&stopped, evo_stopped.p, 4, cudaMemcpyDeviceToHost, st));
-            HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        uint32_t stopped = 0;
+        for (size_t j = 0; j < parts.size(); ++j) {
+            if (j > 0 && one_capped) {
+                readback(&stopped, evo_stopped.p, 4);
+                sync_st();
+                if (stopped) break;
+            }
+            level_range(opt, parts[j].first, parts[j].second);
+        }
+        if (parts.size() > 1 && one_capped) {
+            readback(&stopped, evo_stopped.p, 4);
+            sync_st();
             // a level with a cut sends none of the evolution's new states on (the cut range has
-            // sent none of its own; the earlier range's are dropped here)
+            // sent none of its own; the earlier ranges' are dropped here)
             cut = stopped != 0;
             if (cut) {
                 sub_nf = 0;
@@ -1499,8 +1896,9 @@ struct Engine::Impl {
             evo_states.p, opt.event_keys ? evo_sigs.p : nullptr, evo_first_ev.p, evo_last_ev.p,
             static_cast<uint32_t>(nevo), sync_pack.p);
         check_launch();
-        HGX_CUDA_CHECK(cudaMemcpyAsync(hs, sync_pack.p, w1 * 8, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        readback(hs, sync_pack.p, w1 * 8);
+        sync_st();
+        if (sr.on) stream_issue();   // the previous range's result chunk (its counts are here now)
         const uint32_t tot[6] = {uint32_t(hs[0]), uint32_t(hs[0] >> 32), uint32_t(hs[1]),
                                  uint32_t(hs[1] >> 32), uint32_t(hs[2]), uint32_t(hs[2] >> 32)};
         const uint32_t fmax_cnt = uint32_t(hs[3]);
@@ -1661,9 +2059,9 @@ struct Engine::Impl {
             } else {
                 tune = false;   // rounds: several launches, no single measurement window
                 std::vector<uint32_t> h_item(NI + 1), h_fr(2 * nevo);
-                HGX_CUDA_CHECK(cudaMemcpyAsync(h_item.data(), item_ev.p, (NI + 1) * 4, cudaMemcpyDeviceToHost, st));
-                HGX_CUDA_CHECK(cudaMemcpyAsync(h_fr.data(), evo_frange.p, 2 * nevo * 4, cudaMemcpyDeviceToHost, st));
-                HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+                readback(h_item.data(), item_ev.p, (NI + 1) * 4);
+                readback(h_fr.data(), evo_frange.p, 2 * nevo * 4);
+                sync_st();
                 auto fev = [&](uint32_t f) -> uint64_t { return h_item[uint64_t(f) * R]; };
                 std::vector<uint8_t> is_capped(nevo, 0);
                 for (Capped& c : capped) {
@@ -1735,8 +2133,8 @@ struct Engine::Impl {
                     }
                     HGX_CUDA_CHECK(cudaMemsetAsync(evo_new.p, 0, nevo * 8, st));
                     run_ranges(true);
-                    HGX_CUDA_CHECK(cudaMemcpyAsync(h_new.data(), evo_new.p, nevo * 8, cudaMemcpyDeviceToHost, st));
-                    HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+                    readback(h_new.data(), evo_new.p, nevo * 8);
+                    sync_st();
                     bool any_open = false;
                     for (size_t i = 0; i < capped.size(); ++i) {
                         Capped& c = capped[i];
@@ -1764,8 +2162,8 @@ struct Engine::Impl {
             }
             const uint32_t n_ev_eff = F_eff == F ? n_ev : [&] {
                 uint32_t v = 0;
-                HGX_CUDA_CHECK(cudaMemcpyAsync(&v, item_ev.p + uint64_t(F_eff) * R, 4, cudaMemcpyDeviceToHost, st));
-                HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+                readback(&v, item_ev.p + uint64_t(F_eff) * R, 4);
+                sync_st();
                 return v;
             }();
             A.n_events = n_ev_eff;
@@ -1804,8 +2202,12 @@ struct Engine::Impl {
         A.boff = boff.p;
         if (opt.branchial && ne2) {
             tic();
-            k_bpairs<false><<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
+            k_bpairs<false><<<grid_for(uint64_t(F_eff) * 32, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
+            if (fmax_ne > 63) {   // parents without position masks
+                k_bpairs_walk<false><<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
+                check_launch();
+            }
             scan(bcount.p, boff.p, ne2);
             toc(times.branchial);
         } else {
@@ -1828,8 +2230,8 @@ struct Engine::Impl {
                                        lvl_ranges.p + 7 * nevo);
         check_launch();
         uint32_t* hs2 = reinterpret_cast<uint32_t*>(sync_host((7 * nevo + 4 + 1) / 2));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(hs2, lvl_ranges.p, (7 * nevo + 4) * 4, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaStreamSynchronize(st));
+        readback(hs2, lvl_ranges.p, (7 * nevo + 4) * 4);
+        sync_st();
         const std::vector<uint32_t> h_rng(hs2, hs2 + 7 * nevo);
         const uint32_t* s2 = hs2 + 7 * nevo;
         if (tune) {
@@ -1899,8 +2301,12 @@ struct Engine::Impl {
             // pair offsets are absolute: shift by the running total
             A.boff = boff.p;
             A.bpairs = bpairs.p + 2ull * n_bpairs;
-            k_bpairs<true><<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
+            k_bpairs<true><<<grid_for(uint64_t(F_eff) * 32, 256), 256, 0, st>>>(ptrs(), A);
             check_launch();
+            if (fmax_ne > 63) {
+                k_bpairs_walk<true><<<grid_for(ne2, 256), 256, 0, st>>>(ptrs(), A);
+                check_launch();
+            }
             toc(times.branchial);
         }
 
@@ -1925,6 +2331,7 @@ struct Engine::Impl {
         sub_no = std::max(sub_no, max_no);
         sub_ev += n_ev;
         sub_new += n_new;
+        if (sr.on && !evo_done[0] && h_first[0] != kNone) stream_prep(&h_rng[0], max_ne, max_no);
     }
 };
 
@@ -1941,11 +2348,23 @@ std::vector<EvolutionResult> Engine::run(const std::vector<EvolutionSpec>& specs
     std::vector<const EvolutionSpec*> ptrs;
     for (const auto& s : specs) ptrs.push_back(&s);
     const std::vector<uint32_t> ids = I.admit_many(ptrs);
+    I.stream_begin(opt);
     while (I.level(opt)) {}
     std::vector<EvolutionResult> out;
-    if (!opt.readback) I.read_counts(ids, out, opt.event_keys != 0);
-    else if (ids.size() == 1) out.push_back(I.finalize_single(opt));
-    else out = I.finalize_many(ids, opt);
+    if (!opt.readback) {
+        I.read_counts(ids, out, opt.event_keys != 0);
+    } else if (ids.size() == 1) {
+        EvolutionResult r;
+        if (I.sr.on && !I.sr.failed) r = I.finalize_streamed();
+        if (!r.flat) {   // not streamed, or a block had no room: the whole result at once
+            if (I.sr.on) I.stream_abort();
+            r = I.finalize_single(opt);
+            if (Impl::stream_eligible(opt, 1)) I.stream_hints(r.flat->count);
+        }
+        out.push_back(std::move(r));
+    } else {
+        out = I.finalize_many(ids, opt);
+    }
     I.finish_times();
     return out;
 }

@@ -61,7 +61,7 @@ struct EvolutionResult {
     std::vector<uint32_t> state_edge_off;       // [n+1] offsets into state_edge_ids (if kept)
     std::vector<uint32_t> state_edge_ids;
     std::vector<uint32_t> state_vert_off;       // [n+1] offsets into state_verts
-    std::vector<uint32_t> state_arity;          // per edge, parallel to state_edge_ids
+    std::vector<uint8_t> state_arity;           // per edge, parallel to state_edge_ids
     std::vector<uint32_t> state_verts;
     // Events (ids local to this evolution, in canonical order).
     std::vector<uint32_t> ev_in, ev_out, ev_rule, ev_step;
@@ -107,6 +107,12 @@ struct RunOptions {
     // Join indices (vertex and signature) for staged states past 96 edges: 1 = on, 0 = every
     // candidate is tested against every edge. Results are identical.
     uint32_t join_index = 1;
+    // Single evolutions read back to the host: 1 = when the engine's last result was at least
+    // 64 MB, each finished frontier range's share of the result is copied out while later ranges
+    // compute (page-locked blocks sized from that result; one that outgrows them is copied whole
+    // at the end); 2 = the same whatever the size; 0 = the whole result is copied at the end.
+    // Identical results.
+    uint32_t stream_result = 1;
 };
 
 // Per-stage device time of the last run (CUDA events on the engine stream), milliseconds.
@@ -116,6 +122,8 @@ struct StageTimes {
     uint64_t launches = 0;   // kernels this engine launched during the run
     uint64_t expand_launches = 0;
     uint64_t walk_launches = 0;      // lane-kernel launches that used the lane-parallel walk
+    uint64_t result_streamed = 0;    // 1: the result was copied out range by range during the run
+    uint64_t result_chunks = 0;      // its chunks
     // lane-per-child expand kernel (k_expand<true>)
     uint64_t expand_bytes = 0;       // per-stage algorithmic bytes
     uint64_t expand_hbm_bytes = 0;   // bytes the fused kernel must move to/from HBM

@@ -2161,13 +2161,13 @@ __global__ void k_fin_records_multi(DevPtrs P, const uint32_t* sids, uint32_t n,
         const uint32_t s = sids[i], k = seg_of(sb, K, i);
         const uint32_t e0 = eoff[i] - eoff[sb[k]], v0 = voff[i] - voff[sb[k]];
         uint32_t* oids = sec_ptr<uint32_t>(stage, sec, k, 9);
-        uint32_t* oar = sec_ptr<uint32_t>(stage, sec, k, 10);
+        uint8_t* oar = sec_ptr<uint8_t>(stage, sec, k, 10);
         uint32_t* overts = sec_ptr<uint32_t>(stage, sec, k, 12);
         const uint32_t ne = P.st_ne[s], nocc = P.st_nocc[s], aw = (ne + 3) >> 2;
         const uint32_t* rec = P.arena + P.st_off[s];
         for (uint32_t t = lane; t < ne; t += 32) {
             if (with_ids) oids[e0 + t] = rec[t];
-            oar[e0 + t] = (rec[ne + (t >> 2)] >> ((t & 3u) * 8u)) & 0xFFu;
+            oar[e0 + t] = static_cast<uint8_t>(rec[ne + (t >> 2)] >> ((t & 3u) * 8u));
         }
         for (uint32_t t = lane; t < nocc; t += 32) overts[v0 + t] = rec[ne + aw + t];
     }
@@ -2644,51 +2644,102 @@ __global__ void __launch_bounds__(256, 4) k_materialize(DevPtrs P, LevelArgs A, 
 
 // Branchial pairs (CausalGraph::record_branchial_overlaps, hypergraph/src/causal_graph.cpp:324-350):
 // two kept events of the same input state that consumed a common edge, each unordered pair once
-// as (a, b), a < b. One thread per event a of the level: the events of one input state are
-// contiguous (they are numbered in frontier order), so a walks its successors until the input
-// state changes. Pass 0 counts a's pairs into bcount[t]; pass 1 writes them at the scanned offset
+// as (a, b), a < b. The events of one input state are contiguous (they are numbered in frontier
+// order). Pass 0 counts a's pairs into bcount[t]; pass 1 writes them at the scanned offset
 // boff[t] in (a, then b) order.
+//
+// One event a (level index t) walking its successors until the input state changes: the form for
+// states whose events carry no position masks (parents past 63 edges; the test compares edge ids).
+template <bool kEmit>
+__device__ void bpairs_walk(const DevPtrs& P, const LevelArgs& A, uint32_t t) {
+    const uint32_t a = A.ev_base + t;
+    const uint32_t end = A.ev_base + A.n_events;
+    uint32_t cnt = 0;
+    if (P.ev_kept[a]) {
+        const uint32_t in = P.ev_in[a];
+        const uint32_t na = P.rules[P.ev_rule[a]].n_lhs, ca0 = P.ev_coff[a];
+        const unsigned long long ma = P.ev_bmask[a];
+        uint32_t ca[kMaxPatternEdges];   // edge ids, for parents past the mask's 63 positions
+        bool have_ca = false;
+        uint32_t out = kEmit ? A.boff[t] : 0u;
+        for (uint32_t c = a + 1; c < end && P.ev_in[c] == in; ++c) {
+            const unsigned long long mc = P.ev_bmask[c];
+            bool share = false;
+            if (ma && mc) {
+                // a consumed parent position in common (never with a dropped event's mask)
+                share = (ma & mc) != 0ull;
+            } else if (P.ev_kept[c]) {
+                if (!have_ca) {
+                    for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[ca0 + k];
+                    have_ca = true;
+                }
+                const uint32_t nc = P.rules[P.ev_rule[c]].n_lhs, cc0 = P.ev_coff[c];
+                for (uint32_t k = 0; k < nc && !share; ++k) {
+                    const uint32_t x = P.ev_cons[cc0 + k];
+                    for (uint32_t m = 0; m < na; ++m) share |= (ca[m] == x);
+                }
+            }
+            if (!share) continue;
+            if (kEmit) {
+                A.bpairs[2ull * out] = a;
+                A.bpairs[2ull * out + 1] = c;
+                ++out;
+            }
+            ++cnt;
+        }
+    }
+    if (!kEmit) A.bcount[t] = cnt;
+}
+
+// Thread per event of the level whose parent carries no position masks (more than 63 edges; then
+// none of its events has one): the per-event walk. The other events are k_bpairs'.
+template <bool kEmit>
+__global__ void k_bpairs_walk(DevPtrs P, LevelArgs A) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events; t += gridDim.x * blockDim.x)
+        if (P.ev_bmask[A.ev_base + t] == 0ull) bpairs_walk<kEmit>(P, A, t);
+}
+
+// Warp per input state (frontier position f, events [item_ev[f R], item_ev[(f+1) R]) of the
+// level) whose events carry position masks (a parent of at most 63 edges; a dropped event carries
+// kMaskDropped): lane i holds the mask of event i of a 32-event tile and takes the masks of the
+// later events from the other lanes by shuffles, so every pair test is one AND of registers.
 template <bool kEmit>
 __global__ void k_bpairs(DevPtrs P, LevelArgs A) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
-         t += gridDim.x * blockDim.x) {
-        const uint32_t a = A.ev_base + t;
-        const uint32_t end = A.ev_base + A.n_events;
-        uint32_t cnt = 0;
-        if (P.ev_kept[a]) {
-            const uint32_t in = P.ev_in[a];
-            const uint32_t na = P.rules[P.ev_rule[a]].n_lhs, ca0 = P.ev_coff[a];
-            const unsigned long long ma = P.ev_bmask[a];
-            uint32_t ca[kMaxPatternEdges];   // edge ids, for parents past the mask's 63 positions
-            bool have_ca = false;
-            uint32_t out = kEmit ? A.boff[t] : 0u;
-            for (uint32_t c = a + 1; c < end && P.ev_in[c] == in; ++c) {
-                const unsigned long long mc = P.ev_bmask[c];
-                bool share = false;
-                if (ma && mc) {
-                    // a consumed parent position in common (never with a dropped event's mask)
-                    share = (ma & mc) != 0ull;
-                } else if (P.ev_kept[c]) {
-                    if (!have_ca) {
-                        for (uint32_t k = 0; k < na; ++k) ca[k] = P.ev_cons[ca0 + k];
-                        have_ca = true;
-                    }
-                    const uint32_t nc = P.rules[P.ev_rule[c]].n_lhs, cc0 = P.ev_coff[c];
-                    for (uint32_t k = 0; k < nc && !share; ++k) {
-                        const uint32_t x = P.ev_cons[cc0 + k];
-                        for (uint32_t m = 0; m < na; ++m) share |= (ca[m] == x);
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t R = A.rules_stride;
+    for (uint32_t f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); f < A.n_frontier; f += warps) {
+        const uint32_t g0 = A.item_ev[f * R];
+        const uint32_t g1 = min(A.item_ev[(f + 1) * R], A.n_events);
+        if (g1 <= g0) continue;
+        const uint32_t k = g1 - g0;
+        const uint32_t e0 = A.ev_base + g0;
+        if (P.ev_bmask[e0] == 0ull) continue;   // no masks: k_bpairs_walk's
+        for (uint32_t t0 = 0; t0 < k; t0 += 32) {
+            const uint32_t i = t0 + lane;
+            const bool mine = i < k;
+            // a dropped event pairs with nothing
+            const unsigned long long ma = (mine && P.ev_kept[e0 + i]) ? P.ev_bmask[e0 + i] : 0ull;
+            uint32_t cnt = 0;
+            uint32_t out = (kEmit && mine) ? A.boff[g0 + i] : 0u;
+            for (uint32_t c0 = t0; c0 < k; c0 += 32) {
+                const uint32_t ic = c0 + lane;
+                const unsigned long long mine_c = ic < k ? P.ev_bmask[e0 + ic] : 0ull;
+                const uint32_t jn = min(32u, k - c0);
+                for (uint32_t j = 0; j < jn; ++j) {
+                    const unsigned long long mc = __shfl_sync(0xFFFFFFFFu, mine_c, j);
+                    if (c0 + j > i && (ma & mc) != 0ull) {
+                        if (kEmit) {
+                            A.bpairs[2ull * out] = e0 + i;
+                            A.bpairs[2ull * out + 1] = e0 + c0 + j;
+                            ++out;
+                        }
+                        ++cnt;
                     }
                 }
-                if (!share) continue;
-                if (kEmit) {
-                    A.bpairs[2ull * out] = a;
-                    A.bpairs[2ull * out + 1] = c;
-                    ++out;
-                }
-                ++cnt;
             }
+            if (!kEmit && mine) A.bcount[g0 + i] = cnt;
         }
-        if (!kEmit) A.bcount[t] = cnt;
     }
 }
 
@@ -2713,11 +2764,12 @@ __global__ void k_fin_events(DevPtrs P, uint32_t roots, uint32_t n, uint32_t rul
     }
 }
 
-// Causal triples per event: pass 0 counts (into cnt[i]), pass 1 writes at the scanned offsets.
-__global__ void k_fin_causal(DevPtrs P, uint32_t roots, uint32_t n, uint32_t* cnt,
+// Causal triples of events first + i (i < n): pass 0 counts (into cnt[i]), pass 1 writes at the
+// scanned offsets. Event ids are local (minus roots).
+__global__ void k_fin_causal(DevPtrs P, uint32_t roots, uint32_t first, uint32_t n, uint32_t* cnt,
                              const uint32_t* off, uint32_t* out, int pass) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t e = roots + i;
+        const uint32_t e = first + i;
         const uint32_t co = P.ev_coff[e], k = P.rules[P.ev_rule[e]].n_lhs;
         uint32_t w = pass ? off[i] : 0u;
         for (uint32_t j = 0; j < k; ++j) {
@@ -2725,7 +2777,7 @@ __global__ void k_fin_causal(DevPtrs P, uint32_t roots, uint32_t n, uint32_t* cn
             if (p == kNone) continue;
             if (pass) {
                 out[3 * w] = p - roots;
-                out[3 * w + 1] = i;
+                out[3 * w + 1] = e - roots;
                 out[3 * w + 2] = P.ev_cons[co + j];
             }
             ++w;
@@ -2740,20 +2792,64 @@ __global__ void k_fin_shift(const uint32_t* in, uint64_t n, uint32_t sub, uint32
         out[i] = in[i] - sub;
 }
 
-// Warp per state: its record's edge ids, arities and vertices at the scanned CSR offsets.
-__global__ void k_fin_states(DevPtrs P, uint32_t n, const uint32_t* eoff, const uint32_t* voff,
-                             uint32_t* ids, uint32_t* ar, uint32_t* verts) {
+// Warp per state s0 + s (s < n): its record's edge ids, arities and vertices at the scanned CSR
+// offsets eoff[s] / voff[s].
+__global__ void k_fin_states(DevPtrs P, uint32_t s0, uint32_t n, const uint32_t* eoff,
+                             const uint32_t* voff, uint32_t* ids, uint8_t* ar, uint32_t* verts) {
     const uint32_t lane = lane_id();
     for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < n;
          s += (gridDim.x * blockDim.x) >> 5) {
-        const uint32_t ne = P.st_ne[s], nocc = P.st_nocc[s], aw = (ne + 3) >> 2;
-        const uint32_t* rec = P.arena + P.st_off[s];
+        const uint32_t ne = P.st_ne[s0 + s], nocc = P.st_nocc[s0 + s], aw = (ne + 3) >> 2;
+        const uint32_t* rec = P.arena + P.st_off[s0 + s];
         const uint32_t e0 = eoff[s], v0 = voff[s];
         for (uint32_t i = lane; i < ne; i += 32) {
             if (ids) ids[e0 + i] = rec[i];   // null: the ids are not part of the result
-            ar[e0 + i] = (rec[ne + (i >> 2)] >> ((i & 3u) * 8u)) & 0xFFu;
+            ar[e0 + i] = static_cast<uint8_t>(rec[ne + (i >> 2)] >> ((i & 3u) * 8u));
         }
         for (uint32_t j = lane; j < nocc; j += 32) verts[v0 + j] = rec[ne + aw + j];
+    }
+}
+
+// Byte copy by the SMs (device to device, or device to page-locked host memory): copies the
+// engine stream makes this way never queue on a copy engine behind the result copies of the copy
+// stream. 16-byte words when both ends are 16-byte aligned, else bytes.
+__global__ void k_copy_bytes(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, uint64_t n) {
+    const uint64_t t = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0) {
+        const uint64_t w = n / 16;
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        uint4* d4 = reinterpret_cast<uint4*>(dst);
+        for (uint64_t i = t; i < w; i += stride) d4[i] = s4[i];
+        for (uint64_t i = w * 16 + t; i < n; i += stride) dst[i] = src[i];
+    } else {
+        for (uint64_t i = t; i < n; i += stride) dst[i] = src[i];
+    }
+}
+
+// Streamed result: the consumed lists of events first + i (i < n), contiguous from the first
+// one's, into out; the thread of the last event writes the chunk's consumed count to *count.
+__global__ void k_fin_cons_chunk(DevPtrs P, uint32_t first, uint32_t n, uint32_t* out, uint32_t* count) {
+    const uint32_t base = P.ev_coff[first];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t e = first + i;
+        const uint32_t co = P.ev_coff[e], k = P.rules[P.ev_rule[e]].n_lhs;
+        for (uint32_t j = 0; j < k; ++j) out[co - base + j] = P.ev_cons[co + j];
+        if (i + 1 == n) *count = co + k - base;
+    }
+}
+
+// Streamed result: adds the running total tot[w] to the n chunk-local offsets a[0..n).
+__global__ void k_fin_rebase(uint32_t* a, uint32_t n, const uint32_t* tot, uint32_t w) {
+    const uint32_t base = tot[w];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        a[i] += base;
+}
+// Streamed result: records a chunk's total (sizes[w]) and advances the running total tot[w].
+__global__ void k_fin_advance(const uint32_t* chunk_total, uint32_t* tot, uint32_t* sizes, uint32_t w) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sizes[w] = *chunk_total;
+        tot[w] += *chunk_total;
     }
 }
 

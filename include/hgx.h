@@ -119,7 +119,14 @@ typedef enum hgx_option {
        ids (HGX_ARR_STATE_EDGE_IDS); 0 = arities and vertices only, HGX_ARR_STATE_EDGE_IDS empty.
        The reference's results carry the ids only under EvolveInput::edge_identity
        (gpu/include/hg_gpu/evolve.hpp:36, default false); the hg_gpu shim maps it here. */
-    HGX_OPT_KEEP_STATE_EDGE_IDS = 15
+    HGX_OPT_KEEP_STATE_EDGE_IDS = 15,
+    /* Result of a single evolution (hgx_evolve with readback): 1 (default) = when the engine's
+       previous result was at least 64 MB, each finished frontier range's share of the result
+       arrays is finalised and copied to the host while the later ranges compute (the copies
+       overlap the evolution; page-locked blocks are sized from that previous result, and a result
+       that outgrows them is copied whole at the end); 2 = the same for results of any size; 0 =
+       the whole result is copied after the last level. Identical results. The reference reads its result back after the last step (gpu/src/evolve.cu:489-496). */
+    HGX_OPT_STREAM_RESULT = 16
 } hgx_option;
 
 /* One evolution of a batch or a served request. */
@@ -162,7 +169,7 @@ typedef enum hgx_array {
     HGX_ARR_EVENT_PROD = 7,      /* [u32 x EVENTS*2] (first produced edge id, count) */
     HGX_ARR_STATE_EDGE_OFF = 8,  /* [u32 x STATES+1] (needs HGX_OPT_KEEP_STATE_EDGES) */
     HGX_ARR_STATE_EDGE_IDS = 9,  /* [u32 x STATE_EDGES] (empty under HGX_OPT_KEEP_STATE_EDGE_IDS = 0) */
-    HGX_ARR_STATE_ARITY = 10,    /* [u32 x STATE_EDGES] */
+    HGX_ARR_STATE_ARITY = 10,    /* [u8 x STATE_EDGES] (arity <= 16) */
     HGX_ARR_STATE_VERT_OFF = 11, /* [u32 x STATES+1] */
     HGX_ARR_STATE_VERTS = 12,    /* [u32 x STATE_VERTS] */
     HGX_ARR_EVENT_SIG = 13       /* [u64 x EVENTS] event signature (hg_gpu::Event::signature);
@@ -259,6 +266,10 @@ HGX_API hgx_status hgx_engine_stage_times(hgx_engine* engine, double* out_ms, ui
    the same first four figures; out[9] its total device time in nanoseconds; out[10] lane-kernel
    launches that ran the lane-parallel walk (the join autotuner's choice; out has 11 entries). */
 HGX_API hgx_status hgx_engine_expand_stats(hgx_engine* engine, uint64_t* out);
+
+/* The last evolve call's result: out[0] = 1 if it was streamed (copied to the host range by
+   range while the run continued, HGX_OPT_STREAM_RESULT), out[1] = the chunks copied. */
+HGX_API hgx_status hgx_engine_result_stats(hgx_engine* engine, uint64_t* out);
 
 /* The CUDA stream (cudaStream_t) the engine launches on, for callers that time or order
    work against it. */

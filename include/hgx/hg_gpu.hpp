@@ -300,7 +300,7 @@ inline EvolveResult convert(const hgx_result* rr, const EvolveInput& in) {
     auto hash = copy_array<uint64_t>(rr, HGX_ARR_STATE_HASH);
     auto eoff = copy_array<uint32_t>(rr, HGX_ARR_STATE_EDGE_OFF);
     auto eids = copy_array<uint32_t>(rr, HGX_ARR_STATE_EDGE_IDS);
-    auto ar = copy_array<uint32_t>(rr, HGX_ARR_STATE_ARITY);
+    auto ar = copy_array<uint8_t>(rr, HGX_ARR_STATE_ARITY);
     auto voff = copy_array<uint32_t>(rr, HGX_ARR_STATE_VERT_OFF);
     auto verts = copy_array<uint32_t>(rr, HGX_ARR_STATE_VERTS);
     out.states.resize(hash.size());

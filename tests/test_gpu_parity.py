@@ -317,3 +317,61 @@ def test_state_edge_ids_optional(engine):
             assert np.array_equal(getattr(a, f), getattr(b, f)), f
         assert all(a.state_edges(s) == b.state_edges(s) for s in range(0, a.num_states, 97))
         assert b.bytes() < a.bytes()
+
+
+_RESULT_FIELDS = ("state_hash", "state_depth", "events", "causal", "branchial", "event_cons_off",
+                  "event_cons", "event_prod", "state_edge_off", "state_edge_ids", "state_arity",
+                  "state_vert_off", "state_verts")
+
+
+def test_streamed_result_matches_whole(engine):
+    """A single evolution's result copied out range by range while the run continues
+    (HGX_OPT_STREAM_RESULT) is array for array the result copied whole after the run: capped
+    (the cut level split into parts) and uncapped, quotient and full multiway, with each record
+    option off in turn. The second streamed call of each runs with the room the first left."""
+    import numpy as np
+    from hypergraphrewritingengine_b200 import api
+    cases_ = [
+        (W.config2(8), {}),
+        (W.config2(6), {}),
+        (W.Evolution(rules=[cases.C2_RULE], roots=[cases.C2_INIT], steps=7, max_states=26_700), {}),
+        (W.config3(5), {}),
+        (W.Evolution(rules=[cases.C1_RULE], roots=[cases.C1_INIT], steps=5, quotient=False), {}),
+        (W.Evolution(rules=[([[0, 1], [0, 1], [1, 2]], [[0, 1], [1, 2], [1, 2], [2, 3]])],
+                     roots=[[[1, 2]] * 4 + [[2, 3]] * 3 + [[2, 2], [3, 1]]], steps=4, max_states=20_000,
+                     name="twin-pairs"), {}),
+        (W.config2(6), {api.OPT_RECORD_CAUSAL: 0}),
+        (W.config2(6), {api.OPT_RECORD_BRANCHIAL: 0}),
+        (W.config2(6), {api.OPT_KEEP_STATE_EDGE_IDS: 0}),
+        (W.config2(6), {api.OPT_KEEP_STATE_EDGES: 0}),
+        (W.Evolution(rules=[cases.C2_RULE], roots=[cases.C2_INIT], steps=0), {}),
+    ]
+    defaults = {api.OPT_RECORD_CAUSAL: 1, api.OPT_RECORD_BRANCHIAL: 1, api.OPT_KEEP_STATE_EDGE_IDS: 1,
+                api.OPT_KEEP_STATE_EDGES: 1}
+    streamed_any = 0
+    try:
+        for ev, opts in cases_:
+            for k, v in opts.items():
+                engine.set_option(k, v)
+            engine.set_option(api.OPT_STREAM_RESULT, 0)
+            whole = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient, max_states=ev.max_states)
+            assert not engine.result_stats()["streamed"]
+            engine.set_option(api.OPT_STREAM_RESULT, 2)   # whatever the result's size
+            for rep in range(2):
+                res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient, max_states=ev.max_states)
+                st = engine.result_stats()
+                streamed_any += st["streamed"]
+                if rep == 1 and ev.steps > 0:
+                    assert st["streamed"], f"{ev.name} {opts}: second call not streamed"
+                for f in _RESULT_FIELDS:
+                    a, b = getattr(res, f), getattr(whole, f)
+                    assert a.dtype == b.dtype and np.array_equal(a, b), f"{ev.name} {opts} rep {rep}: {f}"
+                assert (res.num_states, res.num_events, res.num_classes, res.truncated) == \
+                    (whole.num_states, whole.num_events, whole.num_classes, whole.truncated)
+            for k in opts:
+                engine.set_option(k, defaults[k])
+        assert streamed_any >= 10
+    finally:
+        engine.set_option(api.OPT_STREAM_RESULT, 1)
+        for k, v in defaults.items():
+            engine.set_option(k, v)
