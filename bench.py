@@ -702,7 +702,8 @@ def served_vs_plain(eng, n=400, rates=(100.0, 1000.0, 3000.0, 10000.0, float("in
     from hypergraphrewritingengine_b200.serve import Server, serve_plain, summarize
     out = {"workload": f"c5: {n} requests per rate, seed 0xC0FFEE, lognormal initial edges "
                        "(median 16, max 256), 2-8 steps, WL quotient, cap 4096 states; "
-                       "admission by estimated device bytes <= 140 GB",
+                       "admission by estimated device bytes <= 140 GB; per arm the shorter of "
+                       "two real-time runs",
            "rates": []}
     for rate in rates:
         stream = W.config5_stream(n, rate_per_s=rate if rate != float("inf") else 1e12,
@@ -713,8 +714,14 @@ def served_vs_plain(eng, n=400, rates=(100.0, 1000.0, 3000.0, 10000.0, float("in
         # page-locked result blocks reach their working sizes, as in a long-running server)
         Server(eng).run(stream, realtime=False, admit_per_step=len(stream))
         serve_plain(eng, stream, realtime=False)
-        served = Server(eng).run(stream, realtime=True)
-        plain = serve_plain(eng, stream, realtime=True)
+        # two real-time runs per arm, alternating; each arm's shorter makespan is kept (the first
+        # real-time run of a process can stall on one-off host allocations)
+        runs_s, runs_p = [], []
+        for _ in range(2):
+            runs_s.append(Server(eng).run(stream, realtime=True))
+            runs_p.append(serve_plain(eng, stream, realtime=True))
+        served = min(runs_s, key=lambda r: summarize(r)["makespan_ms"])
+        plain = min(runs_p, key=lambda r: summarize(r)["makespan_ms"])
         same = all(a.result.num_classes == b.result.num_classes and a.result.same_as(b.result)
                    for a, b in zip(served, plain))
         ss, sp = summarize(served), summarize(plain)

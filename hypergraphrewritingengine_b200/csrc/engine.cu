@@ -5,7 +5,9 @@
 
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <numeric>
 
 #include "../../include/hgx.h"
@@ -1060,6 +1062,20 @@ struct Engine::Impl {
         return static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(g, kNumSMs * 16)));
     }
 
+    // Resident blocks per SM of a kernel at a block size and shared-memory size (the driver's
+    // occupancy answer, kept: a level asks the same few questions again).
+    std::map<std::tuple<const void*, uint32_t, uint32_t>, int> occ_cache;
+    int occupancy(const void* kernel, uint32_t block, uint32_t smem) {
+        const auto key = std::make_tuple(kernel, block, smem);
+        const auto it = occ_cache.find(key);
+        if (it != occ_cache.end()) return it->second;
+        int bps = 0;
+        HGX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, block, smem));
+        bps = std::max(bps, 1);
+        occ_cache.emplace(key, bps);
+        return bps;
+    }
+
     template <class K>
     LaunchShape warp_shape(K kernel, const Layout& L, uint64_t items) {
         if (L.bytes > kMaxDynSmem)
@@ -1069,9 +1085,7 @@ struct Engine::Impl {
         LaunchShape s;
         s.block = 32 * wpb;
         s.smem = L.bytes * wpb;
-        int bps = 0;
-        HGX_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, s.block, s.smem));
-        bps = std::max(bps, 1);
+        int bps = occupancy(reinterpret_cast<const void*>(kernel), s.block, s.smem);
         const uint64_t want = (items + wpb - 1) / wpb;
         s.grid = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(want, uint64_t(kNumSMs) * bps)));
         return s;
