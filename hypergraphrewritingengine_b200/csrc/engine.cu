@@ -434,7 +434,7 @@ struct Engine::Impl {
     DVec<uint32_t> state_of_arrival;
     DVec<unsigned long long> tab_keys;
     DVec<uint32_t> tab_vals;
-    DVec<unsigned long long> evo_classes, evo_states;
+    DVec<unsigned long long> evo_classes, evo_states, evo_causal;
     DVec<uint32_t> evo_cut, evo_first_ev, evo_last_ev, evo_stopped;
     DVec<uint32_t> err;
     // level temporaries
@@ -905,6 +905,7 @@ struct Engine::Impl {
         arena_top.release(st);
         tab_keys.release(st);
         evo_classes.release(st);
+        evo_causal.release(st);
         evo_states.release(st);
         stats.release(st);
         totals.release(st);
@@ -1005,6 +1006,7 @@ struct Engine::Impl {
         P.tab_keys = tab_keys.p;
         P.tab_vals = tab_vals.p;
         P.evo_classes = evo_classes.p;
+        P.evo_causal = evo_causal.p;
         P.evo_states = evo_states.p;
         P.evo_cut = evo_cut.p;
         P.evo_first_ev = evo_first_ev.p;
@@ -1263,6 +1265,8 @@ struct Engine::Impl {
         evos.ensure(nevo, evo0, st);
         HGX_CUDA_CHECK(cudaMemcpyAsync(evos.p + evo0, &h_evos[evo0], nnew * sizeof(DevEvo), cudaMemcpyHostToDevice, st));
         evo_classes.ensure(nevo, evo0, st);
+        evo_causal.ensure(nevo, evo0, st);
+        HGX_CUDA_CHECK(cudaMemsetAsync(evo_causal.p + evo0, 0, nnew * sizeof(unsigned long long), st));
         evo_states.ensure(nevo, evo0, st);
         evo_sigs.ensure(nevo, evo0, st);
         HGX_CUDA_CHECK(cudaMemsetAsync(evo_sigs.p + evo0, 0, nnew * sizeof(unsigned long long), st));
@@ -1702,23 +1706,16 @@ struct Engine::Impl {
     // this scratch instead of the result.
 
     // Counts only (results stay on the device): events and branchial pairs from the recorded
-    // per-evolution ranges, states and classes from the device counters, causal triples by one
-    // pass over the events.
+    // per-evolution ranges; states, classes and causal triples from the device counters (the
+    // causal ones counted level by level in k_outstate).
     void read_counts(const std::vector<uint32_t>& which, std::vector<EvolutionResult>& out,
                      bool signatures) {
         const size_t nevo = h_evos.size();
-        totals.ensure(nevo, 0, st);
-        HGX_CUDA_CHECK(cudaMemsetAsync(totals.p, 0, nevo * sizeof(unsigned long long), st));
-        if (n_events) {
-            k_evo_causal<<<grid_for(n_events, 256), 256, 0, st>>>(ptrs(), static_cast<uint32_t>(n_events),
-                                                                  totals.p);
-            check_launch();
-        }
         std::vector<unsigned long long> causal(nevo), cls(nevo), sts(nevo), sig(nevo, 0);
         std::vector<uint32_t> stop(nevo);
         if (signatures)
             HGX_CUDA_CHECK(cudaMemcpyAsync(sig.data(), evo_sigs.p, nevo * 8, cudaMemcpyDeviceToHost, st));
-        HGX_CUDA_CHECK(cudaMemcpyAsync(causal.data(), totals.p, nevo * 8, cudaMemcpyDeviceToHost, st));
+        HGX_CUDA_CHECK(cudaMemcpyAsync(causal.data(), evo_causal.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(cls.data(), evo_classes.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(sts.data(), evo_states.p, nevo * 8, cudaMemcpyDeviceToHost, st));
         HGX_CUDA_CHECK(cudaMemcpyAsync(stop.data(), evo_stopped.p, nevo * 4, cudaMemcpyDeviceToHost, st));

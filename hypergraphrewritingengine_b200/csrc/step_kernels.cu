@@ -654,6 +654,50 @@ __device__ uint32_t lane_walk(const Layout& L, const char* sm, const DevRule& R,
     const uint16_t* pevo = smp<uint16_t>(const_cast<char*>(sm), L.o_pevo);
     const uint16_t* vloc = smp<uint16_t>(const_cast<char*>(sm), L.o_vloc);
     const uint32_t n = R.n_lhs;
+    if (n == 2) {
+        // two pattern edges: bind the first at e0, then every second edge in ascending order
+        // (the same matches in the same order as the depth-first walk below)
+        const uint32_t p0 = R.sched[0], p1 = R.sched[1];
+        const uint32_t a0 = R.lhs_ar[p0], a1 = R.lhs_ar[p1];
+        if (pear[e0] != a0) return 0;
+        uint16_t bind[kMaxVars];
+        uint32_t bound = 0;
+        const uint8_t* v0 = &R.lhs_vars[R.lhs_off[p0]];
+        const uint8_t* v1 = &R.lhs_vars[R.lhs_off[p1]];
+        const uint32_t vo0 = pevo[e0];
+        for (uint32_t q = 0; q < a0; ++q) {
+            const uint32_t var = v0[q];
+            const uint16_t x = vloc[vo0 + q];
+            if ((bound >> var) & 1u) {
+                if (bind[var] != x) return 0;
+            } else {
+                bind[var] = x;
+                bound |= 1u << var;
+            }
+        }
+        uint32_t found = 0;
+        const uint32_t jend = min(pa.ne, j1_hi);
+        for (uint32_t j = j1_lo; j < jend; ++j) {
+            if (j == e0 || pear[j] != a1) continue;
+            const uint32_t vo = pevo[j];
+            uint32_t nb = 0;
+            bool ok = true;
+            for (uint32_t q = 0; q < a1 && ok; ++q) {
+                const uint32_t var = v1[q];
+                const uint16_t x = vloc[vo + q];
+                if (((bound | nb) >> var) & 1u) {
+                    ok = bind[var] == x;
+                } else {
+                    bind[var] = x;
+                    nb |= 1u << var;
+                }
+            }
+            if (!ok) continue;
+            on_match((e0 << (8u * p0)) | (j << (8u * p1)));
+            ++found;
+        }
+        return found;
+    }
     uint16_t bind[kMaxVars];
     uint32_t bound = 0;
     uint32_t newly[kLaneJoinLhs];
@@ -1730,32 +1774,6 @@ __global__ void k_tr(DevPtrs P, uint32_t ev_base, uint32_t n) {
     }
 }
 
-// Causal triples per evolution without reading the result back: kept events whose consumed
-// edges have a producer. out[evo] += count (warp-aggregated per evolution).
-__global__ void k_evo_causal(DevPtrs P, uint32_t n_events, unsigned long long* out) {
-    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-    for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < n_events; t0 += stride) {
-        const uint64_t e = t0 + threadIdx.x;
-        uint32_t evo = 0, nc = 0;
-        if (e < n_events && P.ev_in[e] != kNone && P.ev_kept[e]) {
-            evo = P.st_evo[P.ev_in[e]];
-            const DevRule& R = P.rules[P.ev_rule[e]];
-            const uint32_t co = P.ev_coff[e];
-            for (uint32_t k = 0; k < R.n_lhs; ++k) nc += P.ev_cprod[co + k] != kNone ? 1u : 0u;
-        }
-        const bool live = nc != 0;
-        const uint32_t act = __ballot_sync(0xFFFFFFFFu, live);
-        if (live) {
-            const uint32_t peers = __match_any_sync(act, evo);
-            uint32_t sum = nc;
-            // sum nc over the peers (same evolution) -- lanes of one warp, tiny loop
-            for (uint32_t m = peers & ~(1u << lane_id()); m; m &= m - 1)
-                sum += __shfl_sync(peers, nc, __ffs(m) - 1);
-            if (lane_id() == static_cast<uint32_t>(__ffs(peers) - 1))
-                atomicAdd(&out[evo], static_cast<unsigned long long>(sum));
-        }
-    }
-}
 
 
 
@@ -2436,19 +2454,40 @@ __global__ void k_assign(DevPtrs P, LevelArgs A) {
     }
 }
 
+// Also counts each evolution's causal triples (the kept events' consumed edges that have a
+// producer; the level's producers are final here, after k_cprod and k_tr).
 __global__ void k_outstate(DevPtrs P, LevelArgs A) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < A.n_events;
-         t += gridDim.x * blockDim.x) {
-        const uint32_t e = A.ev_base + t;
-        if (!P.ev_kept[e]) { P.ev_out[e] = kNone; continue; }
-        const uint32_t evo = P.st_evo[P.ev_in[e]];
-        const bool rep = A.flag_rep[t + 1] != A.flag_rep[t];
-        if (rep || !P.evos[evo].quotient) {
-            P.ev_out[e] = P.state_of_arrival[e];
-        } else {
-            const uint32_t w = P.ev_out[e];
-            if (w == kNone) { atomicOr(P.err, kErrTableFull); P.ev_out[e] = kNone; }
-            else P.ev_out[e] = P.state_of_arrival[w];
+    for (uint32_t t0 = blockIdx.x * blockDim.x; t0 < A.n_events; t0 += gridDim.x * blockDim.x) {
+        const uint32_t t = t0 + threadIdx.x;
+        uint32_t evo = 0, nc = 0;
+        if (t < A.n_events) {
+            const uint32_t e = A.ev_base + t;
+            if (!P.ev_kept[e]) {
+                P.ev_out[e] = kNone;
+            } else {
+                evo = P.st_evo[P.ev_in[e]];
+                const bool rep = A.flag_rep[t + 1] != A.flag_rep[t];
+                if (rep || !P.evos[evo].quotient) {
+                    P.ev_out[e] = P.state_of_arrival[e];
+                } else {
+                    const uint32_t w = P.ev_out[e];
+                    if (w == kNone) { atomicOr(P.err, kErrTableFull); P.ev_out[e] = kNone; }
+                    else P.ev_out[e] = P.state_of_arrival[w];
+                }
+                const uint32_t co = P.ev_coff[e], k = P.rules[P.ev_rule[e]].n_lhs;
+                for (uint32_t i = 0; i < k; ++i) nc += P.ev_cprod[co + i] != kNone ? 1u : 0u;
+            }
+        }
+        // per evolution, one atomic per warp
+        const bool live = nc != 0;
+        const uint32_t act = __ballot_sync(0xFFFFFFFFu, live);
+        if (live) {
+            const uint32_t peers = __match_any_sync(act, evo);
+            uint32_t sum = nc;
+            for (uint32_t m = peers & ~(1u << lane_id()); m; m &= m - 1)
+                sum += __shfl_sync(peers, nc, __ffs(m) - 1);
+            if (lane_id() == static_cast<uint32_t>(__ffs(peers) - 1))
+                atomicAdd(&P.evo_causal[evo], static_cast<unsigned long long>(sum));
         }
     }
 }
@@ -2680,11 +2719,7 @@ __device__ void bpairs_walk(const DevPtrs& P, const LevelArgs& A, uint32_t t) {
                 }
             }
             if (!share) continue;
-            if (kEmit) {
-                A.bpairs[2ull * out] = a;
-                A.bpairs[2ull * out + 1] = c;
-                ++out;
-            }
+            if (kEmit) reinterpret_cast<uint2*>(A.bpairs)[out++] = make_uint2(a, c);
             ++cnt;
         }
     }
@@ -2729,11 +2764,7 @@ __global__ void k_bpairs(DevPtrs P, LevelArgs A) {
                 for (uint32_t j = 0; j < jn; ++j) {
                     const unsigned long long mc = __shfl_sync(0xFFFFFFFFu, mine_c, j);
                     if (c0 + j > i && (ma & mc) != 0ull) {
-                        if (kEmit) {
-                            A.bpairs[2ull * out] = e0 + i;
-                            A.bpairs[2ull * out + 1] = e0 + c0 + j;
-                            ++out;
-                        }
+                        if (kEmit) reinterpret_cast<uint2*>(A.bpairs)[out++] = make_uint2(e0 + i, e0 + c0 + j);
                         ++cnt;
                     }
                 }

@@ -58,6 +58,7 @@ struct DevPtrs {
     uint32_t* tab_vals;
     // per-evolution counters
     unsigned long long* evo_classes;   // WL classes seen so far
+    unsigned long long* evo_causal;    // causal triples of the kept events so far
     unsigned long long* evo_states;    // states recorded so far
     uint32_t* evo_cut;                 // first event cut off by the cap this level (kNone = none)
     uint32_t* evo_first_ev;            // first event of the evolution in this level

@@ -375,3 +375,39 @@ def test_streamed_result_matches_whole(engine):
         engine.set_option(api.OPT_STREAM_RESULT, 1)
         for k, v in defaults.items():
             engine.set_option(k, v)
+
+
+def test_counts_only_causal_matches_result(engine):
+    """The causal triples counted on the device level by level (results left on the device)
+    equal the triples of the result read back: quotient and full multiway, capped, with and
+    without transitive reduction, alone and batched."""
+    from hypergraphrewritingengine_b200 import api
+    evs = [W.config2(6), W.config3(5), W.config1(),
+           W.Evolution(rules=[cases.C2_RULE], roots=[cases.C2_INIT], steps=7, max_states=26_700)]
+    try:
+        for tr in (0, 1):
+            engine.set_option(api.OPT_TRANSITIVE_REDUCTION, tr)
+            for ev in evs:
+                res = engine.evolve(ev.rules, ev.roots, ev.steps, quotient=ev.quotient, max_states=ev.max_states)
+                c = engine.counts(ev.rules, ev.roots, ev.steps, quotient=ev.quotient, max_states=ev.max_states)
+                assert c["causal"] == len(res.causal), (ev.name, tr)
+                assert c["events"] == res.num_events and c["branchial"] == len(res.branchial), (ev.name, tr)
+        engine.set_option(api.OPT_TRANSITIVE_REDUCTION, 0)
+        batch = W.config4(n=24, max_states=1024)
+        results = engine.evolve_batch(batch)
+        jobs, _keep = engine.make_jobs(batch)
+        outs = (api.ctypes.c_void_p * len(batch))()
+        engine.set_option(api.OPT_READBACK, 0)
+        try:
+            api._check(engine._L.hgx_evolve_batch(engine._h, jobs, len(batch), outs))
+        finally:
+            engine.set_option(api.OPT_READBACK, 1)
+        try:
+            for i, (ev, r) in enumerate(zip(batch, results)):
+                assert int(engine._L.hgx_result_count(outs[i], api.COUNT_CAUSAL)) == len(r.causal), ev.name
+                assert int(engine._L.hgx_result_count(outs[i], api.COUNT_EVENTS)) == r.num_events, ev.name
+        finally:
+            for i in range(len(batch)):
+                engine._L.hgx_result_free(outs[i])
+    finally:
+        engine.set_option(api.OPT_TRANSITIVE_REDUCTION, 0)
