@@ -2296,11 +2296,10 @@ struct Engine::Impl {
                 }
             }
             if (n_new) {
-                // lanes per state: the level's largest parent in one pass
-                if (fmax_ne <= 8)
+                // lanes per state: 8 up to 16-edge parents (four states per warp pass share its
+                // fixed cost; measured faster than 16 lanes and one pass), else 32
+                if (fmax_ne <= 16)   // 8-lane segments, two passes over a 9-16-edge parent
                     k_materialize<8><<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
-                else if (fmax_ne <= 16)
-                    k_materialize<16><<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
                 else
                     k_materialize<32><<<grid_for(n_new, 256), 256, 0, st>>>(ptrs(), A, n_new);
                 check_launch();
