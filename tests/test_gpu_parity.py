@@ -411,3 +411,28 @@ def test_counts_only_causal_matches_result(engine):
                 engine._L.hgx_result_free(outs[i])
     finally:
         engine.set_option(api.OPT_TRANSITIVE_REDUCTION, 0)
+
+
+def test_streamed_result_outgrowing_its_blocks(engine):
+    """A result larger than the page-locked blocks its engine's previous result sized is not
+    streamed: it is finalised whole after the run and equals the unstreamed result; the call
+    after it streams into blocks of its own size."""
+    import numpy as np
+    from hypergraphrewritingengine_b200 import api
+    small, big = W.config2(4), W.config2(6)
+    try:
+        engine.set_option(api.OPT_STREAM_RESULT, 0)
+        whole = engine.evolve(big.rules, big.roots, big.steps, quotient=True)
+        engine.set_option(api.OPT_STREAM_RESULT, 2)
+        engine.evolve(small.rules, small.roots, small.steps, quotient=True)
+        engine.evolve(small.rules, small.roots, small.steps, quotient=True)
+        assert engine.result_stats()["streamed"]
+        first = engine.evolve(big.rules, big.roots, big.steps, quotient=True)
+        assert not engine.result_stats()["streamed"]
+        second = engine.evolve(big.rules, big.roots, big.steps, quotient=True)
+        assert engine.result_stats()["streamed"]
+        for res in (first, second):
+            for f in _RESULT_FIELDS:
+                assert np.array_equal(getattr(res, f), getattr(whole, f)), f
+    finally:
+        engine.set_option(api.OPT_STREAM_RESULT, 1)
