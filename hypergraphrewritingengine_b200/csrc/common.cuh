@@ -31,8 +31,18 @@ constexpr int kMaxVars = 32;
 constexpr int kMaxSideVars = 64;   // total positions over one rule side (16 edges x 4 avg)
 
 // Lane-per-child WL: a parent with at most kLaneEMax edges whose children have at most
-// kLaneVMax vertices is expanded with one child per lane.
+// kLaneVMax vertices is expanded with one child per lane -- on a level whose frontier fills the
+// GPU with lane-kernel warps (kLaneFullStates states, one warp per parent in every warp slot of
+// 148 SMs x 4 blocks x 8 warps). A smaller level takes the lane path only for children of at
+// most kLaneVMaxSmall vertices: a lane's WL work grows with the square of the child's vertices,
+// and the warp-per-child path spreads a larger child over the lanes and a small level over more
+// warps (256 evolutions of the random batch, one per call: 439 -> 326 ms; the 1024-evolution
+// batch at cap 4,096: 118 -> 113 ms); on full levels the lane path stays faster (the batch at cap
+// 65,536: 628 ms either way, 805 ms with the lower limit on every level), and 9-vertex children
+// run 7x faster one per lane either way.
 constexpr int kLaneVMax = 32;
+constexpr int kLaneVMaxSmall = 12;
+constexpr uint32_t kLaneFullStates = 148 * 4 * 8;
 constexpr int kLaneEMax = 64;
 constexpr int kLaneNMax = 64;    // neighbour entries a lane sorts for one vertex
 

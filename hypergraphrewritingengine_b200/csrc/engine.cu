@@ -1875,6 +1875,7 @@ struct Engine::Impl {
         const bool fwd = opt.forwarding != 0;
         A.fwd_mode = opt.forwarding;
         A.ev_keys = opt.event_keys;
+        A.lane_vmax = F >= kLaneFullStates ? kLaneVMax : kLaneVMaxSmall;
         const Layout Lc = make_layout(ne_bound, nocc_bound, rm, LayoutKind::Count, fwd, kLaneJoinCap,
                                       opt.join_index != 0);
         fmode.ensure(F, 0, st);

@@ -1416,7 +1416,7 @@ __global__ void __launch_bounds__(256, 4) k_count(DevPtrs P, LevelArgs A, Layout
         build_join_index(L, sm, pa);
         const DevEvo ev = P.evos[P.st_evo[sid]];
         // lane-per-child eligibility: few enough vertices and a bounded neighbour count
-        bool lane_ok = pa.nvp <= kLaneVMax && pa.ne <= kLaneEMax && pa.ne > 0;
+        bool lane_ok = pa.nvp <= A.lane_vmax && pa.ne <= kLaneEMax && pa.ne > 0;
         uint32_t pnn_max = 0;
         if (lane_ok) {
             const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
@@ -1436,7 +1436,7 @@ __global__ void __launch_bounds__(256, 4) k_count(DevPtrs P, LevelArgs A, Layout
                 load_rule(sm, L, &P.rules[ev.rule_begin + r]);
                 uint32_t gain = 0;
                 for (uint32_t k = 0; k < R.n_rhs; ++k) gain += uint32_t(R.rhs_ar[k]) * (R.rhs_ar[k] - 1u);
-                lane_ok = lane_ok && pa.nvp + R.n_fresh <= kLaneVMax && pnn_max + gain <= kLaneNMax;
+                lane_ok = lane_ok && pa.nvp + R.n_fresh <= A.lane_vmax && pnn_max + gain <= kLaneNMax;
                 const Fwd fw = fwd_prepare(P, A, L, sm, R, ev, pa, sid, true);
                 fwd_on = fw.on;
                 if (fw.on) cnt = fwd_count(P, L, sm, R, pa, fw);

@@ -104,6 +104,7 @@ struct LevelArgs {
     uint8_t* fmode;             // [F] bit 0: children hashed lane-per-child; bit 1: forwarding
     uint32_t fwd_mode;          // 0 off, 1 every eligible state, 2 states with >= 48 edges
     uint32_t ev_keys;           // event signature keys (0 = no event canonicalisation)
+    uint32_t lane_vmax;         // largest child (vertices) of this level the lane path takes
     uint32_t* work;             // work-queue counters
     // select / assign
     uint32_t* flag_new;         // [n_events]
