@@ -874,7 +874,45 @@ __device__ uint32_t wl_distinct(const uint64_t* cur, const uint32_t* deg, uint32
     return total;
 }
 
-__device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, WlInfo& info) {
+// Whether a staged parent is one component: lock-free union-find over its edges (as in warp_wl),
+// then one root among its vertices (every staged vertex occurs in an edge). Uses the layout's
+// component scratch.
+__device__ bool parent_connected(const Layout& L, char* sm, const Parent& pa) {
+    const uint32_t lane = lane_id();
+    const uint8_t* pear = smp<uint8_t>(sm, L.o_pear);
+    const uint16_t* pevo = smp<uint16_t>(sm, L.o_pevo);
+    const uint16_t* vloc = smp<uint16_t>(sm, L.o_vloc);
+    uint32_t* comp = smp<uint32_t>(sm, L.o_comp);
+    for (uint32_t v = lane; v < pa.nvp; v += 32) comp[v] = v;
+    __syncwarp();
+    {
+        volatile uint32_t* vc = comp;
+        for (uint32_t e = lane; e < pa.ne; e += 32) {
+            const uint32_t a = pear[e], vo = pevo[e];
+            for (uint32_t q = 1; q < a; ++q) {
+                uint32_t x = vloc[vo], y = vloc[vo + q];
+                for (uint32_t tries = 0; tries < 2 * pa.nvp + 8; ++tries) {
+                    while (vc[x] != x) x = vc[x];
+                    while (vc[y] != y) y = vc[y];
+                    if (x == y) break;
+                    if (x < y) { const uint32_t t = x; x = y; y = t; }
+                    if (atomicCAS(&comp[x], x, y) == x) break;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    uint32_t nroots = 0;
+    for (uint32_t v = lane; v < pa.nvp; v += 32) nroots += comp[v] == v ? 1u : 0u;
+    const bool one = warp_sum32(nroots) == 1;
+    __syncwarp();
+    return one;
+}
+
+// connected: the child is known to be one component (a connected parent under a rule whose
+// right-hand side joins every left-hand vertex): the union-find is skipped.
+__device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, WlInfo& info,
+                        bool connected = false) {
     const uint32_t lane = lane_id();
     const uint8_t* car = smp<uint8_t>(sm, L.o_car);
     const uint16_t* cvo = smp<uint16_t>(sm, L.o_cvo);
@@ -993,32 +1031,35 @@ __device__ uint64_t warp_wl(const Layout& L, char* sm, uint32_t ne, uint32_t V, 
     }
 
     // components (union-find on one lane; the partition is what enters the hash)
-    for (uint32_t v = lane; v < V; v += 32) { comp[v] = v; csum[v] = 0; ccnt[v] = 0; }
-    __syncwarp();
-    // lock-free union-find: a root is only ever hooked under a smaller root (atomicCAS), so the
-    // forest stays acyclic and every failed hook means another lane made progress
-    {
-        volatile uint32_t* vc = comp;
-        for (uint32_t e = lane; e < ne; e += 32) {
-            const uint32_t a = car[e], vo = cvo[e];
-            for (uint32_t q = 1; q < a; ++q) {
-                uint32_t x = vloc[vo], y = vloc[vo + q];
-                for (uint32_t tries = 0; tries < 2 * V + 8; ++tries) {
-                    while (vc[x] != x) x = vc[x];
-                    while (vc[y] != y) y = vc[y];
-                    if (x == y) break;
-                    if (x < y) { const uint32_t t = x; x = y; y = t; }
-                    if (atomicCAS(&comp[x], x, y) == x) break;
+    bool one = connected;
+    if (!connected) {
+        for (uint32_t v = lane; v < V; v += 32) { comp[v] = v; csum[v] = 0; ccnt[v] = 0; }
+        __syncwarp();
+        // lock-free union-find: a root is only ever hooked under a smaller root (atomicCAS), so the
+        // forest stays acyclic and every failed hook means another lane made progress
+        {
+            volatile uint32_t* vc = comp;
+            for (uint32_t e = lane; e < ne; e += 32) {
+                const uint32_t a = car[e], vo = cvo[e];
+                for (uint32_t q = 1; q < a; ++q) {
+                    uint32_t x = vloc[vo], y = vloc[vo + q];
+                    for (uint32_t tries = 0; tries < 2 * V + 8; ++tries) {
+                        while (vc[x] != x) x = vc[x];
+                        while (vc[y] != y) y = vc[y];
+                        if (x == y) break;
+                        if (x < y) { const uint32_t t = x; x = y; y = t; }
+                        if (atomicCAS(&comp[x], x, y) == x) break;
+                    }
                 }
             }
         }
+        __syncwarp();
+        // one component (the usual case): its term folds every vertex and edge, so the per-root
+        // sums -- shared-memory atomics that would all hit the one root -- are skipped
+        uint32_t nroots = 0;
+        for (uint32_t v = lane; v < V; v += 32) nroots += (deg[v] && comp[v] == v) ? 1u : 0u;
+        one = warp_sum32(nroots) == 1;
     }
-    __syncwarp();
-    // one component (the usual case): its term folds every vertex and edge, so the per-root
-    // sums -- shared-memory atomics that would all hit the one root -- are skipped
-    uint32_t nroots = 0;
-    for (uint32_t v = lane; v < V; v += 32) nroots += (deg[v] && comp[v] == v) ? 1u : 0u;
-    const bool one = warp_sum32(nroots) == 1;
     uint64_t vs = 0, es = 0, cs = 0;
     for (uint32_t v = lane; v < V; v += 32) {
         if (!deg[v]) continue;
@@ -1570,6 +1611,9 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
         if (lane == 0 && c_lo == 0) b_hbm += 4ull * (pa.ne + (pa.ne + 3) / 4 + pa.nocc) + 20;
         if (kLane) build_parent_csr(L, sm, pa);
         else build_join_index(L, sm, pa);
+        // warp path: whether the parent is one component (then so is every child of a rule whose
+        // right-hand side joins its left-hand vertices, and warp_wl skips its union-find)
+        const bool pconn = !kLane && parent_connected(L, sm, pa);
         for (uint32_t r = 0; r < A.rules_stride && r < ev.rule_count; ++r) {
             const uint32_t item = f * A.rules_stride + r;
             if (lane == 0 && c_lo == 0) b_stage += 4ull * pa.ne + 4ull * pa.nocc;   // join: ids and vertices
@@ -1698,7 +1742,8 @@ __global__ void __launch_bounds__(256, 3) k_expand(DevPtrs P, LevelArgs A, Layou
                         for (uint32_t k = 0; k < R.n_lhs; ++k) rpos[k] = static_cast<uint8_t>(match[k]);
                         const uint32_t nec = build_child(L, sm, R, pa, nm);
                         WlInfo info;
-                        const uint64_t h = warp_wl(L, sm, nec, pa.nvp + R.n_fresh, info);
+                        const uint64_t h = warp_wl(L, sm, nec, pa.nvp + R.n_fresh, info,
+                                                   pconn && (R.flags & kRuleRhsJoinsLhs));
                         if (lane == 0) finish(idx, h, info, rpos);
                         __syncwarp();
                     }
