@@ -1316,6 +1316,7 @@ struct Engine::Impl {
         tic();
         k_roots<<<sh.grid, sh.block, sh.smem, st>>>(ptrs(), root_ids.p, nr, work.p, L);
         check_launch();
+        hist.have_ok = false;   // the roots move the class and state counters
         k_root_counts<<<grid_for(nr, 256), 256, 0, st>>>(ptrs(), root_ids.p, nr);
         check_launch();
         toc(times.roots);
@@ -1761,6 +1762,9 @@ struct Engine::Impl {
     struct LevelHist {
         bool valid = false;
         double ev_per_state = 0, ev_per_new = 0;
+        bool have_ok = false;   // have, stopped: evolution 0's classes, states and stopped flag
+        unsigned long long have[2] = {0, 0};   // after the last range (one evolution)
+        uint32_t stopped = 0;
     } hist;
     uint32_t sub_nf = 0;                           // next-frontier states written by earlier ranges
     uint64_t sub_ne = 0, sub_no = 0, sub_ev = 0, sub_new = 0;
@@ -1780,10 +1784,12 @@ struct Engine::Impl {
         if (one_capped && opt.level_split >= 2) {
             if (F > opt.level_split) P = static_cast<uint32_t>(opt.level_split);
         } else if (one_capped && opt.level_split == 0 && hist.valid && F >= 4096) {
-            unsigned long long have[2];
-            readback(&have[0], evo_classes.p, 8);
-            readback(&have[1], evo_states.p, 8);
-            sync_st();
+            unsigned long long have[2] = {hist.have[0], hist.have[1]};
+            if (!hist.have_ok) {
+                readback(&have[0], evo_classes.p, 8);
+                readback(&have[1], evo_states.p, 8);
+                sync_st();
+            }
             const uint64_t h = h_evos[0].quotient ? have[0] : have[1];
             const uint64_t remaining = h_evos[0].max_states > h ? h_evos[0].max_states - h : 0;
             const double need = double(remaining) * (h_evos[0].quotient ? hist.ev_per_new : 1.0);
@@ -1799,17 +1805,23 @@ struct Engine::Impl {
         if (P < F) parts.emplace_back(P, F);
         bool cut = false;
         uint32_t stopped = 0;
+        // evolution 0's stopped flag: from the last range's second sync, else read
+        auto stopped_now = [&]() -> uint32_t {
+            if (hist.have_ok) return hist.stopped;
+            uint32_t v = 0;
+            readback(&v, evo_stopped.p, 4);
+            sync_st();
+            return v;
+        };
         for (size_t j = 0; j < parts.size(); ++j) {
             if (j > 0 && one_capped) {
-                readback(&stopped, evo_stopped.p, 4);
-                sync_st();
+                stopped = stopped_now();
                 if (stopped) break;
             }
             level_range(opt, parts[j].first, parts[j].second);
         }
         if (parts.size() > 1 && one_capped) {
-            readback(&stopped, evo_stopped.p, 4);
-            sync_st();
+            stopped = stopped_now();
             // a level with a cut sends none of the evolution's new states on (the cut range has
             // sent none of its own; the earlier ranges' are dropped here)
             cut = stopped != 0;
@@ -1843,6 +1855,7 @@ struct Engine::Impl {
         if (F == 0) return;
         const uint32_t R = rm.stride;
         const uint64_t items = uint64_t(F) * R;
+        hist.have_ok = false;   // until this range's second sync
         if (items + 1 > 0xFFFFFFFFull) throw std::runtime_error("hgx: frontier too large for one level");
         const uint32_t NI = static_cast<uint32_t>(items);
         counts.ensure(NI, 0, st);
@@ -1902,7 +1915,7 @@ struct Engine::Impl {
         const size_t nevo = h_evos.size();
         const size_t w1 = 5 + 4 * nevo;
         sync_pack.ensure(w1, 0, st);
-        unsigned long long* hs = sync_host(std::max<size_t>(w1, (7 * nevo + 4 + 1) / 2));
+        unsigned long long* hs = sync_host(std::max<size_t>(w1, (7 * nevo + 9 + 1) / 2));
         k_sync1_pack<<<grid_for(std::max<size_t>(nevo, 1), 256), 256, 0, st>>>(
             item_ev.p, item_cons.p, item_prod.p, item_fresh.p, NI, level_max.p, evo_classes.p,
             evo_states.p, opt.event_keys ? evo_sigs.p : nullptr, evo_first_ev.p, evo_last_ev.p,
@@ -2230,7 +2243,7 @@ struct Engine::Impl {
         // per-evolution ranges of this level (events kept, new states, branchial pairs)
         A.state_base = static_cast<uint32_t>(n_states);
         A.bbase = static_cast<uint32_t>(n_bpairs);
-        lvl_ranges.ensure(7 * nevo + 4, 0, st);
+        lvl_ranges.ensure(7 * nevo + 9, 0, st);
         if (ne2 || F_eff) {
             A.n_frontier = F;   // boundaries over the whole frontier; event ranges clamp to ne2
             k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, lvl_ranges.p);
@@ -2238,12 +2251,18 @@ struct Engine::Impl {
             A.n_frontier = F_eff;
         }
         // ---- sync 2: new states, next frontier, branchial pairs, errors (behind the ranges)
-        k_sync2_pack<<<1, 32, 0, st>>>(flag_rep.p, flag_front.p, boff.p, ne2, err.p,
-                                       lvl_ranges.p + 7 * nevo);
+        k_sync2_pack<<<1, 32, 0, st>>>(flag_rep.p, flag_front.p, boff.p, ne2, err.p, evo_classes.p,
+                                       evo_states.p, evo_stopped.p, lvl_ranges.p + 7 * nevo);
         check_launch();
-        uint32_t* hs2 = reinterpret_cast<uint32_t*>(sync_host((7 * nevo + 4 + 1) / 2));
-        readback(hs2, lvl_ranges.p, (7 * nevo + 4) * 4);
+        uint32_t* hs2 = reinterpret_cast<uint32_t*>(sync_host((7 * nevo + 9 + 1) / 2));
+        readback(hs2, lvl_ranges.p, (7 * nevo + 9) * 4);
         sync_st();
+        if (nevo == 1) {
+            hist.have[0] = hs2[7 * nevo + 4] | (uint64_t(hs2[7 * nevo + 5]) << 32);
+            hist.have[1] = hs2[7 * nevo + 6] | (uint64_t(hs2[7 * nevo + 7]) << 32);
+            hist.stopped = hs2[7 * nevo + 8];
+            hist.have_ok = true;
+        }
         const std::vector<uint32_t> h_rng(hs2, hs2 + 7 * nevo);
         const uint32_t* s2 = hs2 + 7 * nevo;
         if (tune) {

@@ -1897,14 +1897,23 @@ __global__ void k_sync1_pack(const uint32_t* item_ev, const uint32_t* item_cons,
 
 // The level's second read-back rides behind the per-evolution ranges: new states, next-frontier
 // states, branchial pairs and the error flags.
+// out[4..8]: evolution 0's class and state counters and its stopped flag (final for the range:
+// k_rep has run), which the level's range loop and the next level's prefix estimate read without
+// round trips of their own.
 __global__ void k_sync2_pack(const uint32_t* flag_rep, const uint32_t* flag_front,
                              const uint32_t* boff, uint32_t ne2, const uint32_t* err,
-                             uint32_t* out) {
+                             const unsigned long long* classes, const unsigned long long* states,
+                             const uint32_t* stopped, uint32_t* out) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         out[0] = flag_rep[ne2];
         out[1] = flag_front[ne2];
         out[2] = boff[ne2];
         out[3] = *err;
+        out[4] = static_cast<uint32_t>(classes[0]);
+        out[5] = static_cast<uint32_t>(classes[0] >> 32);
+        out[6] = static_cast<uint32_t>(states[0]);
+        out[7] = static_cast<uint32_t>(states[0] >> 32);
+        out[8] = stopped[0];
     }
 }
 
