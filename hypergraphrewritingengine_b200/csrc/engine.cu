@@ -443,7 +443,7 @@ struct Engine::Impl {
     DVec<uint32_t> bcount, boff, bpairs, scan_sums, sync_buf, root_ids;
     DVec<unsigned long long> stats, totals;
     DVec<uint8_t> fmode, fin;
-    DVec<uint32_t> fin_cnt, evo_frange, lvl_ranges, fin_ids, map_s, map_e, frng, slice_off;
+    DVec<uint32_t> fin_cnt, evo_frange, fin_ids, map_s, map_e, frng, slice_off;
     DVec<unsigned long long> evo_new, ev_anc, ev_sig, evo_sigs;
     DVec<unsigned long long> ev_bmask;
     DVec<uint64_t> fin_rng;
@@ -458,9 +458,10 @@ struct Engine::Impl {
     std::vector<EvoRanges> evo_ranges;
     std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     uint64_t n_roots_admitted = 0;
-    // the per-level read-backs: packed on the device, one copy each into a page-locked block
-    DVec<unsigned long long> sync_pack;
+    // the per-level read-backs: packed by a kernel straight into mapped page-locked memory (no
+    // copy to issue or wait for; the stream's synchronisation makes the writes visible)
     unsigned long long* h_sync = nullptr;
+    unsigned long long* d_sync = nullptr;   // h_sync as the device addresses it
     size_t h_sync_words = 0;
     unsigned long long* sync_host(size_t words) {
         if (words > h_sync_words) {
@@ -468,7 +469,8 @@ struct Engine::Impl {
             if (h_sync) HGX_CUDA_CHECK(cudaFreeHost(h_sync));
             h_sync = nullptr;
             const size_t nw = std::max<size_t>(words, 2 * h_sync_words);
-            HGX_CUDA_CHECK(cudaMallocHost(reinterpret_cast<void**>(&h_sync), nw * 8));
+            HGX_CUDA_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&h_sync), nw * 8, cudaHostAllocMapped));
+            HGX_CUDA_CHECK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&d_sync), h_sync, 0));
             h_sync_words = nw;
         }
         return h_sync;
@@ -920,14 +922,12 @@ struct Engine::Impl {
         ev_bmask.release(st);
         ev_sig.release(st);
         evo_sigs.release(st);
-        lvl_ranges.release(st);
         fin_ids.release(st);
         map_s.release(st);
         map_e.release(st);
         fin_rng.release(st);
         fin_tab.release(st);
         fin_sec.release(st);
-        sync_pack.release(st);
         sr_dev.release(st);
         cudaStreamSynchronize(cst);
         for (uint8_t* b : sr.bufs) cudaFreeAsync(b, st);
@@ -1914,14 +1914,12 @@ struct Engine::Impl {
         // ---- sync 1: level totals, per-evolution event ranges, exact frontier maxima
         const size_t nevo = h_evos.size();
         const size_t w1 = 5 + 4 * nevo;
-        sync_pack.ensure(w1, 0, st);
-        unsigned long long* hs = sync_host(std::max<size_t>(w1, (7 * nevo + 9 + 1) / 2));
+        const unsigned long long* hs = sync_host(std::max<size_t>(w1, (7 * nevo + 9 + 1) / 2));
         k_sync1_pack<<<grid_for(std::max<size_t>(nevo, 1), 256), 256, 0, st>>>(
             item_ev.p, item_cons.p, item_prod.p, item_fresh.p, NI, level_max.p, evo_classes.p,
             evo_states.p, opt.event_keys ? evo_sigs.p : nullptr, evo_first_ev.p, evo_last_ev.p,
-            static_cast<uint32_t>(nevo), sync_pack.p);
+            static_cast<uint32_t>(nevo), d_sync);
         check_launch();
-        readback(hs, sync_pack.p, w1 * 8);
         sync_st();
         if (sr.on) stream_issue();   // the previous range's result chunk (its counts are here now)
         const uint32_t tot[6] = {uint32_t(hs[0]), uint32_t(hs[0] >> 32), uint32_t(hs[1]),
@@ -2243,19 +2241,18 @@ struct Engine::Impl {
         // per-evolution ranges of this level (events kept, new states, branchial pairs)
         A.state_base = static_cast<uint32_t>(n_states);
         A.bbase = static_cast<uint32_t>(n_bpairs);
-        lvl_ranges.ensure(7 * nevo + 9, 0, st);
+        const uint32_t* hs2 = reinterpret_cast<const uint32_t*>(sync_host((7 * nevo + 9 + 1) / 2));
+        uint32_t* ds2 = reinterpret_cast<uint32_t*>(d_sync);
         if (ne2 || F_eff) {
             A.n_frontier = F;   // boundaries over the whole frontier; event ranges clamp to ne2
-            k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, lvl_ranges.p);
+            k_evo_ranges<<<grid_for(F, 256), 256, 0, st>>>(ptrs(), A, evo_last_ev.p, ds2);
             check_launch();
             A.n_frontier = F_eff;
         }
         // ---- sync 2: new states, next frontier, branchial pairs, errors (behind the ranges)
         k_sync2_pack<<<1, 32, 0, st>>>(flag_rep.p, flag_front.p, boff.p, ne2, err.p, evo_classes.p,
-                                       evo_states.p, evo_stopped.p, lvl_ranges.p + 7 * nevo);
+                                       evo_states.p, evo_stopped.p, ds2 + 7 * nevo);
         check_launch();
-        uint32_t* hs2 = reinterpret_cast<uint32_t*>(sync_host((7 * nevo + 9 + 1) / 2));
-        readback(hs2, lvl_ranges.p, (7 * nevo + 9) * 4);
         sync_st();
         if (nevo == 1) {
             hist.have[0] = hs2[7 * nevo + 4] | (uint64_t(hs2[7 * nevo + 5]) << 32);
